@@ -1,0 +1,357 @@
+"""Benchmark: close-coupling scattering solves per second on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload cfg1|cfg2|cfg0]
+
+One step = one pass of the hot path over one batch: for ``cfg1`` one full
+solve of the 41x41-channel, 200-node hexagonal He-4 system (336,200 complex
+unknowns); for ``cfg2`` the 512-beam batched sweep (uneven channel counts);
+``cfg0`` is the small square case.  ``value`` is whole-job solves/s with the
+inputs resident in HBM; ``e2e`` is the same metric through the drop-in
+``run_multiscat_fortran`` call with host buffers (H2D/D2H inside the timed
+region).  Multi-GPU runs are independent replicas (weak scaling, no
+collective on the data path); the time is the max over ranks.
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+oracle: a C restatement of the reference Fortran solve) on the host cores,
+on a bounded sample of the same workload, extrapolated to a full solve.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "solves/s (close-coupling S-matrix solves, FP64 plain form; mixed+batched target)"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return dict(PEAKS_FALLBACK), "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples: list[list[str]] = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                     "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                line = out.stdout.strip().splitlines()
+                if line:
+                    self.samples.append([x.strip() for x in line[0].split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 2 + i and s[2 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+
+def build_workload(name: str):
+    from multiscat_b200 import workloads as wl
+    if name == "cfg1":
+        case = wl.cfg1_case()
+        return case, [case.system()]
+    if name == "cfg0":
+        case = wl.cfg0_case()
+        return case, [case.system()]
+    if name == "cfg2":
+        return wl.cfg2_batch()
+    raise ValueError(name)
+
+
+def algorithmic_counts(n: int, rows: int, taps: int) -> dict:
+    """Per-launch algorithmic work of the kernels (one launch covers all rows).
+
+    block inverse: two real GEMMs (n x n) x (n x 2 rows): 8 n^2 rows flops;
+    reads x and writes u once (32 n rows bytes) plus E, E^T.
+    coupling: 8 taps flops per complex output; reads src + in0, writes out.
+    """
+    return {
+        "block_inverse_flops": 8.0 * n * n * rows,
+        "block_inverse_bytes": 32.0 * n * rows + 16.0 * n * n,
+        "coupling_flops": 8.0 * taps * n * rows,
+        "coupling_bytes": 48.0 * n * rows + 16.0 * taps * n,
+    }
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+
+def run_b200(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from multiscat_b200 import ScatteringPlan, run_multiscat_fortran
+    from multiscat_b200 import _native as nat
+
+    case, systems = build_workload(args.workload)
+    plan = ScatteringPlan(case.v, case.t, systems, rtol=args.rtol, restart=args.restart)
+    n_solves = len(systems)
+    stream = torch.cuda.current_stream()
+    dev_time = []
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        res = plan.solve()
+    torch.cuda.synchronize()
+    iters = res.iterations.tolist()
+
+    plan.enable_kernel_timing(True)
+    barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            res = plan.solve()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = start.elapsed_time(stop)
+    ktimes = plan.kernel_timing()
+    plan.enable_kernel_timing(False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n_solves * args.steps / (ms / 1e3)
+
+    # e2e: the drop-in call with host buffers (one full-grid system per step)
+    e2e = None
+    if len(systems) == 1 and systems[0].pkd.size == case.v.shape[0] * case.v.shape[1]:
+        host = [case.v, case.pkd, case.wa, case.wb, case.wc, case.t]
+        h2d = sum(int(np.asarray(a).nbytes) for a in host)
+        d2h = int(case.v.nbytes)
+        run_multiscat_fortran(1, 10, *host[:1], *host[1:])
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e_steps = max(1, min(args.steps, 5))
+        e0.record(stream)
+        for _ in range(e_steps):
+            run_multiscat_fortran(1, 10, *host[:1], *host[1:])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * e_steps / (ems / 1e3), "unit": "solves/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "path": "run_multiscat_fortran (host numpy in/out, rtol 5e-13)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_sample(args.workload, case, systems, budget_s=args.cpu_budget)
+
+    peaks, peak_kind = load_peaks()
+    n = case.v.shape[2]
+    rows = plan.total_rows
+    counts = algorithmic_counts(n, rows, plan.n_taps)
+    roof = None
+    if ktimes.get("block_inverse", {}).get("launches"):
+        kt = ktimes["block_inverse"]
+        avg_s = kt["ms"] / kt["launches"] / 1e3
+        # FP64 GEMM work: bounded by the FP64 pipe (no FP64 tensor path on
+        # sm_100a); reported against the HBM roofline of its own bytes too.
+        achieved_gbs = counts["block_inverse_bytes"] / avg_s / 1e9
+        roof = {"kernel": "k_block_inverse (FP64 D^-1: 2 GEMMs + Sherman-Morrison)",
+                "bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": None,
+                "peak_source": peak_kind,
+                "fp64_tflops": counts["block_inverse_flops"] / avg_s / 1e12,
+                "avg_launch_us": avg_s * 1e6, "launches": kt["launches"]}
+    kernels = {}
+    for k, v in ktimes.items():
+        if v.get("launches"):
+            kernels[k] = {"avg_us": 1e3 * v["ms"] / v["launches"], "launches": v["launches"],
+                          "total_ms": v["ms"]}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded corrugated-Morse potentials built in-process)",
+            "config": {"workload": case.name, "systems_per_step": n_solves, "rows": rows,
+                       "n_z": n, "taps": plan.n_taps, "restart": args.restart,
+                       "rtol": args.rtol, "precision": "fp64",
+                       "l2": "working set (Krylov basis) exceeds the 126 MB L2",
+                       "parallelism": f"replicas x{world}"},
+            "iterations": iters, "roofline": roof, "kernels": kernels,
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
+            "gpu_launches": plan.launches_per_solve(res) * args.steps,
+        }
+        print(json.dumps(line))
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# reference (CPU) arm
+# ---------------------------------------------------------------------------
+
+def _oracle_time(case, system, maxiter: int) -> tuple[float, int]:
+    from oracle import solver as osol
+    t0 = time.perf_counter()
+    _, info, iters, _ = osol.solve_channels(case.v, system.channel_ix, system.channel_iy, system.pkd,
+                                            system.wave_c, system.specular,
+                                            system.wave_b[system.specular], case.t,
+                                            eps=0.5e-10, maxiter=maxiter)
+    return time.perf_counter() - t0, iters
+
+
+def _full_iterations(workload: str) -> int:
+    g = ROOT / "tests" / "golden" / {"cfg1": "oracle_cfg1.json", "cfg0": "oracle_cfg0.json"}.get(
+        workload, "oracle_subsets.json")
+    if g.exists():
+        rec = json.loads(g.read_text())
+        if isinstance(rec, list):
+            return int(np.mean([r["iterations"] for r in rec]))
+        return int(rec["iterations"])
+    return 20
+
+
+def cpu_reference_sample(workload: str, case, systems, budget_s: float = 20.0) -> dict:
+    """Time the oracle on a bounded sample and extrapolate to solves/s."""
+    system = systems[0]
+    t1, _ = _oracle_time(case, system, 1)
+    t2, _ = _oracle_time(case, system, 2)
+    per_iter = max(t2 - t1, 1e-9)
+    full = _full_iterations(workload)
+    solve_s = t1 + (full - 1) * per_iter
+    return {"value": 1.0 / solve_s, "unit": "solves/s", "cores": 1, "kind": "port",
+            "sample": (f"oracle (C restatement of the reference Fortran GMRES) on system 0 of "
+                       f"{workload}: timed 1- and 2-iteration runs ({t1:.2f}s, {t2:.2f}s), "
+                       f"extrapolated to the oracle's {full} iterations"),
+            "seconds_per_solve": solve_s}
+
+
+def run_reference(args) -> None:
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import solver as osol
+    osol.build()
+    case, systems = build_workload(args.workload)
+    system = systems[0]
+    full = _full_iterations(args.workload)
+    t1, _ = _oracle_time(case, system, 1)
+    for _ in range(max(0, args.warmup - 1)):
+        _oracle_time(case, system, 1)
+    t2, _ = _oracle_time(case, system, 2)
+    per_iter = max(t2 - t1, 1e-9)
+    samples = []
+    for _ in range(args.steps):
+        t, _ = _oracle_time(case, system, 1)
+        samples.append(t)
+    t_step = float(np.mean(samples))
+    solve_s = t_step + (full - 1) * per_iter
+    value = 1.0 / solve_s
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * solve_s, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": case.name, "systems_per_step": 1},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "port",
+                         "sample": (f"each step: 1-iteration oracle solve ({t_step:.2f}s mean); "
+                                    f"per-iteration cost {per_iter:.2f}s; extrapolated to "
+                                    f"{full} iterations")},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg0"])
+    ap.add_argument("--rtol", type=float, default=1e-10)
+    ap.add_argument("--restart", type=int, default=30)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

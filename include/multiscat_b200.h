@@ -1,0 +1,178 @@
+/*
+ * multiscat_b200.h -- C-ABI of the B200 close-coupling scattering solver.
+ *
+ * Plain C types only (no torch, no C++).  Complex numbers are interleaved
+ * (re, im) pairs of double or float.  Every function returns an msc_status
+ * and never aborts the process.
+ *
+ * Reference interfaces replaced (paths relative to the multiscat project):
+ *   msc_run_multiscat   <- run_multiscat_fortran
+ *        lib/multiscat_fortran/fortran/multiscat_python_bindings.f90:1-61
+ *        lib/multiscat_fortran/fortran/multiscat_python_bindings.pyf:3-17
+ *        lib/multiscat_fortran/src/multiscat_fortran/__init__.py:39-60
+ *   msc_plan_* / msc_solve  <- solve_scattering_gmres + run_preconditioned_gmres
+ *        lib/multiscat_fortran/fortran/multiscat_gmres.f90:105-202
+ *        (batched, device-resident form; no reference counterpart for the
+ *        batching itself)
+ *   msc_debug_apply_coupling     <- debug_apply_upper_block
+ *        multiscat_gmres.f90:338-382 (full off-diagonal coupling here)
+ *   msc_debug_apply_block_inverse <- the block-diagonal inverse D^-1 of
+ *        multiscat/multiscat/_scipy.py:249-259 (apply_inverse_diagonal)
+ *   msc_intensities          <- _get_scattered_intensity_data
+ *        multiscat/multiscat/_multiscat.py:40-60
+ */
+#ifndef MULTISCAT_B200_H
+#define MULTISCAT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1 and 2 keep the meaning of the reference's ierr
+ * (bindings.f90:42-45 bad dimensions, :58-60 GMRES not converged). */
+typedef enum {
+    MSC_OK = 0,
+    MSC_ERR_DIMS = 1,          /* non-positive or inconsistent sizes        */
+    MSC_ERR_NOT_CONVERGED = 2, /* iteration limit reached                   */
+    MSC_ERR_CUDA = 3,          /* CUDA runtime error or allocation failure  */
+    MSC_ERR_NONFINITE = 4,     /* NaN/Inf met in a residual                 */
+    MSC_ERR_EIGEN = 5,         /* preconditioner eigensolver failed         */
+    MSC_ERR_ARG = 6,           /* null pointer or unsupported option        */
+    MSC_ERR_NOT_BUILT = 7      /* solver compiled without a needed feature  */
+} msc_status;
+
+/* Arithmetic of the inner Krylov solve. */
+typedef enum {
+    MSC_PRECISION_FP64 = 0,   /* plain FP64 restarted GMRES                  */
+    MSC_PRECISION_MIXED = 1   /* FP32 inner GMRES, FP64 iterative refinement */
+} msc_precision;
+
+/* Sizes and options of one plan.  A plan holds one potential (one z grid,
+ * one coupling torus nkx x nky) and a batch of n_systems beams, each with
+ * its own channel list. */
+typedef struct {
+    int32_t n_z;            /* Lobatto nodes per channel (<= 512)               */
+    int32_t nkx, nky;       /* coupling torus (the potential's Fourier grid)    */
+    int32_t n_systems;      /* batch size                                       */
+    int32_t restart;        /* GMRES restart length m (1..64)                   */
+    int32_t max_iterations; /* total Krylov iterations per system               */
+    double rtol;            /* stop when ||b - A psi|| <= rtol ||b|| (per system)*/
+    int32_t precision;      /* msc_precision                                    */
+    int32_t inner_restart;  /* mixed: inner FP32 restart length (0 = restart)   */
+    double inner_rtol;      /* mixed: inner relative tolerance (0 = 1e-4)       */
+    int32_t max_refinements;/* mixed: outer FP64 refinement steps (0 = 30)      */
+} msc_plan_desc;
+
+typedef struct msc_plan msc_plan;
+
+/* Per-system result written by msc_solve. */
+typedef struct {
+    int32_t iterations;     /* Krylov iterations (inner iterations for mixed) */
+    int32_t refinements;    /* FP64 outer steps (mixed), restart cycles (FP64)*/
+    int32_t status;         /* msc_status of this system                      */
+    int32_t reserved;
+    double residual;        /* final true relative residual ||b-A psi||/||b|| */
+} msc_result;
+
+/* Create a plan on the current CUDA device.  Allocates all device memory
+ * the solve needs; *plan is NULL on failure. */
+msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc);
+msc_status msc_plan_destroy(msc_plan *plan);
+
+/* Set the potential (host arrays, C order):
+ *   potential_values  complex [nkx][nky][n_z]  V_G(z_k) in 1/Angstrom^2
+ *   kinetic           double  [n_z][n_z]       positive Lobatto kinetic T
+ * Builds H0 = T + diag Re V_00, its eigen-decomposition (FP64) and the
+ * coupling taps (all nonzero V_G with G != 0).
+ * Replaces build_preconditioner, multiscat_gmres.f90:226-273. */
+msc_status msc_plan_set_potential(msc_plan *plan, const double *potential_values,
+                                  const double *kinetic);
+
+/* Set system s's channels (host arrays):
+ *   n_channels        C_s (<= nkx*nky)
+ *   channel_ix/iy     storage position of each channel on the torus [C_s]
+ *   pkd               perpendicular kinetic difference per channel [C_s]
+ *   wave_b, wave_c    complex per channel [C_s]
+ *   specular          index of the specular channel in this list
+ *   wave_a_spec       complex a of the specular channel (for S extraction)
+ * All systems must be set before msc_solve. */
+msc_status msc_plan_set_system(msc_plan *plan, int32_t s, int32_t n_channels,
+                               const int32_t *channel_ix, const int32_t *channel_iy,
+                               const double *pkd, const double *wave_b,
+                               const double *wave_c, int32_t specular,
+                               const double *wave_a_spec);
+
+/* Solve all systems.  psi_out (device, may be NULL): complex FP64 packed
+ * rows [sum_s C_s][n_z] in system order.  intensities_out (device, may be
+ * NULL): double [sum_s C_s] = |S_G0|^2.  results (host, may be NULL):
+ * msc_result [n_systems].  stream is a cudaStream_t (NULL = legacy). */
+msc_status msc_solve(msc_plan *plan, double *psi_out, double *intensities_out,
+                     msc_result *results, void *stream);
+
+/* Total channel rows of the plan (sum of C_s) once all systems are set. */
+int64_t msc_plan_total_rows(const msc_plan *plan);
+
+/* Drop-in twin of the reference's run_multiscat_fortran (host buffers,
+ * synchronous).  potential_values complex [nkx][nky][nz], perpendicular_
+ * kinetic_difference [nkx][nky], waves complex [nkx*nky] (wave_a unused, as
+ * in the reference), parallel_kinetic_energy [nz][nz]; scattered_state_out
+ * complex [nkx][nky][nz].  gmres_preconditioner_flag is accepted for
+ * signature parity (this solver always uses its block-diagonal
+ * preconditioner); the stop rule is ||b - A psi|| <= 0.005 * 10^-sig ||b||.
+ * iterations_out may be NULL.  Returns 0, 1 (bad dims), 2 (not converged)
+ * or another msc_status. */
+int msc_run_multiscat(int gmres_preconditioner_flag, int convergence_significant_figures,
+                      int nkx, int nky, int nz, const double *potential_values,
+                      const double *perpendicular_kinetic_difference,
+                      const double *wave_a, const double *wave_b, const double *wave_c,
+                      const double *parallel_kinetic_energy, double *scattered_state_out,
+                      int *iterations_out);
+
+/* Debug / test entry points on device buffers of one full-grid system
+ * (plan with n_systems == 1):
+ *   msc_debug_apply_coupling:       y = sum_{G' != G} V_{G-G'} x_{G'}
+ *   msc_debug_apply_block_inverse:  y = D^-1 x
+ *   msc_debug_apply_operator:       y = A x = D x + V_off x
+ * x, y: complex FP64 [C][n_z] device pointers. */
+msc_status msc_debug_apply_coupling(msc_plan *plan, const double *x, double *y, void *stream);
+msc_status msc_debug_apply_block_inverse(msc_plan *plan, const double *x, double *y, void *stream);
+msc_status msc_debug_apply_operator(msc_plan *plan, const double *x, double *y, void *stream);
+
+/* |S_G0|^2 per channel from psi[C][n_z] (device pointers), for one system. */
+msc_status msc_intensities(msc_plan *plan, int32_t s, const double *psi, double *intensities,
+                           void *stream);
+
+/* Plan facts for callers and benchmarks. */
+typedef struct {
+    int64_t total_rows;        /* sum over systems of C_s                          */
+    int32_t n_taps;            /* nonzero off-diagonal coupling taps               */
+    int32_t n_tiles;           /* row tiles (kernel grid size)                     */
+    int64_t launches_last;     /* kernel launches issued by the last msc_solve     */
+    int32_t cycles_last;       /* restart cycles run by the last msc_solve         */
+    int32_t reserved;
+} msc_plan_info;
+
+msc_status msc_plan_get_info(const msc_plan *plan, msc_plan_info *info);
+
+/* Kernel timing (measurement only).  When enabled, the solve graphs carry
+ * CUDA event pairs around every Arnoldi-step launch of kernel kind k
+ * (0 = block-diagonal inverse, 1 = channel coupling) and msc_solve adds the
+ * device time of the launches that did work.  msc_plan_kernel_timing copies
+ * ms[2] and launches[2] accumulated since the previous call and resets them. */
+msc_status msc_plan_set_kernel_timing(msc_plan *plan, int enable);
+msc_status msc_plan_kernel_timing(msc_plan *plan, double *ms, int64_t *launches);
+
+/* Human-readable text of the last error on this thread. */
+const char *msc_last_error(void);
+
+/* Library version string. */
+const char *msc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MULTISCAT_B200_H */

@@ -1,0 +1,200 @@
+"""Reference-shaped public API: conditions and configs in, intensities out.
+
+Mirrors ``multiscat/multiscat/_multiscat.py:131-175`` (``get_scattering_matrix``)
+and ``multiscat/config.py:41-227`` (``OptimizationConfig``, ``UnitSystem``,
+``ScatteringCondition.from_angles``, ``momentum_from_angles``) with the same
+field names, without the slate basis objects: a condition carries its lattice
+vectors, grid shape, z domain and the potential's Fourier components on the
+Lobatto nodes (what ``potential_as_array`` returns, ``_util.py:150-163``).
+
+``get_scattering_matrix`` returns |S_G0|^2 on the (nkx, nky) channel grid as
+complex128, exactly as the reference's array does (``_multiscat.py:166-175``).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Literal, Sequence
+
+import numpy as np
+
+from . import setup_arrays as sa
+from .solver import ScatteringPlan, SolveResult, channel_subset_system, full_grid_system
+
+
+@dataclass(frozen=True, kw_only=True)
+class OptimizationConfig:
+    """Solver options (``config.py:41-58``) plus the GPU solver's own."""
+
+    precision: float = 1e-5
+    max_iterations: int = 1000
+    use_neumann_preconditioner: bool = True
+    n_channels: int | None = None
+    restart: int = 30
+    precision_mode: Literal["fp64", "mixed"] = "fp64"
+
+    @property
+    def residual_tolerance(self) -> float:
+        """Stop rule ||b - A psi|| <= precision/100 ||b|| (see DESIGN notes in the package)."""
+        if self.precision <= 0:
+            raise ValueError("Optimization precision must be greater than zero")
+        return self.precision * 1e-2
+
+
+@dataclass(frozen=True, kw_only=True)
+class UnitSystem:
+    """Units of a condition (``config.py:61-84``); SI by default."""
+
+    hbar: float = sa.HBAR
+    atomic_mass: float = sa.ATOMIC_MASS
+    angstrom: float = sa.ANGSTROM
+
+    @property
+    def kinetic_energy_unit(self) -> float:
+        return self.hbar**2 / (2 * self.atomic_mass * self.angstrom**2)
+
+
+SI_UNITS = UnitSystem()
+
+
+@dataclass
+class ScatteringMetadata:
+    """Grid of a scattering problem: lattice vectors, channel grid and z domain.
+
+    ``vectors`` are the two lattice vectors (SI lengths, 2 or 3 components);
+    ``shape`` = (nkx, nky, nz); the z domain is [z_start, z_start + z_delta].
+    """
+
+    vectors: tuple[Sequence[float], Sequence[float]]
+    shape: tuple[int, int, int]
+    z_delta: float
+    z_start: float = 0.0
+
+
+def momentum_from_angles(theta: float, phi: float, energy: float, mass: float, *,
+                         units: UnitSystem = SI_UNITS) -> tuple[float, float, float]:
+    """Incident momentum from angles (``config.py:213-227``)."""
+    abs_k = math.sqrt(2 * mass * energy) / units.hbar
+    return (abs_k * math.sin(theta) * math.cos(phi), abs_k * math.sin(theta) * math.sin(phi),
+            abs_k * math.cos(theta))
+
+
+@dataclass
+class ScatteringCondition:
+    """Mass (kg), incident k (1/m), potential V_G(z_k) (J) and grid."""
+
+    mass: float
+    incident_k: tuple[float, float, float]
+    potential_values: np.ndarray
+    metadata: ScatteringMetadata
+    units: UnitSystem = field(default_factory=UnitSystem)
+
+    @staticmethod
+    def from_angles(*, mass: float, theta: float = 0.0, phi: float = 0.0, energy: float,
+                    potential_values, metadata: ScatteringMetadata,
+                    units: UnitSystem = SI_UNITS) -> "ScatteringCondition":
+        return ScatteringCondition(mass, momentum_from_angles(theta, phi, energy, mass, units=units),
+                                   np.asarray(potential_values), metadata, units)
+
+    @property
+    def incident_energy(self) -> float:
+        k2 = sum(k * k for k in self.incident_k)
+        return self.units.hbar**2 * k2 / (2 * self.mass)
+
+
+@dataclass
+class NaturalArrays:
+    """The solver's inputs in natural units (1/A^2, A)."""
+
+    potential_values: np.ndarray
+    kinetic: np.ndarray
+    pkd: np.ndarray
+    wave_a: np.ndarray
+    wave_b: np.ndarray
+    wave_c: np.ndarray
+    nodes: np.ndarray
+    weights: np.ndarray
+
+
+def natural_arrays(condition: ScatteringCondition) -> NaturalArrays:
+    """Convert to hbar = 1, m = 1/2, Angstrom (``_multiscat.py:102-128``) and build arrays."""
+    u = condition.units
+    to_ang = 1.0 / u.angstrom                                   # length unit -> Angstrom
+    energy_to_nat = 2.0 * condition.mass / u.hbar**2 * u.angstrom**2   # energy -> 1/A^2
+    md = condition.metadata
+    nkx, nky, nz = md.shape
+    a1 = np.asarray(md.vectors[0], float)[:2] * to_ang
+    a2 = np.asarray(md.vectors[1], float)[:2] * to_ang
+    # Incident k is read in the lattice frame (a1 along x): rotating both
+    # lattice vectors leaves the result unchanged, as the reference's
+    # tests/test_fixed_example.py:259-330 requires.
+    rot = math.atan2(a1[1], a1[0])
+    cr, sr = math.cos(rot), math.sin(rot)
+    unrot = np.array([[cr, sr], [-sr, cr]])
+    a1, a2 = unrot @ a1, unrot @ a2
+    z0 = md.z_start * to_ang
+    dz = md.z_delta * to_ang
+    k = tuple(float(c) * u.angstrom for c in condition.incident_k)
+    nodes, weights = sa.lobatto_rule(z0, z0 + dz, nz)
+    kinetic = sa.kinetic_matrix(nodes, weights)
+    pkd = sa.perpendicular_kinetic_difference(k, a1, a2, nkx, nky)
+    wa, wb, wc = sa.waves(pkd, weights, z0, dz)
+    v = np.asarray(condition.potential_values, np.complex128).reshape(nkx, nky, nz) * energy_to_nat
+    return NaturalArrays(v, kinetic, pkd, wa, wb, wc, nodes, weights)
+
+
+def _system_for(arr: NaturalArrays, config: OptimizationConfig):
+    if config.n_channels is not None:
+        return channel_subset_system(arr.pkd, arr.wave_a, arr.wave_b, arr.wave_c,
+                                     n_channels=config.n_channels)
+    return full_grid_system(arr.pkd, arr.wave_a, arr.wave_b, arr.wave_c)
+
+
+def _to_grid(result: SolveResult, s: int, system, shape) -> np.ndarray:
+    out = np.zeros(shape, np.complex128)
+    vals = result.system_intensities(s).detach().cpu().numpy()
+    out[system.channel_ix, system.channel_iy] = vals
+    return out
+
+
+def get_scattering_matrix(condition: ScatteringCondition, config: OptimizationConfig, *,
+                          backend: Literal["b200"] = "b200") -> np.ndarray:
+    """|S_G0|^2 on the (nkx, nky) channel grid, complex128 (``_multiscat.py:131-175``)."""
+    if backend != "b200":
+        raise ValueError(f"Unknown backend '{backend}'. Expected 'b200'.")
+    arr = natural_arrays(condition)
+    system = _system_for(arr, config)
+    plan = ScatteringPlan(arr.potential_values, arr.kinetic, [system],
+                          rtol=config.residual_tolerance, restart=config.restart,
+                          max_iterations=config.max_iterations,
+                          precision=config.precision_mode)
+    try:
+        result = plan.solve(raise_on_error=False)
+    finally:
+        plan.close()
+    if result.status[0] != 0:
+        raise RuntimeError(
+            f"B200 GMRES did not converge (status={result.status[0]}, "
+            f"iterations={result.iterations[0]}, residual={result.residual[0]:.3e})")
+    return _to_grid(result, 0, system, condition.metadata.shape[:2])
+
+
+def get_scattering_matrices(conditions: Sequence[ScatteringCondition],
+                            config: OptimizationConfig) -> list[np.ndarray]:
+    """Batched sweep: many beams over ONE potential and grid, one GPU solve."""
+    arrays = [natural_arrays(c) for c in conditions]
+    systems = [_system_for(a, config) for a in arrays]
+    plan = ScatteringPlan(arrays[0].potential_values, arrays[0].kinetic, systems,
+                          rtol=config.residual_tolerance, restart=config.restart,
+                          max_iterations=config.max_iterations,
+                          precision=config.precision_mode)
+    try:
+        result = plan.solve(raise_on_error=False)
+    finally:
+        plan.close()
+    bad = np.nonzero(result.status != 0)[0]
+    if bad.size:
+        raise RuntimeError(f"B200 GMRES did not converge for systems {bad.tolist()}")
+    return [_to_grid(result, s, systems[s], c.metadata.shape[:2])
+            for s, c in enumerate(conditions)]

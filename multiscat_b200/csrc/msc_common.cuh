@@ -1,0 +1,62 @@
+// msc_common.cuh -- shared helpers of the B200 close-coupling solver.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+
+namespace msc {
+
+// Complex arithmetic on interleaved pairs.
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+    return make_double2(a.x + b.x, a.y + b.y);
+}
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) {
+    return make_double2(a.x - b.x, a.y - b.y);
+}
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__host__ __device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) {
+    return make_double2(a.x * s, a.y * s);
+}
+// a / b with scaling (Smith's algorithm).
+__host__ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        double r = b.y / b.x, d = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+    } else {
+        double r = b.x / b.y, d = b.y + b.x * r;
+        return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Row tiles: every tile holds up to kTileRows consecutive channel rows of
+// ONE system, so per-tile partial reductions add up per system.
+constexpr int kTileRows = 8;
+constexpr int kMaxNz = 512;
+constexpr int kMaxRestart = 64;
+constexpr int kMaxTaps = 2048;
+
+struct Tiles {
+    const int *row0;   // first row of the tile
+    const int *nrow;   // rows in the tile (1..kTileRows)
+    const int *sys;    // system of the tile
+    int count;
+};
+
+}  // namespace msc

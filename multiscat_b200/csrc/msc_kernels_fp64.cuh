@@ -1,0 +1,558 @@
+// msc_kernels_fp64.cuh -- FP64 kernels of the close-coupling GMRES solve.
+//
+// State layout in HBM: packed channel rows, psi[row][z] complex interleaved
+// (double2), z contiguous.  A row is one diffraction channel of one system;
+// the rows of a system are contiguous.  This is the reference's
+// scattered_state(nz, C) column-major layout (multiscat_gmres.f90:144),
+// extended with a batch of systems.
+//
+// Operator (per system):  A = D + V_off
+//   (D psi)_G     = T psi_G + (Re V_00 + pkd_G) psi_G - c_G psi_G(z_n) e_n
+//   (V_off psi)_G = sum_{G' != G} V_{(G-G') mod torus}(z) psi_{G'}(z)
+// D_G^-1 uses the eigenbasis of H0 = T + diag Re V_00 (H0 = E diag(lam) E^T)
+// and the Sherman-Morrison boundary term, as the reference's
+// solve_lower_block does per channel (multiscat_gmres.f90:662-685) and
+// apply_inverse_diagonal does for all channels (_scipy.py:249-259).
+#pragma once
+
+#include "msc_common.cuh"
+
+namespace msc {
+
+// ---------------------------------------------------------------------------
+// Block-diagonal inverse:  out (=|+=) D^-1 x   on every row of a tile.
+//   xt = E^T x ; s = sum_k en_k xt_k / (pkd + lam_k) ; beta = c s / (1 - c f_n)
+//   yt = (xt + beta en) / (pkd + lam) ; u = E yt
+// Two FP64 GEMMs along z with the tile's 2*kTileRows real columns staged in
+// shared memory; E and E^T stream from L2 (each is n*n doubles).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_block_inverse(Tiles tiles, const int *__restrict__ gate, int n,
+                const double *__restrict__ E, const double *__restrict__ ET,
+                const double *__restrict__ lam, const double *__restrict__ en,
+                const double *__restrict__ row_pkd, const double2 *__restrict__ row_c,
+                const double *__restrict__ row_fn, const double2 *__restrict__ x,
+                double2 *__restrict__ out, int accumulate)
+{
+    constexpr int TR = kTileRows;
+    constexpr int LD = 2 * TR;       // real columns per z row
+    constexpr int HC = TR;           // columns handled per work item (half of LD)
+    extern __shared__ double smem[];
+    double *Xs = smem;               // [n][LD]
+    double *Ys = smem + (size_t)n * LD;
+    __shared__ double2 beta_s[TR];
+
+    const int tile = blockIdx.x;
+    const int sys = tiles.sys[tile];
+    if (gate && gate[sys] == 0) return;
+    const int row0 = tiles.row0[tile];
+    const int nrow = tiles.nrow[tile];
+
+    for (int idx = threadIdx.x; idx < TR * n; idx += blockDim.x) {
+        int r = idx / n, z = idx - r * n;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < nrow) v = x[(size_t)(row0 + r) * n + z];
+        Xs[z * LD + 2 * r] = v.x;
+        Xs[z * LD + 2 * r + 1] = v.y;
+    }
+    __syncthreads();
+
+    // GEMM 1: Ys[k][c] = sum_z E[z][k] Xs[z][c]
+    for (int item = threadIdx.x; item < 2 * n; item += blockDim.x) {
+        const int k = item >> 1, h = item & 1;
+        double acc[HC];
+#pragma unroll
+        for (int c = 0; c < HC; ++c) acc[c] = 0.0;
+        const double *xs = Xs + h * HC;
+        const double *ek = E + k;
+#pragma unroll 4
+        for (int z = 0; z < n; ++z) {
+            const double e = __ldg(ek + (size_t)z * n);
+            const double2 *xr = reinterpret_cast<const double2 *>(xs + z * LD);
+#pragma unroll
+            for (int c = 0; c < HC / 2; ++c) {
+                double2 xv = xr[c];
+                acc[2 * c] = fma(e, xv.x, acc[2 * c]);
+                acc[2 * c + 1] = fma(e, xv.y, acc[2 * c + 1]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < HC; ++c) Ys[k * LD + h * HC + c] = acc[c];
+    }
+    __syncthreads();
+
+    // Sherman-Morrison scalar of each row.
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int r = warp; r < TR; r += (blockDim.x >> 5)) {
+        double sr = 0.0, si = 0.0;
+        double pk = 0.0;
+        if (r < nrow) {
+            pk = row_pkd[row0 + r];
+            for (int k = lane; k < n; k += 32) {
+                const double w = en[k] / (pk + lam[k]);
+                sr = fma(w, Ys[k * LD + 2 * r], sr);
+                si = fma(w, Ys[k * LD + 2 * r + 1], si);
+            }
+        }
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (lane == 0) {
+            double2 b = make_double2(0.0, 0.0);
+            if (r < nrow) {
+                const double2 c = row_c[row0 + r];
+                const double fn = row_fn[row0 + r];
+                const double2 cs = cmul(c, make_double2(sr, si));
+                const double2 den = make_double2(1.0 - c.x * fn, -c.y * fn);
+                b = cdiv(cs, den);
+            }
+            beta_s[r] = b;
+        }
+    }
+    __syncthreads();
+
+    for (int idx = threadIdx.x; idx < n * TR; idx += blockDim.x) {
+        const int k = idx / TR, r = idx - k * TR;
+        double inv = 0.0;
+        if (r < nrow) inv = 1.0 / (row_pkd[row0 + r] + lam[k]);
+        const double2 b = beta_s[r];
+        const double ek = en[k];
+        double *y = Ys + k * LD + 2 * r;
+        y[0] = (y[0] + b.x * ek) * inv;
+        y[1] = (y[1] + b.y * ek) * inv;
+    }
+    __syncthreads();
+
+    // GEMM 2: out[z][c] = sum_k ET[k][z] Ys[k][c]
+    for (int item = threadIdx.x; item < 2 * n; item += blockDim.x) {
+        const int z = item >> 1, h = item & 1;
+        double acc[HC];
+#pragma unroll
+        for (int c = 0; c < HC; ++c) acc[c] = 0.0;
+        const double *ys = Ys + h * HC;
+        const double *ez = ET + z;
+#pragma unroll 4
+        for (int k = 0; k < n; ++k) {
+            const double e = __ldg(ez + (size_t)k * n);
+            const double2 *yr = reinterpret_cast<const double2 *>(ys + k * LD);
+#pragma unroll
+            for (int c = 0; c < HC / 2; ++c) {
+                double2 yv = yr[c];
+                acc[2 * c] = fma(e, yv.x, acc[2 * c]);
+                acc[2 * c + 1] = fma(e, yv.y, acc[2 * c + 1]);
+            }
+        }
+#pragma unroll
+        for (int rr = 0; rr < HC / 2; ++rr) {
+            const int r = h * (HC / 2) + rr;
+            if (r < nrow) {
+                double2 *o = out + (size_t)(row0 + r) * n + z;
+                double2 v = make_double2(acc[2 * rr], acc[2 * rr + 1]);
+                if (accumulate) v = cadd(*o, v);
+                *o = v;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Residual diagonal part:  out = b - D x  on every row of a tile.
+//   D x = T x + (Re V00 + pkd) x - c x(z_n) e_n ; b = b_spec e_n on the
+// specular row.  One FP64 GEMM with the symmetric T.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_residual_diag(Tiles tiles, const int *__restrict__ gate, int n,
+                const double *__restrict__ Tm, const double *__restrict__ v00,
+                const double *__restrict__ row_pkd, const double2 *__restrict__ row_c,
+                const int *__restrict__ sys_spec_row, const double2 *__restrict__ sys_bspec,
+                const double2 *__restrict__ x, double2 *__restrict__ out, int with_b)
+{
+    constexpr int TR = kTileRows;
+    constexpr int LD = 2 * TR;
+    constexpr int HC = TR;
+    extern __shared__ double smem[];
+    double *Xs = smem;  // [n][LD]
+
+    const int tile = blockIdx.x;
+    const int sys = tiles.sys[tile];
+    if (gate && gate[sys] == 0) return;
+    const int row0 = tiles.row0[tile];
+    const int nrow = tiles.nrow[tile];
+    const int spec_row = sys_spec_row[sys];
+    const double2 bspec = sys_bspec[sys];
+
+    for (int idx = threadIdx.x; idx < TR * n; idx += blockDim.x) {
+        int r = idx / n, z = idx - r * n;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < nrow) v = x[(size_t)(row0 + r) * n + z];
+        Xs[z * LD + 2 * r] = v.x;
+        Xs[z * LD + 2 * r + 1] = v.y;
+    }
+    __syncthreads();
+
+    for (int item = threadIdx.x; item < 2 * n; item += blockDim.x) {
+        const int z = item >> 1, h = item & 1;
+        double acc[HC];
+#pragma unroll
+        for (int c = 0; c < HC; ++c) acc[c] = 0.0;
+        const double *xs = Xs + h * HC;
+        const double *tz = Tm + z;
+#pragma unroll 4
+        for (int k = 0; k < n; ++k) {
+            const double t = __ldg(tz + (size_t)k * n);
+            const double2 *xr = reinterpret_cast<const double2 *>(xs + k * LD);
+#pragma unroll
+            for (int c = 0; c < HC / 2; ++c) {
+                double2 xv = xr[c];
+                acc[2 * c] = fma(t, xv.x, acc[2 * c]);
+                acc[2 * c + 1] = fma(t, xv.y, acc[2 * c + 1]);
+            }
+        }
+        const double vz = v00[z];
+#pragma unroll
+        for (int rr = 0; rr < HC / 2; ++rr) {
+            const int r = h * (HC / 2) + rr;
+            if (r < nrow) {
+                const int row = row0 + r;
+                const double diag = vz + row_pkd[row];
+                double2 xz = make_double2(Xs[z * LD + 2 * r], Xs[z * LD + 2 * r + 1]);
+                double2 d = make_double2(acc[2 * rr] + diag * xz.x, acc[2 * rr + 1] + diag * xz.y);
+                if (z == n - 1) d = csub(d, cmul(row_c[row], xz));
+                double2 o = make_double2(-d.x, -d.y);
+                if (with_b && row == spec_row && z == n - 1) o = cadd(o, bspec);
+                out[(size_t)row * n + z] = o;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Channel coupling:  out = in0 + sgn * sum_t V_t(z) src[nbr[row][t]](z)
+// The coupling sum is the reference's apply_upper_block + the coupling half
+// of solve_lower_block (multiscat_gmres.f90:620-660) restricted to nonzero
+// taps: a circular 2-D convolution over the channel torus at every z.
+// Grid: (tiles, z-chunks of 32); block (32 z, kTileRows rows).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_coupling(Tiles tiles, const int *__restrict__ gate, int n, int K,
+           const double2 *__restrict__ Vt, const int *__restrict__ nbr,
+           const double2 *__restrict__ src, const double2 *__restrict__ in0, double sgn,
+           double2 *__restrict__ out)
+{
+    extern __shared__ int nb_s[];   // [kTileRows][K]
+    const int tile = blockIdx.x;
+    const int sys = tiles.sys[tile];
+    if (gate && gate[sys] == 0) return;
+    const int row0 = tiles.row0[tile];
+    const int nrow = tiles.nrow[tile];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int i = tid; i < nrow * K; i += blockDim.x * blockDim.y)
+        nb_s[i] = nbr[(size_t)row0 * K + i];
+    __syncthreads();
+    const int r = threadIdx.y;
+    const int z = blockIdx.y * blockDim.x + threadIdx.x;
+    if (r >= nrow || z >= n) return;
+    const int *nb = nb_s + r * K;
+    double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
+    int t = 0;
+    for (; t + 1 < K; t += 2) {
+        const int j0 = nb[t], j1 = nb[t + 1];
+        const double2 v0 = __ldg(Vt + (size_t)t * n + z);
+        const double2 v1 = __ldg(Vt + (size_t)(t + 1) * n + z);
+        if (j0 >= 0) {
+            const double2 s0 = src[(size_t)j0 * n + z];
+            ar = fma(v0.x, s0.x, ar); ar = fma(-v0.y, s0.y, ar);
+            ai = fma(v0.x, s0.y, ai); ai = fma(v0.y, s0.x, ai);
+        }
+        if (j1 >= 0) {
+            const double2 s1 = src[(size_t)j1 * n + z];
+            br = fma(v1.x, s1.x, br); br = fma(-v1.y, s1.y, br);
+            bi = fma(v1.x, s1.y, bi); bi = fma(v1.y, s1.x, bi);
+        }
+    }
+    if (t < K) {
+        const int j0 = nb[t];
+        const double2 v0 = __ldg(Vt + (size_t)t * n + z);
+        if (j0 >= 0) {
+            const double2 s0 = src[(size_t)j0 * n + z];
+            ar = fma(v0.x, s0.x, ar); ar = fma(-v0.y, s0.y, ar);
+            ai = fma(v0.x, s0.y, ai); ai = fma(v0.y, s0.x, ai);
+        }
+    }
+    const size_t o = (size_t)(row0 + r) * n + z;
+    double2 base = in0 ? in0[o] : make_double2(0.0, 0.0);
+    out[o] = make_double2(base.x + sgn * (ar + br), base.y + sgn * (ai + bi));
+}
+
+// ---------------------------------------------------------------------------
+// Arnoldi reductions.  partial[tile][i] = sum conj(Q_i) W over the tile for
+// i < nvec; slot nvec holds ||W||^2 when with_norm.  One warp per vector.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_dots(Tiles tiles, const int *__restrict__ gate, int n, const double2 *__restrict__ Q,
+       size_t qstride, int nvec, const double2 *__restrict__ W, int with_norm,
+       double2 *__restrict__ partial, int pstride)
+{
+    const int tile = blockIdx.x;
+    const int sys = tiles.sys[tile];
+    if (gate && gate[sys] == 0) return;
+    const size_t e0 = (size_t)tiles.row0[tile] * n;
+    const int ne = tiles.nrow[tile] * n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntask = nvec + (with_norm ? 1 : 0);
+    for (int task = warp; task < ntask; task += (blockDim.x >> 5)) {
+        double sr = 0.0, si = 0.0;
+        if (task < nvec) {
+            const double2 *q = Q + (size_t)task * qstride + e0;
+            const double2 *w = W + e0;
+            for (int e = lane; e < ne; e += 32) {
+                const double2 a = q[e], b = w[e];
+                sr = fma(a.x, b.x, sr); sr = fma(a.y, b.y, sr);
+                si = fma(a.x, b.y, si); si = fma(-a.y, b.x, si);
+            }
+        } else {
+            const double2 *w = W + e0;
+            for (int e = lane; e < ne; e += 32) {
+                const double2 b = w[e];
+                sr = fma(b.x, b.x, sr); sr = fma(b.y, b.y, sr);
+            }
+        }
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (lane == 0) partial[(size_t)tile * pstride + task] = make_double2(sr, si);
+    }
+}
+
+// out[s][i] = sum over the tiles of system s of partial[tile][i], i < nslot.
+__global__ void __launch_bounds__(256)
+k_reduce_partials(const int *__restrict__ sys_tile0, int nsys, const int *__restrict__ gate,
+                  const double2 *__restrict__ partial, int pstride, int nslot,
+                  double2 *__restrict__ out, int ostride)
+{
+    const int s = blockIdx.x;
+    if (s >= nsys) return;
+    if (gate && gate[s] == 0) return;
+    const int t0 = sys_tile0[s], t1 = sys_tile0[s + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = warp; i < nslot; i += (blockDim.x >> 5)) {
+        double sr = 0.0, si = 0.0;
+        for (int t = t0 + lane; t < t1; t += 32) {
+            const double2 p = partial[(size_t)t * pstride + i];
+            sr += p.x;
+            si += p.y;
+        }
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (lane == 0) out[(size_t)s * ostride + i] = make_double2(sr, si);
+    }
+}
+
+// dst = (W - sum_{i<nvec} Q_i coef[s][i]) * (scale ? scale[s] : 1)
+// (dst may alias W).  Grid: (tiles, chunks); 256 threads.
+__global__ void __launch_bounds__(256)
+k_update(Tiles tiles, const int *__restrict__ gate, int n, const double2 *__restrict__ Q,
+         size_t qstride, int nvec, const int *__restrict__ nvec_sys,
+         const double2 *__restrict__ coef, int cstride, const double2 *W,
+         const double *__restrict__ scale, double2 *dst, int negate_sum_only)
+{
+    __shared__ double2 cf[kMaxRestart + 1];
+    const int tile = blockIdx.x;
+    const int sys = tiles.sys[tile];
+    if (gate && gate[sys] == 0) return;
+    int nv = nvec_sys ? nvec_sys[sys] : nvec;
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) cf[i] = coef[(size_t)sys * cstride + i];
+    __syncthreads();
+    const size_t e0 = (size_t)tiles.row0[tile] * n;
+    const int ne = tiles.nrow[tile] * n;
+    const double sc = scale ? scale[sys] : 1.0;
+    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < ne; e += gridDim.y * blockDim.x) {
+        double2 acc = (W && !negate_sum_only) ? W[e0 + e] : make_double2(0.0, 0.0);
+        for (int i = 0; i < nv; ++i) {
+            const double2 q = Q[(size_t)i * qstride + e0 + e];
+            const double2 c = cf[i];
+            if (negate_sum_only) {
+                acc.x = fma(q.x, c.x, acc.x); acc.x = fma(-q.y, c.y, acc.x);
+                acc.y = fma(q.x, c.y, acc.y); acc.y = fma(q.y, c.x, acc.y);
+            } else {
+                acc.x = fma(-q.x, c.x, acc.x); acc.x = fma(q.y, c.y, acc.x);
+                acc.y = fma(-q.x, c.y, acc.y); acc.y = fma(-q.y, c.x, acc.y);
+            }
+        }
+        dst[e0 + e] = make_double2(acc.x * sc, acc.y * sc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-system GMRES control (one thread per system; the work is O(m)).
+// ---------------------------------------------------------------------------
+struct GmresState {
+    double2 *H;       // [B][(m+1)*m]  column j at j*(m+1)
+    double2 *cs;      // [B][m]  Givens c (real stored in .x)
+    double2 *sn;      // [B][m]  Givens s
+    double2 *g;       // [B][m+1]
+    double2 *h1;      // [B][m+2]  first-pass projections
+    double2 *h2;      // [B][m+2]  second-pass projections (+ norm^2 slot)
+    double2 *y;       // [B][m]
+    double *scale;    // [B]  1/beta for the next basis vector
+    double *bnorm;    // [B]  ||b||
+    double *resid;    // [B]  last true relative residual
+    double *est;      // [B]  GMRES residual estimate (absolute)
+    int *active;      // [B]  iterating in this cycle
+    int *kcyc;        // [B]  iterations done in this cycle
+    int *iters;       // [B]  total iterations
+    int *cycles;      // [B]  restart cycles started
+    int *unfinished;  // [B]  1 until converged or failed
+    int *status;      // [B]  msc_status
+    int *counter;     // [1]  systems still unfinished (host reads it)
+};
+
+// Cycle start: norm of r = b - A x from the reduced partials (slot 0).
+__global__ void k_cycle_start(GmresState st, int nsys, int m, const double2 *__restrict__ nrm,
+                              int nstride, double rtol, int max_iter)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    st.active[s] = 0;
+    st.kcyc[s] = 0;
+    if (!st.unfinished[s]) return;
+    const double beta = sqrt(fmax(nrm[(size_t)s * nstride].x, 0.0));
+    const double rel = beta / st.bnorm[s];
+    st.resid[s] = rel;
+    if (!isfinite(beta)) {
+        st.unfinished[s] = 0;
+        st.status[s] = 4;
+        return;
+    }
+    if (rel <= rtol) {
+        st.unfinished[s] = 0;
+        st.status[s] = 0;
+        return;
+    }
+    if (st.iters[s] >= max_iter) {
+        st.unfinished[s] = 0;
+        st.status[s] = 2;
+        return;
+    }
+    st.active[s] = 1;
+    st.cycles[s] += 1;
+    double2 *g = st.g + (size_t)s * (m + 1);
+    g[0] = make_double2(beta, 0.0);
+    for (int i = 1; i <= m; ++i) g[i] = make_double2(0.0, 0.0);
+    st.scale[s] = 1.0 / beta;
+    atomicAdd(st.counter, 1);
+}
+
+// Arnoldi step j: combine the two CGS passes, append column j of H, apply
+// the previous Givens rotations, make rotation j, update g.
+__global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rtol, int max_iter)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys || !st.active[s]) return;
+    const int hs = m + 2;
+    const double2 *h1 = st.h1 + (size_t)s * hs;
+    const double2 *h2 = st.h2 + (size_t)s * hs;
+    double2 *H = st.H + (size_t)s * (m + 1) * m + (size_t)j * (m + 1);
+    double2 *cs = st.cs + (size_t)s * m;
+    double2 *sn = st.sn + (size_t)s * m;
+    double2 *g = st.g + (size_t)s * (m + 1);
+    double proj2 = 0.0;
+    for (int i = 0; i <= j; ++i) {
+        H[i] = cadd(h1[i], h2[i]);
+        proj2 += cabs2(h2[i]);
+    }
+    const double w2 = h2[j + 1].x;          // ||W'||^2 after the first pass
+    const double beta = sqrt(fmax(w2 - proj2, 0.0));
+    // previous rotations
+    for (int i = 0; i < j; ++i) {
+        const double c = cs[i].x;
+        const double2 sv = sn[i];
+        const double2 a = H[i], b = H[i + 1];
+        // [c, s; -conj(s), c] [a; b]
+        H[i] = cadd(cscale(a, c), cmul(sv, b));
+        H[i + 1] = csub(cscale(b, c), cmul(cconj(sv), a));
+    }
+    // new rotation from (H[j], beta)
+    const double2 a = H[j];
+    const double aa = sqrt(cabs2(a));
+    const double r = hypot(aa, beta);
+    double c;
+    double2 sv;
+    if (r == 0.0) {
+        c = 1.0;
+        sv = make_double2(0.0, 0.0);
+    } else if (aa == 0.0) {
+        c = 0.0;
+        sv = make_double2(1.0, 0.0);
+    } else {
+        c = aa / r;
+        sv = cscale(cscale(a, 1.0 / aa), beta / r);   // (a/|a|) * conj(beta) / r, beta real
+    }
+    cs[j] = make_double2(c, 0.0);
+    sn[j] = sv;
+    H[j] = (aa == 0.0) ? make_double2(beta, 0.0) : cscale(a, r / aa);
+    H[j + 1] = make_double2(0.0, 0.0);
+    const double2 gj = g[j];
+    g[j] = cscale(gj, c);
+    g[j + 1] = make_double2(-(sv.x * gj.x + sv.y * gj.y), -(sv.x * gj.y - sv.y * gj.x));  // -conj(s) g_j
+    const double est = sqrt(cabs2(g[j + 1]));
+    st.est[s] = est;
+    st.kcyc[s] = j + 1;
+    st.iters[s] += 1;
+    st.scale[s] = (beta > 0.0) ? 1.0 / beta : 0.0;
+    bool stop = false;
+    if (!isfinite(est) || !isfinite(beta)) stop = true;
+    if (est <= rtol * st.bnorm[s]) stop = true;
+    if (j + 1 >= m) stop = true;
+    if (st.iters[s] >= max_iter) stop = true;
+    if (beta <= 1e-300) stop = true;
+    if (stop) st.active[s] = 0;
+}
+
+// y = R^-1 g over the kcyc columns of this cycle.
+__global__ void k_trisolve(GmresState st, int nsys, int m)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    const int k = st.kcyc[s];
+    if (k == 0) return;
+    const double2 *H = st.H + (size_t)s * (m + 1) * m;
+    const double2 *g = st.g + (size_t)s * (m + 1);
+    double2 *y = st.y + (size_t)s * m;
+    for (int i = k - 1; i >= 0; --i) {
+        double2 acc = g[i];
+        for (int l = i + 1; l < k; ++l) acc = csub(acc, cmul(H[(size_t)l * (m + 1) + i], y[l]));
+        y[i] = cdiv(acc, H[(size_t)i * (m + 1) + i]);
+    }
+}
+
+// I_G = |2i b_G psi_G(z_n) + delta_{G,spec} a_spec|^2
+__global__ void k_intensities(int nrows, int row_offset, int n, const int *__restrict__ row_sys,
+                              const int *__restrict__ sys_spec_row,
+                              const double2 *__restrict__ sys_aspec,
+                              const double2 *__restrict__ row_b, const double2 *__restrict__ psi,
+                              double *__restrict__ out)
+{
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= nrows) return;
+    const int s = row_sys[row];
+    const double2 p = psi[(size_t)row * n + (n - 1)];
+    const double2 b = row_b[row];
+    double2 amp = cmul(make_double2(0.0, 2.0), cmul(b, p));
+    if (row + row_offset == sys_spec_row[s]) amp = cadd(amp, sys_aspec[s]);
+    out[row] = cabs2(amp);
+}
+
+__global__ void k_scale(double2 *p, size_t count, double sc)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
+         i += (size_t)gridDim.x * blockDim.x)
+        p[i] = make_double2(p[i].x * sc, p[i].y * sc);
+}
+
+__global__ void k_fill_zero(double2 *p, size_t count)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
+         i += (size_t)gridDim.x * blockDim.x)
+        p[i] = make_double2(0.0, 0.0);
+}
+
+}  // namespace msc

@@ -1,0 +1,838 @@
+// msc_solver.cu -- plan, restarted GMRES orchestration and the C-ABI.
+//
+// One plan = one potential (z grid, coupling torus) + a batch of beams
+// (systems).  The solve is right-preconditioned restarted GMRES(m):
+//     A M y = b,  psi = M y,  M = D^-1 (block-diagonal, per channel)
+// in FP64.  Each restart cycle recomputes the true residual b - A psi, so
+// the stop rule ||b - A psi|| <= rtol ||b|| is checked on the real operator.
+// The reference solves the same A psi = b with block Gauss-Seidel left
+// preconditioning and unrestarted MGS GMRES
+// (multiscat_gmres.f90:452-618); the converged psi is the same.
+//
+// Execution: one CUDA graph per restart cycle start (true residual + norm)
+// and one for the m Arnoldi steps + solution update.  Per-system activity
+// flags live on the device, so systems that converge early stop doing work
+// while the rest of the batch carries on.  The host reads one counter per
+// cycle.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/multiscat_b200.h"
+#include "msc_common.cuh"
+#include "msc_eigh.hpp"
+#include "msc_kernels_fp64.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+msc_status fail(msc_status st, const std::string &msg)
+{
+    g_last_error = msg;
+    return st;
+}
+
+#define MSC_CUDA(call)                                                                  \
+    do {                                                                                \
+        cudaError_t _e = (call);                                                        \
+        if (_e != cudaSuccess) {                                                        \
+            return fail(MSC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+        }                                                                               \
+    } while (0)
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t count = 0;
+    cudaError_t alloc(size_t c)
+    {
+        release();
+        count = c;
+        if (c == 0) return cudaSuccess;
+        return cudaMalloc(&p, c * sizeof(T));
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        count = 0;
+    }
+};
+
+struct SystemHost {
+    int C = 0;
+    int spec = 0;
+    std::vector<int> ix, iy;
+    std::vector<double> pkd;
+    std::vector<double2> b, c;
+    double2 a_spec{0.0, 0.0};
+    bool set = false;
+};
+
+}  // namespace
+
+struct msc_plan {
+    msc_plan_desc desc{};
+    int n = 0, nkx = 0, nky = 0, B = 0, m = 30;
+    bool potential_set = false;
+    bool finalized = false;
+    // potential
+    std::vector<double> T_host, v00_host, lam_host, E_host, en_host;
+    std::vector<std::pair<int, int>> taps;     // (dx, dy) storage offsets
+    std::vector<double2> Vt_host;              // [K][n]
+    int K = 0;
+    std::vector<SystemHost> sys;
+    // rows / tiles
+    int R = 0, ntiles = 0;
+    std::vector<int> tile_row0_h, tile_nrow_h, tile_sys_h, sys_tile0_h, sys_row0_h, row_sys_h;
+    // device data
+    DevBuf<double> E, ET, Tm, lam, en, v00, row_pkd, row_fn;
+    DevBuf<double2> Vt, row_c, row_b, sys_bspec, sys_aspec;
+    DevBuf<int> nbr, tile_row0, tile_nrow, tile_sys, sys_tile0, sys_spec_row, row_sys;
+    // solver state
+    DevBuf<double2> X, W, U, TMP, Q, partial;
+    DevBuf<double2> H, cs, sn, g, h1, h2, y;
+    DevBuf<double> scale, bnorm, resid, est;
+    DevBuf<int> active, kcyc, iters, cycles, unfinished, status, counter;
+    int *counter_host = nullptr;   // pinned
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t g_start = nullptr, g_iter = nullptr;
+    int pstride = 0;
+    // measurement
+    bool timing = false;
+    std::vector<cudaEvent_t> tev;        // [2 kinds][m + 1 slots][start, stop]
+    double t_ms[2] = {0.0, 0.0};
+    int64_t t_launches[2] = {0, 0};
+    int *kcyc_host = nullptr;            // pinned [B]
+    int64_t launches_last = 0;
+    int cycles_last = 0;
+    int64_t launches_start = 0, launches_iter = 0;   // kernel nodes per graph
+
+    ~msc_plan()
+    {
+        if (g_start) cudaGraphExecDestroy(g_start);
+        if (g_iter) cudaGraphExecDestroy(g_iter);
+        if (counter_host) cudaFreeHost(counter_host);
+        if (kcyc_host) cudaFreeHost(kcyc_host);
+        for (cudaEvent_t e : tev) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+        E.release(); ET.release(); Tm.release(); lam.release(); en.release(); v00.release();
+        row_pkd.release(); row_fn.release(); Vt.release(); row_c.release(); row_b.release();
+        sys_bspec.release(); sys_aspec.release(); nbr.release(); tile_row0.release();
+        tile_nrow.release(); tile_sys.release(); sys_tile0.release(); sys_spec_row.release();
+        row_sys.release(); X.release(); W.release(); U.release(); TMP.release(); Q.release();
+        partial.release(); H.release(); cs.release(); sn.release(); g.release(); h1.release();
+        h2.release(); y.release(); scale.release(); bnorm.release(); resid.release();
+        est.release(); active.release(); kcyc.release(); iters.release(); cycles.release();
+        unfinished.release(); status.release(); counter.release();
+    }
+
+    msc::Tiles tiles() const
+    {
+        return msc::Tiles{tile_row0.p, tile_nrow.p, tile_sys.p, ntiles};
+    }
+    msc::GmresState state() const
+    {
+        msc::GmresState s;
+        s.H = H.p; s.cs = cs.p; s.sn = sn.p; s.g = g.p; s.h1 = h1.p; s.h2 = h2.p; s.y = y.p;
+        s.scale = scale.p; s.bnorm = bnorm.p; s.resid = resid.p; s.est = est.p;
+        s.active = active.p; s.kcyc = kcyc.p; s.iters = iters.p; s.cycles = cycles.p;
+        s.unfinished = unfinished.p; s.status = status.p; s.counter = counter.p;
+        return s;
+    }
+};
+
+namespace {
+
+template <typename T>
+cudaError_t upload(DevBuf<T> &buf, const std::vector<T> &h)
+{
+    cudaError_t e = buf.alloc(h.size());
+    if (e != cudaSuccess) return e;
+    if (h.empty()) return cudaSuccess;
+    return cudaMemcpy(buf.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+size_t smem_block_inverse(int n) { return (size_t)2 * n * 2 * msc::kTileRows * sizeof(double); }
+size_t smem_residual(int n) { return (size_t)n * 2 * msc::kTileRows * sizeof(double); }
+size_t smem_coupling(int K) { return (size_t)msc::kTileRows * K * sizeof(int); }
+
+// --- kernel launch wrappers (all on plan->stream) ---------------------------
+
+void launch_block_inverse(msc_plan *p, const int *gate, const double2 *x, double2 *out, int acc,
+                          cudaStream_t st)
+{
+    msc::k_block_inverse<<<p->ntiles, 256, smem_block_inverse(p->n), st>>>(
+        p->tiles(), gate, p->n, p->E.p, p->ET.p, p->lam.p, p->en.p, p->row_pkd.p, p->row_c.p,
+        p->row_fn.p, x, out, acc);
+}
+
+void launch_residual_diag(msc_plan *p, const int *gate, const double2 *x, double2 *out, int with_b,
+                          cudaStream_t st)
+{
+    msc::k_residual_diag<<<p->ntiles, 256, smem_residual(p->n), st>>>(
+        p->tiles(), gate, p->n, p->Tm.p, p->v00.p, p->row_pkd.p, p->row_c.p, p->sys_spec_row.p,
+        p->sys_bspec.p, x, out, with_b);
+}
+
+void launch_coupling(msc_plan *p, const int *gate, const double2 *src, const double2 *in0,
+                     double sgn, double2 *out, cudaStream_t st)
+{
+    dim3 grid(p->ntiles, (p->n + 31) / 32);
+    dim3 block(32, msc::kTileRows);
+    msc::k_coupling<<<grid, block, smem_coupling(std::max(p->K, 1)), st>>>(
+        p->tiles(), gate, p->n, p->K, p->Vt.p, p->nbr.p, src, in0, sgn, out);
+}
+
+void launch_dots(msc_plan *p, const int *gate, int nvec, const double2 *W, int with_norm,
+                 cudaStream_t st)
+{
+    msc::k_dots<<<p->ntiles, 256, 0, st>>>(p->tiles(), gate, p->n, p->Q.p,
+                                            (size_t)p->R * p->n, nvec, W, with_norm,
+                                            p->partial.p, p->pstride);
+}
+
+void launch_reduce(msc_plan *p, const int *gate, int nslot, double2 *out, cudaStream_t st)
+{
+    msc::k_reduce_partials<<<p->B, 256, 0, st>>>(p->sys_tile0.p, p->B, gate, p->partial.p,
+                                                  p->pstride, nslot, out, p->m + 2);
+}
+
+void launch_update(msc_plan *p, const int *gate, int nvec, const int *nvec_sys,
+                   const double2 *coef, int cstride, const double2 *W, const double *scale,
+                   double2 *dst, int sum_only, cudaStream_t st)
+{
+    int chunks = (msc::kTileRows * p->n + 255) / 256;
+    dim3 grid(p->ntiles, chunks);
+    msc::k_update<<<grid, 256, 0, st>>>(p->tiles(), gate, p->n, p->Q.p, (size_t)p->R * p->n,
+                                         nvec, nvec_sys, coef, cstride, W, scale, dst, sum_only);
+}
+
+int sys_blocks(int B) { return (B + 127) / 128; }
+
+// Cycle start: r = b - A x into Q0, its norm, activation, Q0 /= ||r||.
+void record_cycle_start(msc_plan *p, cudaStream_t st)
+{
+    double2 *Q0 = p->Q.p;
+    cudaMemsetAsync(p->counter.p, 0, sizeof(int), st);
+    launch_residual_diag(p, p->unfinished.p, p->X.p, p->TMP.p, 1, st);
+    launch_coupling(p, p->unfinished.p, p->X.p, p->TMP.p, -1.0, Q0, st);
+    launch_dots(p, p->unfinished.p, 0, Q0, 1, st);
+    launch_reduce(p, p->unfinished.p, 1, p->h2.p, st);
+    msc::k_cycle_start<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m, p->h2.p,
+                                                         p->m + 2, p->desc.rtol,
+                                                         p->desc.max_iterations);
+    launch_update(p, p->active.p, 0, nullptr, p->h1.p, p->m + 2, Q0, p->scale.p, Q0, 0, st);
+    cudaMemcpyAsync(p->counter_host, p->counter.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+}
+
+cudaEvent_t tev_at(msc_plan *p, int kind, int slot, int which)
+{
+    return p->tev[((size_t)kind * (p->m + 1) + slot) * 2 + which];
+}
+
+// m Arnoldi steps (CGS2) and the solution update x += M (Q y).
+void record_cycle_iterations(msc_plan *p, cudaStream_t st)
+{
+    const size_t vs = (size_t)p->R * p->n;
+    const bool tm = p->timing;
+    for (int j = 0; j < p->m; ++j) {
+        double2 *Qj = p->Q.p + (size_t)j * vs;
+        double2 *Qn = p->Q.p + (size_t)(j + 1) * vs;
+        if (tm) cudaEventRecord(tev_at(p, 0, j, 0), st);
+        launch_block_inverse(p, p->active.p, Qj, p->U.p, 0, st);
+        if (tm) cudaEventRecord(tev_at(p, 0, j, 1), st);
+        if (tm) cudaEventRecord(tev_at(p, 1, j, 0), st);
+        launch_coupling(p, p->active.p, p->U.p, Qj, 1.0, p->W.p, st);
+        if (tm) cudaEventRecord(tev_at(p, 1, j, 1), st);
+        launch_dots(p, p->active.p, j + 1, p->W.p, 0, st);
+        launch_reduce(p, p->active.p, j + 1, p->h1.p, st);
+        launch_update(p, p->active.p, j + 1, nullptr, p->h1.p, p->m + 2, p->W.p, nullptr, p->W.p,
+                      0, st);
+        launch_dots(p, p->active.p, j + 1, p->W.p, 1, st);
+        launch_reduce(p, p->active.p, j + 2, p->h2.p, st);
+        msc::k_arnoldi_step<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m, j,
+                                                              p->desc.rtol,
+                                                              p->desc.max_iterations);
+        launch_update(p, p->active.p, j + 1, nullptr, p->h2.p, p->m + 2, p->W.p, p->scale.p, Qn,
+                      0, st);
+    }
+    msc::k_trisolve<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m);
+    launch_update(p, p->kcyc.p, 0, p->kcyc.p, p->y.p, p->m, nullptr, nullptr, p->U.p, 1, st);
+    if (tm) cudaEventRecord(tev_at(p, 0, p->m, 0), st);
+    launch_block_inverse(p, p->kcyc.p, p->U.p, p->X.p, 1, st);
+    if (tm) cudaEventRecord(tev_at(p, 0, p->m, 1), st);
+    cudaMemcpyAsync(p->kcyc_host, p->kcyc.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, st);
+}
+
+// Kernel nodes in a captured graph (launch accounting).
+int64_t count_kernel_nodes(cudaGraph_t g)
+{
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+    int64_t k = 0;
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    }
+    return k;
+}
+
+// Add the device time of the timed launches of the last iteration graph.
+void accumulate_timing(msc_plan *p)
+{
+    int maxk = 0;
+    for (int s = 0; s < p->B; ++s) maxk = std::max(maxk, p->kcyc_host[s]);
+    if (maxk == 0) return;
+    for (int kind = 0; kind < 2; ++kind) {
+        for (int j = 0; j < maxk; ++j) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, tev_at(p, kind, j, 0), tev_at(p, kind, j, 1)) == cudaSuccess) {
+                p->t_ms[kind] += ms;
+                p->t_launches[kind] += 1;
+            }
+        }
+    }
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, tev_at(p, 0, p->m, 0), tev_at(p, 0, p->m, 1)) == cudaSuccess) {
+        p->t_ms[0] += ms;
+        p->t_launches[0] += 1;
+    }
+}
+
+msc_status capture(msc_plan *p, void (*rec)(msc_plan *, cudaStream_t), cudaGraphExec_t *out,
+                   int64_t *kernel_nodes)
+{
+    cudaGraph_t graph = nullptr;
+    if (*out) {
+        cudaGraphExecDestroy(*out);
+        *out = nullptr;
+    }
+    MSC_CUDA(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    rec(p, p->stream);
+    cudaError_t e = cudaStreamEndCapture(p->stream, &graph);
+    if (e != cudaSuccess) return fail(MSC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    if (kernel_nodes) *kernel_nodes = count_kernel_nodes(graph);
+    e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(MSC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return MSC_OK;
+}
+
+msc_status set_kernel_attributes(int n, int K)
+{
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_block_inverse(msc::kMaxNz)));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_residual_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_residual(msc::kMaxNz)));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_coupling(msc::kMaxTaps)));
+    (void)n;
+    (void)K;
+    return MSC_OK;
+}
+
+// Build rows, tiles, neighbour tables; upload everything; allocate state.
+msc_status finalize(msc_plan *p)
+{
+    if (p->finalized) return MSC_OK;
+    if (!p->potential_set) return fail(MSC_ERR_ARG, "potential not set");
+    for (int s = 0; s < p->B; ++s)
+        if (!p->sys[s].set) return fail(MSC_ERR_ARG, "system " + std::to_string(s) + " not set");
+    const int n = p->n;
+    // rows and tiles
+    p->R = 0;
+    p->sys_row0_h.assign(p->B + 1, 0);
+    p->sys_tile0_h.assign(p->B + 1, 0);
+    p->tile_row0_h.clear(); p->tile_nrow_h.clear(); p->tile_sys_h.clear(); p->row_sys_h.clear();
+    for (int s = 0; s < p->B; ++s) {
+        p->sys_row0_h[s] = p->R;
+        p->sys_tile0_h[s] = (int)p->tile_row0_h.size();
+        const int C = p->sys[s].C;
+        for (int r = 0; r < C; r += msc::kTileRows) {
+            p->tile_row0_h.push_back(p->R + r);
+            p->tile_nrow_h.push_back(std::min(msc::kTileRows, C - r));
+            p->tile_sys_h.push_back(s);
+        }
+        for (int r = 0; r < C; ++r) p->row_sys_h.push_back(s);
+        p->R += C;
+    }
+    p->sys_row0_h[p->B] = p->R;
+    p->sys_tile0_h[p->B] = (int)p->tile_row0_h.size();
+    p->ntiles = (int)p->tile_row0_h.size();
+    // per-row data and neighbour table
+    std::vector<double> pkd(p->R), fn(p->R);
+    std::vector<double2> rc(p->R), rb(p->R), bspec(p->B), aspec(p->B);
+    std::vector<int> spec_row(p->B), nbr((size_t)p->R * std::max(p->K, 1), -1);
+    std::vector<int> lookup((size_t)p->nkx * p->nky);
+    for (int s = 0; s < p->B; ++s) {
+        const SystemHost &sh = p->sys[s];
+        const int r0 = p->sys_row0_h[s];
+        std::fill(lookup.begin(), lookup.end(), -1);
+        for (int j = 0; j < sh.C; ++j) lookup[(size_t)sh.ix[j] * p->nky + sh.iy[j]] = r0 + j;
+        for (int j = 0; j < sh.C; ++j) {
+            const int row = r0 + j;
+            pkd[row] = sh.pkd[j];
+            rc[row] = sh.c[j];
+            rb[row] = sh.b[j];
+            double f = 0.0;
+            for (int k = 0; k < n; ++k) f += p->en_host[k] * p->en_host[k] / (sh.pkd[j] + p->lam_host[k]);
+            fn[row] = f;
+            for (int t = 0; t < p->K; ++t) {
+                const int sx = ((sh.ix[j] - p->taps[t].first) % p->nkx + p->nkx) % p->nkx;
+                const int sy = ((sh.iy[j] - p->taps[t].second) % p->nky + p->nky) % p->nky;
+                nbr[(size_t)row * p->K + t] = lookup[(size_t)sx * p->nky + sy];
+            }
+        }
+        spec_row[s] = r0 + sh.spec;
+        bspec[s] = sh.b[sh.spec];
+        aspec[s] = sh.a_spec;
+    }
+    std::vector<double> bn(p->B);
+    for (int s = 0; s < p->B; ++s) bn[s] = std::sqrt(msc::cabs2(bspec[s]));
+
+    MSC_CUDA(upload(p->row_pkd, pkd));
+    MSC_CUDA(upload(p->row_fn, fn));
+    MSC_CUDA(upload(p->row_c, rc));
+    MSC_CUDA(upload(p->row_b, rb));
+    MSC_CUDA(upload(p->sys_bspec, bspec));
+    MSC_CUDA(upload(p->sys_aspec, aspec));
+    MSC_CUDA(upload(p->sys_spec_row, spec_row));
+    MSC_CUDA(upload(p->nbr, nbr));
+    MSC_CUDA(upload(p->tile_row0, p->tile_row0_h));
+    MSC_CUDA(upload(p->tile_nrow, p->tile_nrow_h));
+    MSC_CUDA(upload(p->tile_sys, p->tile_sys_h));
+    MSC_CUDA(upload(p->sys_tile0, p->sys_tile0_h));
+    MSC_CUDA(upload(p->row_sys, p->row_sys_h));
+    MSC_CUDA(upload(p->bnorm, bn));
+
+    const size_t vs = (size_t)p->R * n;
+    const int m = p->m;
+    p->pstride = m + 2;
+    MSC_CUDA(p->X.alloc(vs));
+    MSC_CUDA(p->W.alloc(vs));
+    MSC_CUDA(p->U.alloc(vs));
+    MSC_CUDA(p->TMP.alloc(vs));
+    MSC_CUDA(p->Q.alloc(vs * (m + 1)));
+    MSC_CUDA(p->partial.alloc((size_t)p->ntiles * p->pstride));
+    MSC_CUDA(p->H.alloc((size_t)p->B * (m + 1) * m));
+    MSC_CUDA(p->cs.alloc((size_t)p->B * m));
+    MSC_CUDA(p->sn.alloc((size_t)p->B * m));
+    MSC_CUDA(p->g.alloc((size_t)p->B * (m + 1)));
+    MSC_CUDA(p->h1.alloc((size_t)p->B * (m + 2)));
+    MSC_CUDA(p->h2.alloc((size_t)p->B * (m + 2)));
+    MSC_CUDA(p->y.alloc((size_t)p->B * m));
+    MSC_CUDA(p->scale.alloc(p->B));
+    MSC_CUDA(p->resid.alloc(p->B));
+    MSC_CUDA(p->est.alloc(p->B));
+    MSC_CUDA(p->active.alloc(p->B));
+    MSC_CUDA(p->kcyc.alloc(p->B));
+    MSC_CUDA(p->iters.alloc(p->B));
+    MSC_CUDA(p->cycles.alloc(p->B));
+    MSC_CUDA(p->unfinished.alloc(p->B));
+    MSC_CUDA(p->status.alloc(p->B));
+    MSC_CUDA(p->counter.alloc(1));
+    MSC_CUDA(cudaMemset(p->H.p, 0, p->H.count * sizeof(double2)));
+    MSC_CUDA(cudaMemset(p->h1.p, 0, p->h1.count * sizeof(double2)));
+    MSC_CUDA(cudaMemset(p->y.p, 0, p->y.count * sizeof(double2)));
+
+    MSC_CUDA(cudaMallocHost(&p->kcyc_host, p->B * sizeof(int)));
+    for (int s = 0; s < p->B; ++s) p->kcyc_host[s] = 0;
+    p->tev.resize((size_t)2 * (m + 1) * 2);
+    for (cudaEvent_t &e : p->tev) MSC_CUDA(cudaEventCreate(&e));
+    msc_status st = capture(p, record_cycle_start, &p->g_start, &p->launches_start);
+    if (st != MSC_OK) return st;
+    st = capture(p, record_cycle_iterations, &p->g_iter, &p->launches_iter);
+    if (st != MSC_OK) return st;
+    p->finalized = true;
+    return MSC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *msc_last_error(void) { return g_last_error.c_str(); }
+const char *msc_version(void) { return "multiscat_b200 0.1 (sm_100a)"; }
+
+msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc)
+{
+    if (!plan || !desc) return fail(MSC_ERR_ARG, "null argument");
+    *plan = nullptr;
+    if (desc->n_z <= 1 || desc->n_z > msc::kMaxNz || desc->nkx <= 0 || desc->nky <= 0 ||
+        desc->n_systems <= 0)
+        return fail(MSC_ERR_DIMS, "bad plan dimensions");
+    if (desc->restart < 1 || desc->restart > msc::kMaxRestart || desc->max_iterations < 1 ||
+        !(desc->rtol > 0.0))
+        return fail(MSC_ERR_ARG, "bad solver options");
+    if (desc->precision != MSC_PRECISION_FP64)
+        return fail(MSC_ERR_NOT_BUILT, "only MSC_PRECISION_FP64 is available in this build");
+    msc_plan *p = new (std::nothrow) msc_plan();
+    if (!p) return fail(MSC_ERR_CUDA, "host allocation failed");
+    p->desc = *desc;
+    p->n = desc->n_z;
+    p->nkx = desc->nkx;
+    p->nky = desc->nky;
+    p->B = desc->n_systems;
+    p->m = desc->restart;
+    p->sys.resize(p->B);
+    msc_status st = set_kernel_attributes(p->n, 0);
+    if (st != MSC_OK) { delete p; return st; }
+    cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost(&p->counter_host, sizeof(int));
+    if (e != cudaSuccess) {
+        delete p;
+        return fail(MSC_ERR_CUDA, std::string("plan create: ") + cudaGetErrorString(e));
+    }
+    *plan = p;
+    return MSC_OK;
+}
+
+msc_status msc_plan_destroy(msc_plan *plan)
+{
+    if (!plan) return MSC_OK;
+    cudaStreamSynchronize(plan->stream);
+    delete plan;
+    return MSC_OK;
+}
+
+msc_status msc_plan_set_potential(msc_plan *p, const double *potential_values, const double *kinetic)
+{
+    if (!p || !potential_values || !kinetic) return fail(MSC_ERR_ARG, "null argument");
+    if (p->finalized) return fail(MSC_ERR_ARG, "plan already finalized");
+    const int n = p->n, nkx = p->nkx, nky = p->nky;
+    const double2 *V = reinterpret_cast<const double2 *>(potential_values);
+    // H0 = T + diag Re V00
+    std::vector<double> H(kinetic, kinetic + (size_t)n * n);
+    p->T_host.assign(kinetic, kinetic + (size_t)n * n);
+    p->v00_host.resize(n);
+    for (int k = 0; k < n; ++k) {
+        p->v00_host[k] = V[k].x;   // storage (0, 0)
+        H[(size_t)k * n + k] += V[k].x;
+    }
+    for (double hv : H)
+        if (!std::isfinite(hv)) return fail(MSC_ERR_NONFINITE, "non-finite kinetic or V00");
+    p->lam_host.resize(n);
+    p->E_host.resize((size_t)n * n);
+    if (msc::symmetric_eigh(n, H.data(), p->lam_host.data(), p->E_host.data()) != 0)
+        return fail(MSC_ERR_EIGEN, "eigensolver did not converge");
+    p->en_host.resize(n);
+    for (int k = 0; k < n; ++k) p->en_host[k] = p->E_host[(size_t)(n - 1) * n + k];
+    std::vector<double> ET((size_t)n * n);
+    for (int z = 0; z < n; ++z)
+        for (int k = 0; k < n; ++k) ET[(size_t)k * n + z] = p->E_host[(size_t)z * n + k];
+    // coupling taps: every nonzero V_G with G != 0
+    p->taps.clear();
+    p->Vt_host.clear();
+    for (int dx = 0; dx < nkx; ++dx)
+        for (int dy = 0; dy < nky; ++dy) {
+            if (dx == 0 && dy == 0) continue;
+            const double2 *v = V + ((size_t)dx * nky + dy) * n;
+            bool nz = false;
+            for (int k = 0; k < n && !nz; ++k) nz = (v[k].x != 0.0 || v[k].y != 0.0);
+            if (!nz) continue;
+            p->taps.emplace_back(dx, dy);
+            p->Vt_host.insert(p->Vt_host.end(), v, v + n);
+        }
+    p->K = (int)p->taps.size();
+    if (p->K > msc::kMaxTaps) return fail(MSC_ERR_DIMS, "too many nonzero coupling taps");
+    for (const double2 &v : p->Vt_host)
+        if (!std::isfinite(v.x) || !std::isfinite(v.y)) return fail(MSC_ERR_NONFINITE, "non-finite potential");
+    MSC_CUDA(upload(p->E, p->E_host));
+    MSC_CUDA(upload(p->ET, ET));
+    MSC_CUDA(upload(p->Tm, p->T_host));
+    MSC_CUDA(upload(p->lam, p->lam_host));
+    MSC_CUDA(upload(p->en, p->en_host));
+    MSC_CUDA(upload(p->v00, p->v00_host));
+    if (p->K > 0) {
+        MSC_CUDA(upload(p->Vt, p->Vt_host));
+    } else {
+        std::vector<double2> dummy(1, double2{0.0, 0.0});
+        MSC_CUDA(upload(p->Vt, dummy));
+    }
+    p->potential_set = true;
+    return MSC_OK;
+}
+
+msc_status msc_plan_set_system(msc_plan *p, int32_t s, int32_t n_channels, const int32_t *channel_ix,
+                               const int32_t *channel_iy, const double *pkd, const double *wave_b,
+                               const double *wave_c, int32_t specular, const double *wave_a_spec)
+{
+    if (!p || !channel_ix || !channel_iy || !pkd || !wave_b || !wave_c)
+        return fail(MSC_ERR_ARG, "null argument");
+    if (p->finalized) return fail(MSC_ERR_ARG, "plan already finalized");
+    if (s < 0 || s >= p->B) return fail(MSC_ERR_ARG, "system index out of range");
+    if (n_channels <= 0 || n_channels > p->nkx * p->nky) return fail(MSC_ERR_DIMS, "bad channel count");
+    if (specular < 0 || specular >= n_channels) return fail(MSC_ERR_ARG, "bad specular index");
+    SystemHost &sh = p->sys[s];
+    sh.C = n_channels;
+    sh.spec = specular;
+    sh.ix.assign(channel_ix, channel_ix + n_channels);
+    sh.iy.assign(channel_iy, channel_iy + n_channels);
+    std::vector<char> seen((size_t)p->nkx * p->nky, 0);
+    for (int j = 0; j < n_channels; ++j) {
+        if (sh.ix[j] < 0 || sh.ix[j] >= p->nkx || sh.iy[j] < 0 || sh.iy[j] >= p->nky)
+            return fail(MSC_ERR_DIMS, "channel position outside the torus");
+        char &f = seen[(size_t)sh.ix[j] * p->nky + sh.iy[j]];
+        if (f) return fail(MSC_ERR_DIMS, "duplicate channel position");
+        f = 1;
+    }
+    sh.pkd.assign(pkd, pkd + n_channels);
+    sh.b.resize(n_channels);
+    sh.c.resize(n_channels);
+    for (int j = 0; j < n_channels; ++j) {
+        sh.b[j] = double2{wave_b[2 * j], wave_b[2 * j + 1]};
+        sh.c[j] = double2{wave_c[2 * j], wave_c[2 * j + 1]};
+        if (!std::isfinite(sh.pkd[j]) || !std::isfinite(sh.c[j].x) || !std::isfinite(sh.c[j].y))
+            return fail(MSC_ERR_NONFINITE, "non-finite channel data");
+    }
+    sh.a_spec = wave_a_spec ? double2{wave_a_spec[0], wave_a_spec[1]} : double2{0.0, 0.0};
+    if (sh.b[specular].x == 0.0 && sh.b[specular].y == 0.0)
+        return fail(MSC_ERR_ARG, "specular channel is closed (b = 0)");
+    sh.set = true;
+    return MSC_OK;
+}
+
+int64_t msc_plan_total_rows(const msc_plan *p)
+{
+    if (!p) return -1;
+    int64_t r = 0;
+    for (const SystemHost &sh : p->sys) r += sh.C;
+    return r;
+}
+
+msc_status msc_solve(msc_plan *p, double *psi_out, double *intensities_out, msc_result *results,
+                     void *stream)
+{
+    if (!p) return fail(MSC_ERR_ARG, "null plan");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
+    cudaStream_t ps = p->stream;
+    cudaEvent_t ev;
+    MSC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    MSC_CUDA(cudaEventRecord(ev, user));
+    MSC_CUDA(cudaStreamWaitEvent(ps, ev, 0));
+    // reset state
+    const size_t vs = (size_t)p->R * p->n;
+    MSC_CUDA(cudaMemsetAsync(p->X.p, 0, vs * sizeof(double2), ps));
+    MSC_CUDA(cudaMemsetAsync(p->iters.p, 0, p->B * sizeof(int), ps));
+    MSC_CUDA(cudaMemsetAsync(p->cycles.p, 0, p->B * sizeof(int), ps));
+    MSC_CUDA(cudaMemsetAsync(p->status.p, 0, p->B * sizeof(int), ps));
+    MSC_CUDA(cudaMemsetAsync(p->kcyc.p, 0, p->B * sizeof(int), ps));
+    {
+        std::vector<int> ones(p->B, 1);
+        MSC_CUDA(cudaMemcpyAsync(p->unfinished.p, ones.data(), p->B * sizeof(int),
+                                 cudaMemcpyHostToDevice, ps));
+        MSC_CUDA(cudaStreamSynchronize(ps));
+    }
+    const int max_cycles = p->desc.max_iterations + 2;
+    int cycle = 0;
+    int64_t launches = 0;
+    bool pending = false;
+    for (; cycle < max_cycles; ++cycle) {
+        MSC_CUDA(cudaGraphLaunch(p->g_start, ps));
+        launches += p->launches_start;
+        MSC_CUDA(cudaStreamSynchronize(ps));
+        if (pending && p->timing) accumulate_timing(p);
+        pending = false;
+        if (*p->counter_host == 0) break;
+        MSC_CUDA(cudaGraphLaunch(p->g_iter, ps));
+        launches += p->launches_iter;
+        pending = true;
+    }
+    p->launches_last = launches;
+    p->cycles_last = cycle;
+    MSC_CUDA(cudaGetLastError());
+    if (psi_out)
+        MSC_CUDA(cudaMemcpyAsync(psi_out, p->X.p, vs * sizeof(double2), cudaMemcpyDeviceToDevice, ps));
+    if (intensities_out) {
+        msc::k_intensities<<<(p->R + 255) / 256, 256, 0, ps>>>(
+            p->R, 0, p->n, p->row_sys.p, p->sys_spec_row.p, p->sys_aspec.p, p->row_b.p, p->X.p,
+            intensities_out);
+        MSC_CUDA(cudaGetLastError());
+    }
+    std::vector<int> iters(p->B), cycles(p->B), status(p->B), unfinished(p->B);
+    std::vector<double> resid(p->B);
+    MSC_CUDA(cudaMemcpyAsync(iters.data(), p->iters.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaMemcpyAsync(cycles.data(), p->cycles.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaMemcpyAsync(status.data(), p->status.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaMemcpyAsync(unfinished.data(), p->unfinished.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaMemcpyAsync(resid.data(), p->resid.p, p->B * sizeof(double), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaEventRecord(ev, ps));
+    MSC_CUDA(cudaStreamWaitEvent(user, ev, 0));
+    MSC_CUDA(cudaStreamSynchronize(ps));
+    cudaEventDestroy(ev);
+    msc_status worst = MSC_OK;
+    for (int s = 0; s < p->B; ++s) {
+        int sst = unfinished[s] ? MSC_ERR_NOT_CONVERGED : status[s];
+        if (results) {
+            results[s].iterations = iters[s];
+            results[s].refinements = cycles[s];
+            results[s].status = sst;
+            results[s].reserved = 0;
+            results[s].residual = resid[s];
+        }
+        if (sst != MSC_OK && worst == MSC_OK) worst = (msc_status)sst;
+    }
+    if (worst != MSC_OK) g_last_error = "at least one system did not converge";
+    return worst;
+}
+
+msc_status msc_plan_get_info(const msc_plan *p, msc_plan_info *info)
+{
+    if (!p || !info) return fail(MSC_ERR_ARG, "null argument");
+    info->total_rows = msc_plan_total_rows(p);
+    info->n_taps = p->K;
+    info->n_tiles = p->ntiles;
+    info->launches_last = p->launches_last;
+    info->cycles_last = p->cycles_last;
+    info->reserved = 0;
+    return MSC_OK;
+}
+
+msc_status msc_plan_set_kernel_timing(msc_plan *p, int enable)
+{
+    if (!p) return fail(MSC_ERR_ARG, "null plan");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    const bool want = enable != 0;
+    if (want == p->timing) return MSC_OK;
+    p->timing = want;
+    p->t_ms[0] = p->t_ms[1] = 0.0;
+    p->t_launches[0] = p->t_launches[1] = 0;
+    return capture(p, record_cycle_iterations, &p->g_iter, &p->launches_iter);
+}
+
+msc_status msc_plan_kernel_timing(msc_plan *p, double *ms, int64_t *launches)
+{
+    if (!p || !ms || !launches) return fail(MSC_ERR_ARG, "null argument");
+    for (int k = 0; k < 2; ++k) {
+        ms[k] = p->t_ms[k];
+        launches[k] = p->t_launches[k];
+        p->t_ms[k] = 0.0;
+        p->t_launches[k] = 0;
+    }
+    return MSC_OK;
+}
+
+msc_status msc_debug_apply_coupling(msc_plan *p, const double *x, double *y, void *stream)
+{
+    if (!p || !x || !y) return fail(MSC_ERR_ARG, "null argument");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    launch_coupling(p, nullptr, reinterpret_cast<const double2 *>(x), nullptr, 1.0,
+                    reinterpret_cast<double2 *>(y), s);
+    MSC_CUDA(cudaGetLastError());
+    return MSC_OK;
+}
+
+msc_status msc_debug_apply_block_inverse(msc_plan *p, const double *x, double *y, void *stream)
+{
+    if (!p || !x || !y) return fail(MSC_ERR_ARG, "null argument");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    launch_block_inverse(p, nullptr, reinterpret_cast<const double2 *>(x),
+                         reinterpret_cast<double2 *>(y), 0, s);
+    MSC_CUDA(cudaGetLastError());
+    return MSC_OK;
+}
+
+msc_status msc_debug_apply_operator(msc_plan *p, const double *x, double *y, void *stream)
+{
+    if (!p || !x || !y) return fail(MSC_ERR_ARG, "null argument");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    // y = -(b - D x) with b switched off, then y += V_off x
+    launch_residual_diag(p, nullptr, reinterpret_cast<const double2 *>(x), p->TMP.p, 0, s);
+    launch_coupling(p, nullptr, reinterpret_cast<const double2 *>(x), p->TMP.p, -1.0,
+                    reinterpret_cast<double2 *>(y), s);
+    // y currently holds -(D x + V_off x)
+    const size_t cnt = (size_t)p->R * p->n;
+    msc::k_scale<<<(unsigned)std::min<size_t>((cnt + 255) / 256, 4096), 256, 0, s>>>(
+        reinterpret_cast<double2 *>(y), cnt, -1.0);
+    MSC_CUDA(cudaGetLastError());
+    return MSC_OK;
+}
+
+msc_status msc_intensities(msc_plan *p, int32_t s, const double *psi, double *intensities, void *stream)
+{
+    if (!p || !psi || !intensities) return fail(MSC_ERR_ARG, "null argument");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    if (s < 0 || s >= p->B) return fail(MSC_ERR_ARG, "system index out of range");
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+    const int r0 = p->sys_row0_h[s], C = p->sys[s].C;
+    msc::k_intensities<<<(C + 255) / 256, 256, 0, cs>>>(
+        C, r0, p->n, p->row_sys.p + r0, p->sys_spec_row.p, p->sys_aspec.p, p->row_b.p + r0,
+        reinterpret_cast<const double2 *>(psi), intensities);
+    MSC_CUDA(cudaGetLastError());
+    return MSC_OK;
+}
+
+int msc_run_multiscat(int gmres_preconditioner_flag, int convergence_significant_figures, int nkx,
+                      int nky, int nz, const double *potential_values,
+                      const double *perpendicular_kinetic_difference, const double *wave_a,
+                      const double *wave_b, const double *wave_c,
+                      const double *parallel_kinetic_energy, double *scattered_state_out,
+                      int *iterations_out)
+{
+    (void)gmres_preconditioner_flag;
+    if (nkx <= 0 || nky <= 0 || nz <= 0) return MSC_ERR_DIMS;
+    if (!potential_values || !perpendicular_kinetic_difference || !wave_b || !wave_c ||
+        !parallel_kinetic_energy || !scattered_state_out)
+        return MSC_ERR_ARG;
+    msc_plan_desc d{};
+    d.n_z = nz;
+    d.nkx = nkx;
+    d.nky = nky;
+    d.n_systems = 1;
+    d.restart = 30;
+    d.max_iterations = 2000;
+    d.rtol = 0.005 * std::pow(10.0, -(double)convergence_significant_figures);
+    d.precision = MSC_PRECISION_FP64;
+    msc_plan *p = nullptr;
+    msc_status st = msc_plan_create(&p, &d);
+    if (st != MSC_OK) return st;
+    const int C = nkx * nky;
+    std::vector<int32_t> ix(C), iy(C);
+    for (int i = 0; i < nkx; ++i)
+        for (int j = 0; j < nky; ++j) {
+            ix[i * nky + j] = i;
+            iy[i * nky + j] = j;
+        }
+    st = msc_plan_set_potential(p, potential_values, parallel_kinetic_energy);
+    if (st == MSC_OK)
+        st = msc_plan_set_system(p, 0, C, ix.data(), iy.data(), perpendicular_kinetic_difference,
+                                 wave_b, wave_c, 0, wave_a);
+    double *psi_dev = nullptr;
+    msc_result res{};
+    if (st == MSC_OK) {
+        if (cudaMalloc(&psi_dev, (size_t)C * nz * sizeof(double2)) != cudaSuccess) st = MSC_ERR_CUDA;
+    }
+    if (st == MSC_OK) st = msc_solve(p, psi_dev, nullptr, &res, nullptr);
+    if (st == MSC_OK || st == MSC_ERR_NOT_CONVERGED) {
+        if (cudaMemcpy(scattered_state_out, psi_dev, (size_t)C * nz * sizeof(double2),
+                       cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = MSC_ERR_CUDA;
+    }
+    if (iterations_out) *iterations_out = res.iterations;
+    if (psi_dev) cudaFree(psi_dev);
+    msc_plan_destroy(p);
+    return st;
+}
+
+}  // extern "C"

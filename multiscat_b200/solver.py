@@ -1,0 +1,249 @@
+"""Host side of the solver: plans on torch device memory, and the drop-in call.
+
+``run_multiscat_fortran`` has the argument list, return value and errors of
+the reference's f2py export (``lib/multiscat_fortran/src/multiscat_fortran/
+__init__.py:39-60``): it returns psi[nkx, nky, nz] and raises
+``RuntimeError("... failed with error code N")`` with N = 1 for bad
+dimensions and N = 2 when GMRES does not converge
+(``multiscat_python_bindings.f90:42-45, 58-60``).
+
+``ScatteringPlan`` is the batched, device-resident form: one potential,
+many beams, all solved in one go on the current CUDA device.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native as nat
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def run_multiscat_fortran(gmres_preconditioner_flag: int, convergence_significant_figures: int,
+                          potential_values, perpendicular_kinetic_difference, wave_a, wave_b,
+                          wave_c, parallel_kinetic_energy) -> np.ndarray:
+    """Drop-in for ``multiscat_fortran.run_multiscat_fortran`` on the GPU (FP64)."""
+    lib = nat.load()
+    v = np.ascontiguousarray(potential_values, dtype=np.complex128)
+    if v.ndim != 3:
+        raise RuntimeError("B200 run_multiscat_fortran failed with error code 1")
+    nkx, nky, nz = v.shape
+    pkd = np.ascontiguousarray(perpendicular_kinetic_difference, dtype=np.float64)
+    wa = np.ascontiguousarray(np.asarray(wave_a, np.complex128).ravel())
+    wb = np.ascontiguousarray(np.asarray(wave_b, np.complex128).ravel())
+    wc = np.ascontiguousarray(np.asarray(wave_c, np.complex128).ravel())
+    t = np.ascontiguousarray(parallel_kinetic_energy, dtype=np.float64)
+    c = nkx * nky
+    if pkd.size != c or wa.size != c or wb.size != c or wc.size != c or t.shape != (nz, nz):
+        raise RuntimeError("B200 run_multiscat_fortran failed with error code 1")
+    out = np.zeros((nkx, nky, nz), np.complex128)
+    iters = ctypes.c_int(0)
+    ierr = lib.msc_run_multiscat(int(gmres_preconditioner_flag),
+                                 int(convergence_significant_figures), nkx, nky, nz,
+                                 _dptr(v.view(np.float64)), _dptr(pkd),
+                                 _dptr(wa.view(np.float64)), _dptr(wb.view(np.float64)),
+                                 _dptr(wc.view(np.float64)), _dptr(t),
+                                 _dptr(out.view(np.float64)), ctypes.byref(iters))
+    if ierr != 0:
+        raise RuntimeError(f"B200 run_multiscat_fortran failed with error code {ierr}"
+                           f" ({nat.last_error()})")
+    return out
+
+
+@dataclass
+class SystemSpec:
+    """One beam: channel list on the torus plus its boundary arrays."""
+
+    channel_ix: np.ndarray      # int32 [C] storage positions
+    channel_iy: np.ndarray
+    pkd: np.ndarray             # float64 [C]
+    wave_a: np.ndarray          # complex128 [C]
+    wave_b: np.ndarray          # complex128 [C]
+    wave_c: np.ndarray          # complex128 [C]
+    specular: int = 0
+
+
+@dataclass
+class SolveResult:
+    psi: torch.Tensor           # complex128 [R, nz] on the device
+    intensities: torch.Tensor   # float64 [R] on the device
+    row_offsets: np.ndarray     # [B + 1]
+    iterations: np.ndarray
+    cycles: np.ndarray
+    status: np.ndarray
+    residual: np.ndarray
+
+    def system_intensities(self, s: int) -> torch.Tensor:
+        return self.intensities[self.row_offsets[s]:self.row_offsets[s + 1]]
+
+    def system_psi(self, s: int) -> torch.Tensor:
+        return self.psi[self.row_offsets[s]:self.row_offsets[s + 1]]
+
+
+class ScatteringPlan:
+    """A batch of beams sharing one potential, solved together on the GPU."""
+
+    def __init__(self, potential_values, kinetic, systems: list[SystemSpec], *,
+                 rtol: float = 1e-10, restart: int = 30, max_iterations: int = 2000,
+                 precision: str = "fp64", inner_rtol: float = 0.0, inner_restart: int = 0,
+                 max_refinements: int = 0):
+        self._lib = nat.load()
+        v = np.ascontiguousarray(np.asarray(potential_values), dtype=np.complex128)
+        nkx, nky, nz = v.shape
+        t = np.ascontiguousarray(np.asarray(kinetic), dtype=np.float64)
+        self.nkx, self.nky, self.nz = nkx, nky, nz
+        self.systems = systems
+        desc = nat.PlanDesc()
+        desc.n_z = nz
+        desc.nkx = nkx
+        desc.nky = nky
+        desc.n_systems = len(systems)
+        desc.restart = restart
+        desc.max_iterations = max_iterations
+        desc.rtol = rtol
+        desc.precision = {"fp64": nat.PRECISION_FP64, "mixed": nat.PRECISION_MIXED}[precision]
+        desc.inner_restart = inner_restart
+        desc.inner_rtol = inner_rtol
+        desc.max_refinements = max_refinements
+        self._plan = ctypes.c_void_p()
+        nat.check("msc_plan_create", self._lib.msc_plan_create(ctypes.byref(self._plan),
+                                                              ctypes.byref(desc)))
+        nat.check("msc_plan_set_potential", self._lib.msc_plan_set_potential(
+            self._plan, _dptr(v.view(np.float64)), _dptr(t)))
+        offsets = [0]
+        for s, sp in enumerate(systems):
+            ix = np.ascontiguousarray(sp.channel_ix, dtype=np.int32)
+            iy = np.ascontiguousarray(sp.channel_iy, dtype=np.int32)
+            pkd = np.ascontiguousarray(sp.pkd, dtype=np.float64)
+            wb = np.ascontiguousarray(sp.wave_b, dtype=np.complex128)
+            wc = np.ascontiguousarray(sp.wave_c, dtype=np.complex128)
+            asp = np.array([complex(sp.wave_a[sp.specular]).real,
+                            complex(sp.wave_a[sp.specular]).imag])
+            nat.check("msc_plan_set_system", self._lib.msc_plan_set_system(
+                self._plan, s, ix.size, _iptr(ix), _iptr(iy), _dptr(pkd),
+                _dptr(wb.view(np.float64)), _dptr(wc.view(np.float64)), int(sp.specular),
+                _dptr(asp)))
+            offsets.append(offsets[-1] + ix.size)
+        self.row_offsets = np.asarray(offsets)
+        self.total_rows = int(offsets[-1])
+
+    def close(self) -> None:
+        if getattr(self, "_plan", None) and self._plan.value:
+            self._lib.msc_plan_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, *, raise_on_error: bool = True) -> SolveResult:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        psi = torch.empty((self.total_rows, self.nz), dtype=torch.complex128, device=dev)
+        inten = torch.empty((self.total_rows,), dtype=torch.float64, device=dev)
+        res = (nat.Result * len(self.systems))()
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        st = self._lib.msc_solve(self._plan, ctypes.c_void_p(psi.data_ptr()),
+                                 ctypes.c_void_p(inten.data_ptr()), res, ctypes.c_void_p(stream))
+        if st not in (nat.MSC_OK, nat.MSC_ERR_NOT_CONVERGED, nat.MSC_ERR_NONFINITE) or (
+                raise_on_error and st != nat.MSC_OK):
+            nat.check("msc_solve", st)
+        return SolveResult(
+            psi=psi, intensities=inten, row_offsets=self.row_offsets,
+            iterations=np.array([r.iterations for r in res]),
+            cycles=np.array([r.refinements for r in res]),
+            status=np.array([r.status for r in res]),
+            residual=np.array([r.residual for r in res]))
+
+    def info(self) -> "nat.PlanInfo":
+        inf = nat.PlanInfo()
+        nat.check("msc_plan_get_info", self._lib.msc_plan_get_info(self._plan, ctypes.byref(inf)))
+        return inf
+
+    @property
+    def n_taps(self) -> int:
+        return int(self.info().n_taps)
+
+    def launches_per_solve(self, _result=None) -> int:
+        """Kernel launches issued by the last solve (graph kernel nodes, all cycles)."""
+        return int(self.info().launches_last)
+
+    def enable_kernel_timing(self, on: bool = True) -> None:
+        nat.check("msc_plan_set_kernel_timing",
+                  self._lib.msc_plan_set_kernel_timing(self._plan, 1 if on else 0))
+
+    def kernel_timing(self) -> dict:
+        ms = (ctypes.c_double * 2)()
+        cnt = (ctypes.c_int64 * 2)()
+        nat.check("msc_plan_kernel_timing", self._lib.msc_plan_kernel_timing(self._plan, ms, cnt))
+        return {"block_inverse": {"ms": ms[0], "launches": cnt[0]},
+                "coupling": {"ms": ms[1], "launches": cnt[1]}}
+
+    # debug operators on one full-grid system (x, y: complex128 [C, nz] cuda tensors)
+    def _debug(self, name: str, x: torch.Tensor) -> torch.Tensor:
+        x = x.contiguous()
+        y = torch.empty_like(x)
+        stream = torch.cuda.current_stream(x.device).cuda_stream
+        nat.check(name, getattr(self._lib, name)(self._plan, ctypes.c_void_p(x.data_ptr()),
+                                                 ctypes.c_void_p(y.data_ptr()),
+                                                 ctypes.c_void_p(stream)))
+        return y
+
+    def apply_coupling(self, x: torch.Tensor) -> torch.Tensor:
+        return self._debug("msc_debug_apply_coupling", x)
+
+    def apply_block_inverse(self, x: torch.Tensor) -> torch.Tensor:
+        return self._debug("msc_debug_apply_block_inverse", x)
+
+    def apply_operator(self, x: torch.Tensor) -> torch.Tensor:
+        return self._debug("msc_debug_apply_operator", x)
+
+
+def full_grid_system(pkd, wave_a, wave_b, wave_c) -> SystemSpec:
+    """All nkx*nky channels in the reference's row-major (ix, iy) order."""
+    pkd = np.asarray(pkd, float)
+    nkx, nky = pkd.shape
+    ix, iy = np.meshgrid(np.arange(nkx), np.arange(nky), indexing="ij")
+    return SystemSpec(ix.ravel().astype(np.int32), iy.ravel().astype(np.int32), pkd.ravel(),
+                      np.asarray(wave_a, complex).ravel(), np.asarray(wave_b, complex).ravel(),
+                      np.asarray(wave_c, complex).ravel(), 0)
+
+
+def channel_subset_system(pkd, wave_a, wave_b, wave_c, n_channels: int | None = None,
+                          max_pkd: float | None = None) -> SystemSpec:
+    """Lowest-pkd channels, as the reference's ``n_channels`` truncation.
+
+    Channels are sorted by pkd (``_scipy.py:414-416``) and the first
+    ``n_channels`` are kept, or all with pkd <= ``max_pkd``.  The specular
+    channel (storage (0, 0)) always has the lowest pkd of a beam whose
+    parallel momentum lies in the first Brillouin zone; it is located
+    explicitly either way.
+    """
+    pkd = np.asarray(pkd, float)
+    nkx, nky = pkd.shape
+    flat = pkd.ravel()
+    order = np.argsort(flat, kind="stable")
+    if n_channels is not None:
+        order = order[:n_channels]
+    if max_pkd is not None:
+        order = order[flat[order] <= max_pkd]
+    if 0 not in set(order.tolist()):
+        raise ValueError("the specular channel is not in the kept channel set")
+    ix, iy = np.unravel_index(order, (nkx, nky))
+    spec = int(np.nonzero(order == 0)[0][0])
+    return SystemSpec(ix.astype(np.int32), iy.astype(np.int32), flat[order],
+                      np.asarray(wave_a, complex).ravel()[order],
+                      np.asarray(wave_b, complex).ravel()[order],
+                      np.asarray(wave_c, complex).ravel()[order], spec)
