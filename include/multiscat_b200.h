@@ -54,7 +54,7 @@ typedef enum {
  * one coupling torus nkx x nky) and a batch of n_systems beams, each with
  * its own channel list. */
 typedef struct {
-    int32_t n_z;            /* Lobatto nodes per channel (<= 512)               */
+    int32_t n_z;            /* Lobatto nodes per channel (2..1024)              */
     int32_t nkx, nky;       /* coupling torus (the potential's Fourier grid)    */
     int32_t n_systems;      /* batch size                                       */
     int32_t restart;        /* GMRES restart length m (1..64)                   */
@@ -121,7 +121,7 @@ int64_t msc_plan_total_rows(const msc_plan *plan);
  * in the reference), parallel_kinetic_energy [nz][nz]; scattered_state_out
  * complex [nkx][nky][nz].  gmres_preconditioner_flag is accepted for
  * signature parity (this solver always uses its block-diagonal
- * preconditioner); the stop rule is ||b - A psi|| <= 0.005 * 10^-sig ||b||.
+ * preconditioner); the stop rule is ||b - A psi|| <= 5e-4 * 10^-sig ||b||.
  * iterations_out may be NULL.  Returns 0, 1 (bad dims), 2 (not converged)
  * or another msc_status. */
 int msc_run_multiscat(int gmres_preconditioner_flag, int convergence_significant_figures,

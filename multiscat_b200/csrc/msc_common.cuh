@@ -48,7 +48,8 @@ __device__ __forceinline__ float warp_sum(float v) {
 // Row tiles: every tile holds up to kTileRows consecutive channel rows of
 // ONE system, so per-tile partial reductions add up per system.
 constexpr int kTileRows = 8;
-constexpr int kMaxNz = 512;
+constexpr int kMaxNz = 1024;
+constexpr int kWideNz = 512;   // above this the block inverse stages 4 rows per pass
 constexpr int kMaxRestart = 64;
 constexpr int kMaxTaps = 2048;
 

@@ -26,6 +26,7 @@ namespace msc {
 // Two FP64 GEMMs along z with the tile's 2*kTileRows real columns staged in
 // shared memory; E and E^T stream from L2 (each is n*n doubles).
 // ---------------------------------------------------------------------------
+template <int TR>
 __global__ void __launch_bounds__(256)
 k_block_inverse(Tiles tiles, const int *__restrict__ gate, int n,
                 const double *__restrict__ E, const double *__restrict__ ET,
@@ -34,7 +35,8 @@ k_block_inverse(Tiles tiles, const int *__restrict__ gate, int n,
                 const double *__restrict__ row_fn, const double2 *__restrict__ x,
                 double2 *__restrict__ out, int accumulate)
 {
-    constexpr int TR = kTileRows;
+    // TR rows are processed per pass (8 for n <= 512, 4 above so that the two
+    // [n][2 TR] staging buffers fit in shared memory).
     constexpr int LD = 2 * TR;       // real columns per z row
     constexpr int HC = TR;           // columns handled per work item (half of LD)
     extern __shared__ double smem[];
@@ -45,8 +47,13 @@ k_block_inverse(Tiles tiles, const int *__restrict__ gate, int n,
     const int tile = blockIdx.x;
     const int sys = tiles.sys[tile];
     if (gate && gate[sys] == 0) return;
-    const int row0 = tiles.row0[tile];
-    const int nrow = tiles.nrow[tile];
+    const int tile_row0 = tiles.row0[tile];
+    const int tile_nrow = tiles.nrow[tile];
+
+    for (int pass = 0; pass < tile_nrow; pass += TR) {
+    const int row0 = tile_row0 + pass;
+    const int nrow = min(TR, tile_nrow - pass);
+    if (pass > 0) __syncthreads();
 
     for (int idx = threadIdx.x; idx < TR * n; idx += blockDim.x) {
         int r = idx / n, z = idx - r * n;
@@ -152,6 +159,7 @@ k_block_inverse(Tiles tiles, const int *__restrict__ gate, int n,
             }
         }
     }
+    }  // pass
 }
 
 // ---------------------------------------------------------------------------

@@ -161,7 +161,8 @@ cudaError_t upload(DevBuf<T> &buf, const std::vector<T> &h)
     return cudaMemcpy(buf.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
 
-size_t smem_block_inverse(int n) { return (size_t)2 * n * 2 * msc::kTileRows * sizeof(double); }
+int block_inverse_rows(int n) { return n <= msc::kWideNz ? 8 : 4; }
+size_t smem_block_inverse(int n) { return (size_t)2 * n * 2 * block_inverse_rows(n) * sizeof(double); }
 size_t smem_residual(int n) { return (size_t)n * 2 * msc::kTileRows * sizeof(double); }
 size_t smem_coupling(int K) { return (size_t)msc::kTileRows * K * sizeof(int); }
 
@@ -170,9 +171,14 @@ size_t smem_coupling(int K) { return (size_t)msc::kTileRows * K * sizeof(int); }
 void launch_block_inverse(msc_plan *p, const int *gate, const double2 *x, double2 *out, int acc,
                           cudaStream_t st)
 {
-    msc::k_block_inverse<<<p->ntiles, 256, smem_block_inverse(p->n), st>>>(
-        p->tiles(), gate, p->n, p->E.p, p->ET.p, p->lam.p, p->en.p, p->row_pkd.p, p->row_c.p,
-        p->row_fn.p, x, out, acc);
+    if (block_inverse_rows(p->n) == 8)
+        msc::k_block_inverse<8><<<p->ntiles, 256, smem_block_inverse(p->n), st>>>(
+            p->tiles(), gate, p->n, p->E.p, p->ET.p, p->lam.p, p->en.p, p->row_pkd.p, p->row_c.p,
+            p->row_fn.p, x, out, acc);
+    else
+        msc::k_block_inverse<4><<<p->ntiles, 256, smem_block_inverse(p->n), st>>>(
+            p->tiles(), gate, p->n, p->E.p, p->ET.p, p->lam.p, p->en.p, p->row_pkd.p, p->row_c.p,
+            p->row_fn.p, x, out, acc);
 }
 
 void launch_residual_diag(msc_plan *p, const int *gate, const double2 *x, double2 *out, int with_b,
@@ -239,6 +245,12 @@ cudaEvent_t tev_at(msc_plan *p, int kind, int slot, int which)
     return p->tev[((size_t)kind * (p->m + 1) + slot) * 2 + which];
 }
 
+// Event record node inside a captured graph (External: a real record at launch).
+void mark(msc_plan *p, int kind, int slot, int which, cudaStream_t st)
+{
+    cudaEventRecordWithFlags(tev_at(p, kind, slot, which), st, cudaEventRecordExternal);
+}
+
 // m Arnoldi steps (CGS2) and the solution update x += M (Q y).
 void record_cycle_iterations(msc_plan *p, cudaStream_t st)
 {
@@ -247,12 +259,12 @@ void record_cycle_iterations(msc_plan *p, cudaStream_t st)
     for (int j = 0; j < p->m; ++j) {
         double2 *Qj = p->Q.p + (size_t)j * vs;
         double2 *Qn = p->Q.p + (size_t)(j + 1) * vs;
-        if (tm) cudaEventRecord(tev_at(p, 0, j, 0), st);
+        if (tm) mark(p, 0, j, 0, st);
         launch_block_inverse(p, p->active.p, Qj, p->U.p, 0, st);
-        if (tm) cudaEventRecord(tev_at(p, 0, j, 1), st);
-        if (tm) cudaEventRecord(tev_at(p, 1, j, 0), st);
+        if (tm) mark(p, 0, j, 1, st);
+        if (tm) mark(p, 1, j, 0, st);
         launch_coupling(p, p->active.p, p->U.p, Qj, 1.0, p->W.p, st);
-        if (tm) cudaEventRecord(tev_at(p, 1, j, 1), st);
+        if (tm) mark(p, 1, j, 1, st);
         launch_dots(p, p->active.p, j + 1, p->W.p, 0, st);
         launch_reduce(p, p->active.p, j + 1, p->h1.p, st);
         launch_update(p, p->active.p, j + 1, nullptr, p->h1.p, p->m + 2, p->W.p, nullptr, p->W.p,
@@ -267,9 +279,9 @@ void record_cycle_iterations(msc_plan *p, cudaStream_t st)
     }
     msc::k_trisolve<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m);
     launch_update(p, p->kcyc.p, 0, p->kcyc.p, p->y.p, p->m, nullptr, nullptr, p->U.p, 1, st);
-    if (tm) cudaEventRecord(tev_at(p, 0, p->m, 0), st);
+    if (tm) mark(p, 0, p->m, 0, st);
     launch_block_inverse(p, p->kcyc.p, p->U.p, p->X.p, 1, st);
-    if (tm) cudaEventRecord(tev_at(p, 0, p->m, 1), st);
+    if (tm) mark(p, 0, p->m, 1, st);
     cudaMemcpyAsync(p->kcyc_host, p->kcyc.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, st);
 }
 
@@ -300,6 +312,8 @@ void accumulate_timing(msc_plan *p)
             if (cudaEventElapsedTime(&ms, tev_at(p, kind, j, 0), tev_at(p, kind, j, 1)) == cudaSuccess) {
                 p->t_ms[kind] += ms;
                 p->t_launches[kind] += 1;
+            } else {
+                (void)cudaGetLastError();   // timing is best effort; keep the error state clean
             }
         }
     }
@@ -307,6 +321,8 @@ void accumulate_timing(msc_plan *p)
     if (cudaEventElapsedTime(&ms, tev_at(p, 0, p->m, 0), tev_at(p, 0, p->m, 1)) == cudaSuccess) {
         p->t_ms[0] += ms;
         p->t_launches[0] += 1;
+    } else {
+        (void)cudaGetLastError();
     }
 }
 
@@ -331,7 +347,9 @@ msc_status capture(msc_plan *p, void (*rec)(msc_plan *, cudaStream_t), cudaGraph
 
 msc_status set_kernel_attributes(int n, int K)
 {
-    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_block_inverse(msc::kWideNz)));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_block_inverse(msc::kMaxNz)));
     MSC_CUDA(cudaFuncSetAttribute(msc::k_residual_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_residual(msc::kMaxNz)));
@@ -802,7 +820,7 @@ int msc_run_multiscat(int gmres_preconditioner_flag, int convergence_significant
     d.n_systems = 1;
     d.restart = 30;
     d.max_iterations = 2000;
-    d.rtol = 0.005 * std::pow(10.0, -(double)convergence_significant_figures);
+    d.rtol = 5e-4 * std::pow(10.0, -(double)convergence_significant_figures);
     d.precision = MSC_PRECISION_FP64;
     msc_plan *p = nullptr;
     msc_status st = msc_plan_create(&p, &d);
