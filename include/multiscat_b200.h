@@ -141,6 +141,28 @@ msc_status msc_debug_apply_coupling(msc_plan *plan, const double *x, double *y, 
 msc_status msc_debug_apply_block_inverse(msc_plan *plan, const double *x, double *y, void *stream);
 msc_status msc_debug_apply_operator(msc_plan *plan, const double *x, double *y, void *stream);
 
+/* Allocation-free twin of msc_debug_apply_operator (no counterpart in the
+ * reference): y = A x = D x + V_off x for ONE full-grid system, without a
+ * plan and without allocating anything.  For callers that cannot call
+ * cudaMalloc -- code running inside another framework's memory pool or
+ * under a fixed device-memory budget, and plug-ins that may only use the
+ * buffers they are handed.  Every argument is a device pointer:
+ *   potential_values complex [nkx][nky][n_z], kinetic [n_z][n_z],
+ *   pkd [nkx*nky], wave_c complex [nkx*nky], x and y complex [nkx*nky][n_z].
+ * Working storage is a 32 MiB __device__ array inside the library, held by
+ * every GPU that loads the library until the process exits; sizes whose tap
+ * table, neighbour table and intermediate do not fit are rejected with
+ * MSC_ERR_DIMS (nkx*nky <= 2049 channels, and about
+ * 32 (nkx*nky) n_z + 4 (nkx*nky)^2 bytes in total).  The first call on each
+ * device looks up the array's device address and sets kernel limits; make
+ * it before any stream capture.  The call waits on `stream` once (to read
+ * the number of nonzero taps).  All calls share the array and keep the last
+ * call's contents: calls that overlap on the GPU race. */
+msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32_t n_z,
+                                      const double *potential_values, const double *kinetic,
+                                      const double *pkd, const double *wave_c, const double *x,
+                                      double *y, void *stream);
+
 /* |S_G0|^2 per channel from psi[C][n_z] (device pointers), for one system. */
 msc_status msc_intensities(msc_plan *plan, int32_t s, const double *psi, double *intensities,
                            void *stream);

@@ -19,7 +19,7 @@ EXPORTED = (
     "msc_solve", "msc_plan_total_rows", "msc_run_multiscat", "msc_debug_apply_coupling",
     "msc_debug_apply_block_inverse", "msc_debug_apply_operator", "msc_intensities",
     "msc_last_error", "msc_version", "msc_plan_get_info", "msc_plan_set_kernel_timing",
-    "msc_plan_kernel_timing",
+    "msc_plan_kernel_timing", "msc_apply_operator_noalloc",
 )
 
 MSC_OK = 0
@@ -124,6 +124,9 @@ def load() -> ctypes.CDLL:
     lib.msc_plan_set_kernel_timing.argtypes = [_vp, ctypes.c_int]
     lib.msc_plan_kernel_timing.restype = ctypes.c_int
     lib.msc_plan_kernel_timing.argtypes = [_vp, _dp, ctypes.POINTER(ctypes.c_int64)]
+    lib.msc_apply_operator_noalloc.restype = ctypes.c_int
+    lib.msc_apply_operator_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                               _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     lib.msc_last_error.restype = ctypes.c_char_p
     lib.msc_last_error.argtypes = []
     lib.msc_version.restype = ctypes.c_char_p

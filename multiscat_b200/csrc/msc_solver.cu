@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -854,3 +855,208 @@ int msc_run_multiscat(int gmres_preconditioner_flag, int convergence_significant
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free operator apply.
+//
+// Some callers cannot call cudaMalloc at all: code that runs inside another
+// framework's memory pool or under a strict device-memory budget, plug-ins
+// that must not grow the process's allocations, and callers that work only
+// on buffers handed to them.  msc_apply_operator_noalloc gives them y = A x
+// for one full-grid system using only the buffers they pass plus a fixed
+// scratch area that is part of this library's image: a file-scope
+// __device__ array of kNoAllocScratchBytes (32 MiB) that every GPU which
+// loads the library holds until the process exits.  The scratch keeps the
+// tap table, neighbour table, row tiles and the D x intermediate of the
+// last call; each call rewrites every byte it reads, so nothing has to start
+// at zero.  All calls share the one array: calls that overlap on the GPU
+// (different streams, or threads using the same device) race on it.
+// ===========================================================================
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 32u << 20;
+constexpr int kNoAllocMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void *g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Nonzero coupling taps of V (storage offsets != (0, 0)) in (dx, dy)
+// row-major order, Re V_00 into v00, the tap count into *count.  One block;
+// order-preserving compaction so the tap order equals the plan builder's.
+__global__ void __launch_bounds__(1024)
+k_noalloc_scan_taps(int nkx, int nky, int n, const double2 *__restrict__ V, int *count,
+                    int2 *__restrict__ taps, double *__restrict__ v00)
+{
+    __shared__ int warp_off[32];
+    __shared__ int base;
+    for (int z = threadIdx.x; z < n; z += blockDim.x) v00[z] = V[z].x;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    const int total = nkx * nky;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    for (int c0 = 0; c0 < total; c0 += blockDim.x) {
+        const int c = c0 + threadIdx.x;
+        int flag = 0;
+        if (c > 0 && c < total) {
+            const double2 *v = V + (size_t)c * n;
+            for (int z = 0; z < n && !flag; ++z) flag = (v[z].x != 0.0 || v[z].y != 0.0);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, flag);
+        const int in_warp = __popc(m & ((1u << lane) - 1u));
+        if (lane == 0) warp_off[warp] = __popc(m);
+        __syncthreads();
+        if (warp == 0) {
+            const int own = (lane < nwarps) ? warp_off[lane] : 0;
+            int inc = own;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int up = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += up;
+            }
+            if (lane < nwarps) warp_off[lane] = inc - own;
+        }
+        __syncthreads();
+        const int pos = base + warp_off[warp] + in_warp;
+        if (flag) taps[pos] = make_int2(c / nky, c % nky);
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) base = pos + flag;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = base;
+}
+
+// Tap values, neighbour table, row tiles and the (unused) right-hand-side
+// slots for one full-grid system.
+__global__ void k_noalloc_tables(int nkx, int nky, int n, int K, const double2 *__restrict__ V,
+                                 const int2 *__restrict__ taps, double2 *__restrict__ Vt,
+                                 int *__restrict__ nbr, int *__restrict__ tile_row0,
+                                 int *__restrict__ tile_nrow, int *__restrict__ tile_sys, int ntiles,
+                                 int *__restrict__ spec_row, double2 *__restrict__ bspec)
+{
+    const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const int C = nkx * nky;
+    for (size_t i = tid; i < (size_t)K * n; i += stride) {
+        const int t = (int)(i / n), z = (int)(i - (size_t)t * n);
+        Vt[i] = V[((size_t)taps[t].x * nky + taps[t].y) * n + z];
+    }
+    for (size_t i = tid; i < (size_t)C * K; i += stride) {
+        const int r = (int)(i / K), t = (int)(i - (size_t)r * K);
+        const int ix = r / nky, iy = r - ix * nky;
+        const int sx = ((ix - taps[t].x) % nkx + nkx) % nkx;
+        const int sy = ((iy - taps[t].y) % nky + nky) % nky;
+        nbr[i] = sx * nky + sy;
+    }
+    for (size_t i = tid; i < (size_t)ntiles; i += stride) {
+        tile_row0[i] = (int)i * msc::kTileRows;
+        tile_nrow[i] = min(msc::kTileRows, C - (int)i * msc::kTileRows);
+        tile_sys[i] = 0;
+    }
+    if (tid == 0) {
+        spec_row[0] = 0;
+        bspec[0] = make_double2(0.0, 0.0);
+    }
+}
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Device address of the scratch array on the current device (set-up on the
+// first call per device: symbol lookup and kernel shared-memory limits).
+msc_status noalloc_scratch(unsigned char **out)
+{
+    int dev = -1;
+    MSC_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(MSC_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_base[dev]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || ptr == nullptr)
+            return fail(MSC_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        msc_status st = set_kernel_attributes(0, 0);
+        if (st != MSC_OK) return st;
+        g_noalloc_base[dev] = ptr;
+    }
+    *out = static_cast<unsigned char *>(g_noalloc_base[dev]);
+    return MSC_OK;
+}
+
+}  // namespace
+
+extern "C" msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32_t n_z,
+                                                 const double *potential_values,
+                                                 const double *kinetic, const double *pkd,
+                                                 const double *wave_c, const double *x, double *y,
+                                                 void *stream)
+{
+    if (!potential_values || !kinetic || !pkd || !wave_c || !x || !y)
+        return fail(MSC_ERR_ARG, "null argument");
+    if (nkx <= 0 || nky <= 0 || n_z < 2 || n_z > msc::kMaxNz)
+        return fail(MSC_ERR_DIMS, "bad dimensions");
+    const int C = nkx * nky;
+    if (C - 1 > msc::kMaxTaps) return fail(MSC_ERR_DIMS, "more than 2049 channels");
+    const int n = n_z;
+    const int kmax = std::max(C - 1, 1);
+    const int ntiles = (C + msc::kTileRows - 1) / msc::kTileRows;
+    // scratch layout (256-byte aligned pieces)
+    size_t off = 0;
+    const size_t o_count = off;  off += round256(sizeof(int));
+    const size_t o_taps = off;   off += round256(sizeof(int2) * (size_t)kmax);
+    const size_t o_v00 = off;    off += round256(sizeof(double) * (size_t)n);
+    const size_t o_vt = off;     off += round256(sizeof(double2) * (size_t)kmax * n);
+    const size_t o_nbr = off;    off += round256(sizeof(int) * (size_t)C * kmax);
+    const size_t o_t0 = off;     off += round256(sizeof(int) * (size_t)ntiles);
+    const size_t o_tn = off;     off += round256(sizeof(int) * (size_t)ntiles);
+    const size_t o_ts = off;     off += round256(sizeof(int) * (size_t)ntiles);
+    const size_t o_spec = off;   off += round256(sizeof(int));
+    const size_t o_bspec = off;  off += round256(sizeof(double2));
+    const size_t o_tmp = off;    off += round256(sizeof(double2) * (size_t)C * n);
+    if (off > kNoAllocScratchBytes)
+        return fail(MSC_ERR_DIMS, "problem needs " + std::to_string(off) +
+                                      " bytes of scratch; the allocation-free entry point has " +
+                                      std::to_string(kNoAllocScratchBytes));
+    unsigned char *base = nullptr;
+    msc_status st = noalloc_scratch(&base);
+    if (st != MSC_OK) return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int *count = reinterpret_cast<int *>(base + o_count);
+    int2 *taps = reinterpret_cast<int2 *>(base + o_taps);
+    double *v00 = reinterpret_cast<double *>(base + o_v00);
+    double2 *Vt = reinterpret_cast<double2 *>(base + o_vt);
+    int *nbr = reinterpret_cast<int *>(base + o_nbr);
+    int *t0 = reinterpret_cast<int *>(base + o_t0);
+    int *tn = reinterpret_cast<int *>(base + o_tn);
+    int *ts = reinterpret_cast<int *>(base + o_ts);
+    int *spec = reinterpret_cast<int *>(base + o_spec);
+    double2 *bspec = reinterpret_cast<double2 *>(base + o_bspec);
+    double2 *tmp = reinterpret_cast<double2 *>(base + o_tmp);
+    const double2 *V = reinterpret_cast<const double2 *>(potential_values);
+
+    k_noalloc_scan_taps<<<1, 1024, 0, s>>>(nkx, nky, n, V, count, taps, v00);
+    MSC_CUDA(cudaGetLastError());
+    int K = 0;
+    MSC_CUDA(cudaMemcpyAsync(&K, count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MSC_CUDA(cudaStreamSynchronize(s));
+    if (K < 0 || K > kmax) return fail(MSC_ERR_CUDA, "tap scan returned an invalid count");
+    k_noalloc_tables<<<256, 256, 0, s>>>(nkx, nky, n, K, V, taps, Vt, nbr, t0, tn, ts, ntiles, spec,
+                                         bspec);
+    MSC_CUDA(cudaGetLastError());
+    const msc::Tiles tiles{t0, tn, ts, ntiles};
+    msc::k_residual_diag<<<ntiles, 256, smem_residual(n), s>>>(
+        tiles, nullptr, n, kinetic, v00, pkd, reinterpret_cast<const double2 *>(wave_c), spec, bspec,
+        reinterpret_cast<const double2 *>(x), tmp, 0);
+    MSC_CUDA(cudaGetLastError());
+    dim3 grid(ntiles, (n + 31) / 32);
+    dim3 block(32, msc::kTileRows);
+    msc::k_coupling<<<grid, block, smem_coupling(std::max(K, 1)), s>>>(
+        tiles, nullptr, n, K, Vt, nbr, reinterpret_cast<const double2 *>(x), tmp, -1.0,
+        reinterpret_cast<double2 *>(y));
+    MSC_CUDA(cudaGetLastError());
+    const size_t cnt = (size_t)C * n;
+    msc::k_scale<<<(unsigned)std::min<size_t>((cnt + 255) / 256, 4096), 256, 0, s>>>(
+        reinterpret_cast<double2 *>(y), cnt, -1.0);
+    MSC_CUDA(cudaGetLastError());
+    return MSC_OK;
+}
