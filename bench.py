@@ -149,7 +149,8 @@ def run_b200(args) -> None:
     from multiscat_b200 import _native as nat
 
     case, systems = build_workload(args.workload)
-    plan = ScatteringPlan(case.v, case.t, systems, rtol=args.rtol, restart=args.restart)
+    plan = ScatteringPlan(case.v, case.t, systems, rtol=args.rtol, restart=args.restart,
+                          precision=args.precision)
     n_solves = len(systems)
     stream = torch.cuda.current_stream()
     dev_time = []
@@ -244,7 +245,7 @@ def run_b200(args) -> None:
             "data": "synthetic (seeded corrugated-Morse potentials built in-process)",
             "config": {"workload": case.name, "systems_per_step": n_solves, "rows": rows,
                        "n_z": n, "taps": plan.n_taps, "restart": args.restart,
-                       "rtol": args.rtol, "precision": "fp64",
+                       "rtol": args.rtol, "precision": args.precision,
                        "l2": "working set (Krylov basis) exceeds the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
             "iterations": iters, "roofline": roof, "kernels": kernels,
@@ -344,6 +345,7 @@ def main() -> None:
     ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg0"])
     ap.add_argument("--rtol", type=float, default=1e-10)
     ap.add_argument("--restart", type=int, default=30)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

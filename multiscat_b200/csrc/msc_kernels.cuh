@@ -1,8 +1,8 @@
-// msc_kernels_fp64.cuh -- FP64 kernels of the close-coupling GMRES solve.
+// msc_kernels.cuh -- kernels of the close-coupling GMRES solve.
 //
 // State layout in HBM: packed channel rows, psi[row][z] complex interleaved
-// (double2), z contiguous.  A row is one diffraction channel of one system;
-// the rows of a system are contiguous.  This is the reference's
+// (double2 / float2), z contiguous.  A row is one diffraction channel of one
+// system; the rows of a system are contiguous.  This is the reference's
 // scattered_state(nz, C) column-major layout (multiscat_gmres.f90:144),
 // extended with a batch of systems.
 //
@@ -13,35 +13,57 @@
 // and the Sherman-Morrison boundary term, as the reference's
 // solve_lower_block does per channel (multiscat_gmres.f90:662-685) and
 // apply_inverse_diagonal does for all channels (_scipy.py:249-259).
+//
+// The Krylov kernels are templated on the vector precision R: double for the
+// plain FP64 solve, float for the inner solve of the mixed form.  Reductions
+// (dot products, norms) always accumulate in FP64 and the GMRES scalars
+// (Hessenberg, Givens, g) are FP64.
 #pragma once
 
 #include "msc_common.cuh"
 
 namespace msc {
 
+template <typename R> struct CT;
+template <> struct CT<double> { using t = double2; };
+template <> struct CT<float> { using t = float2; };
+
+template <typename R>
+__host__ __device__ __forceinline__ typename CT<R>::t mk2(R a, R b)
+{
+    typename CT<R>::t v;
+    v.x = a;
+    v.y = b;
+    return v;
+}
+
 // ---------------------------------------------------------------------------
 // Block-diagonal inverse:  out (=|+=) D^-1 x   on every row of a tile.
 //   xt = E^T x ; s = sum_k en_k xt_k / (pkd + lam_k) ; beta = c s / (1 - c f_n)
 //   yt = (xt + beta en) / (pkd + lam) ; u = E yt
-// Two FP64 GEMMs along z with the tile's 2*kTileRows real columns staged in
-// shared memory; E and E^T stream from L2 (each is n*n doubles).
+// Two GEMMs along z with the tile's 2*TR real columns staged in shared
+// memory; E and E^T stream from L2 (each is n*n values).  TR rows are
+// processed per pass (8 for n <= 512, 4 above, so the two [n][2 TR] staging
+// buffers fit in shared memory).  The diagonal scaling 1/(pkd + lam_k) and
+// the Sherman-Morrison scalar are formed in FP64 for both precisions: near a
+// channel resonance pkd + lam_k cancels, and an FP32 sum would make the FP32
+// preconditioner inconsistent with D.
 // ---------------------------------------------------------------------------
-template <int TR>
+template <int TR, typename R>
 __global__ void __launch_bounds__(256)
-k_block_inverse(Tiles tiles, const int *__restrict__ gate, int n,
-                const double *__restrict__ E, const double *__restrict__ ET,
-                const double *__restrict__ lam, const double *__restrict__ en,
-                const double *__restrict__ row_pkd, const double2 *__restrict__ row_c,
-                const double *__restrict__ row_fn, const double2 *__restrict__ x,
-                double2 *__restrict__ out, int accumulate)
+k_block_inverse(Tiles tiles, const int *__restrict__ gate, int n, const R *__restrict__ E,
+                const R *__restrict__ ET, const double *__restrict__ lam,
+                const double *__restrict__ en, const double *__restrict__ row_pkd,
+                const double2 *__restrict__ row_c, const double *__restrict__ row_fn,
+                const typename CT<R>::t *__restrict__ x, typename CT<R>::t *__restrict__ out,
+                int accumulate)
 {
-    // TR rows are processed per pass (8 for n <= 512, 4 above so that the two
-    // [n][2 TR] staging buffers fit in shared memory).
+    using C2 = typename CT<R>::t;
     constexpr int LD = 2 * TR;       // real columns per z row
     constexpr int HC = TR;           // columns handled per work item (half of LD)
-    extern __shared__ double smem[];
-    double *Xs = smem;               // [n][LD]
-    double *Ys = smem + (size_t)n * LD;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *Xs = reinterpret_cast<R *>(smem_raw);   // [n][LD]
+    R *Ys = Xs + (size_t)n * LD;
     __shared__ double2 beta_s[TR];
 
     const int tile = blockIdx.x;
@@ -51,119 +73,113 @@ k_block_inverse(Tiles tiles, const int *__restrict__ gate, int n,
     const int tile_nrow = tiles.nrow[tile];
 
     for (int pass = 0; pass < tile_nrow; pass += TR) {
-    const int row0 = tile_row0 + pass;
-    const int nrow = min(TR, tile_nrow - pass);
-    if (pass > 0) __syncthreads();
+        const int row0 = tile_row0 + pass;
+        const int nrow = min(TR, tile_nrow - pass);
+        if (pass > 0) __syncthreads();
 
-    for (int idx = threadIdx.x; idx < TR * n; idx += blockDim.x) {
-        int r = idx / n, z = idx - r * n;
-        double2 v = make_double2(0.0, 0.0);
-        if (r < nrow) v = x[(size_t)(row0 + r) * n + z];
-        Xs[z * LD + 2 * r] = v.x;
-        Xs[z * LD + 2 * r + 1] = v.y;
-    }
-    __syncthreads();
+        for (int idx = threadIdx.x; idx < TR * n; idx += blockDim.x) {
+            int r = idx / n, z = idx - r * n;
+            C2 v = mk2<R>(0, 0);
+            if (r < nrow) v = x[(size_t)(row0 + r) * n + z];
+            Xs[z * LD + 2 * r] = v.x;
+            Xs[z * LD + 2 * r + 1] = v.y;
+        }
+        __syncthreads();
 
-    // GEMM 1: Ys[k][c] = sum_z E[z][k] Xs[z][c]
-    for (int item = threadIdx.x; item < 2 * n; item += blockDim.x) {
-        const int k = item >> 1, h = item & 1;
-        double acc[HC];
+        // GEMM 1: Ys[k][c] = sum_z E[z][k] Xs[z][c]
+        for (int item = threadIdx.x; item < 2 * n; item += blockDim.x) {
+            const int k = item >> 1, h = item & 1;
+            R acc[HC];
 #pragma unroll
-        for (int c = 0; c < HC; ++c) acc[c] = 0.0;
-        const double *xs = Xs + h * HC;
-        const double *ek = E + k;
+            for (int c = 0; c < HC; ++c) acc[c] = 0;
+            const R *xs = Xs + h * HC;
+            const R *ek = E + k;
 #pragma unroll 4
-        for (int z = 0; z < n; ++z) {
-            const double e = __ldg(ek + (size_t)z * n);
-            const double2 *xr = reinterpret_cast<const double2 *>(xs + z * LD);
+            for (int z = 0; z < n; ++z) {
+                const R e = __ldg(ek + (size_t)z * n);
+                const R *xr = xs + z * LD;
 #pragma unroll
-            for (int c = 0; c < HC / 2; ++c) {
-                double2 xv = xr[c];
-                acc[2 * c] = fma(e, xv.x, acc[2 * c]);
-                acc[2 * c + 1] = fma(e, xv.y, acc[2 * c + 1]);
+                for (int c = 0; c < HC; ++c) acc[c] = fma(e, xr[c], acc[c]);
             }
-        }
 #pragma unroll
-        for (int c = 0; c < HC; ++c) Ys[k * LD + h * HC + c] = acc[c];
-    }
-    __syncthreads();
+            for (int c = 0; c < HC; ++c) Ys[k * LD + h * HC + c] = acc[c];
+        }
+        __syncthreads();
 
-    // Sherman-Morrison scalar of each row.
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int r = warp; r < TR; r += (blockDim.x >> 5)) {
-        double sr = 0.0, si = 0.0;
-        double pk = 0.0;
-        if (r < nrow) {
-            pk = row_pkd[row0 + r];
-            for (int k = lane; k < n; k += 32) {
-                const double w = en[k] / (pk + lam[k]);
-                sr = fma(w, Ys[k * LD + 2 * r], sr);
-                si = fma(w, Ys[k * LD + 2 * r + 1], si);
-            }
-        }
-        sr = warp_sum(sr);
-        si = warp_sum(si);
-        if (lane == 0) {
-            double2 b = make_double2(0.0, 0.0);
+        // Sherman-Morrison scalar of each row.
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int r = warp; r < TR; r += (blockDim.x >> 5)) {
+            double sr = 0.0, si = 0.0;
             if (r < nrow) {
-                const double2 c = row_c[row0 + r];
-                const double fn = row_fn[row0 + r];
-                const double2 cs = cmul(c, make_double2(sr, si));
-                const double2 den = make_double2(1.0 - c.x * fn, -c.y * fn);
-                b = cdiv(cs, den);
+                const double pk = row_pkd[row0 + r];
+                for (int k = lane; k < n; k += 32) {
+                    const double w = en[k] / (pk + lam[k]);
+                    sr = fma(w, (double)Ys[k * LD + 2 * r], sr);
+                    si = fma(w, (double)Ys[k * LD + 2 * r + 1], si);
+                }
             }
-            beta_s[r] = b;
+            sr = warp_sum(sr);
+            si = warp_sum(si);
+            if (lane == 0) {
+                double2 b = make_double2(0.0, 0.0);
+                if (r < nrow) {
+                    const double2 c = row_c[row0 + r];
+                    const double fn = row_fn[row0 + r];
+                    // beta = c s / (1 - c fn)
+                    b = cdiv(cmul(c, make_double2(sr, si)), make_double2(1.0 - c.x * fn, -c.y * fn));
+                }
+                beta_s[r] = b;
+            }
         }
-    }
-    __syncthreads();
+        __syncthreads();
 
-    for (int idx = threadIdx.x; idx < n * TR; idx += blockDim.x) {
-        const int k = idx / TR, r = idx - k * TR;
-        double inv = 0.0;
-        if (r < nrow) inv = 1.0 / (row_pkd[row0 + r] + lam[k]);
-        const double2 b = beta_s[r];
-        const double ek = en[k];
-        double *y = Ys + k * LD + 2 * r;
-        y[0] = (y[0] + b.x * ek) * inv;
-        y[1] = (y[1] + b.y * ek) * inv;
-    }
-    __syncthreads();
+        for (int idx = threadIdx.x; idx < n * TR; idx += blockDim.x) {
+            const int k = idx / TR, r = idx - k * TR;
+            double inv = 0.0;
+            if (r < nrow) inv = 1.0 / (row_pkd[row0 + r] + lam[k]);
+            const double2 b = beta_s[r];
+            const double ek = en[k];
+            R *y = Ys + k * LD + 2 * r;
+            y[0] = (R)(((double)y[0] + b.x * ek) * inv);
+            y[1] = (R)(((double)y[1] + b.y * ek) * inv);
+        }
+        __syncthreads();
 
-    // GEMM 2: out[z][c] = sum_k ET[k][z] Ys[k][c]
-    for (int item = threadIdx.x; item < 2 * n; item += blockDim.x) {
-        const int z = item >> 1, h = item & 1;
-        double acc[HC];
+        // GEMM 2: out[z][c] = sum_k ET[k][z] Ys[k][c]
+        for (int item = threadIdx.x; item < 2 * n; item += blockDim.x) {
+            const int z = item >> 1, h = item & 1;
+            R acc[HC];
 #pragma unroll
-        for (int c = 0; c < HC; ++c) acc[c] = 0.0;
-        const double *ys = Ys + h * HC;
-        const double *ez = ET + z;
+            for (int c = 0; c < HC; ++c) acc[c] = 0;
+            const R *ys = Ys + h * HC;
+            const R *ez = ET + z;
 #pragma unroll 4
-        for (int k = 0; k < n; ++k) {
-            const double e = __ldg(ez + (size_t)k * n);
-            const double2 *yr = reinterpret_cast<const double2 *>(ys + k * LD);
+            for (int k = 0; k < n; ++k) {
+                const R e = __ldg(ez + (size_t)k * n);
+                const R *yr = ys + k * LD;
 #pragma unroll
-            for (int c = 0; c < HC / 2; ++c) {
-                double2 yv = yr[c];
-                acc[2 * c] = fma(e, yv.x, acc[2 * c]);
-                acc[2 * c + 1] = fma(e, yv.y, acc[2 * c + 1]);
+                for (int c = 0; c < HC; ++c) acc[c] = fma(e, yr[c], acc[c]);
+            }
+#pragma unroll
+            for (int rr = 0; rr < HC / 2; ++rr) {
+                const int r = h * (HC / 2) + rr;
+                if (r < nrow) {
+                    C2 *o = out + (size_t)(row0 + r) * n + z;
+                    C2 v = mk2<R>(acc[2 * rr], acc[2 * rr + 1]);
+                    if (accumulate) {
+                        const C2 prev = *o;
+                        v.x += prev.x;
+                        v.y += prev.y;
+                    }
+                    *o = v;
+                }
             }
         }
-#pragma unroll
-        for (int rr = 0; rr < HC / 2; ++rr) {
-            const int r = h * (HC / 2) + rr;
-            if (r < nrow) {
-                double2 *o = out + (size_t)(row0 + r) * n + z;
-                double2 v = make_double2(acc[2 * rr], acc[2 * rr + 1]);
-                if (accumulate) v = cadd(*o, v);
-                *o = v;
-            }
-        }
-    }
     }  // pass
 }
 
 // ---------------------------------------------------------------------------
-// Residual diagonal part:  out = b - D x  on every row of a tile.
+// Residual diagonal part (FP64):  out = b - D x  on every row of a tile.
 //   D x = T x + (Re V00 + pkd) x - c x(z_n) e_n ; b = b_spec e_n on the
 // specular row.  One FP64 GEMM with the symmetric T.
 // ---------------------------------------------------------------------------
@@ -177,8 +193,8 @@ k_residual_diag(Tiles tiles, const int *__restrict__ gate, int n,
     constexpr int TR = kTileRows;
     constexpr int LD = 2 * TR;
     constexpr int HC = TR;
-    extern __shared__ double smem[];
-    double *Xs = smem;  // [n][LD]
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *Xs = reinterpret_cast<double *>(smem_raw);  // [n][LD]
 
     const int tile = blockIdx.x;
     const int sys = tiles.sys[tile];
@@ -240,12 +256,14 @@ k_residual_diag(Tiles tiles, const int *__restrict__ gate, int n,
 // taps: a circular 2-D convolution over the channel torus at every z.
 // Grid: (tiles, z-chunks of 32); block (32 z, kTileRows rows).
 // ---------------------------------------------------------------------------
+template <typename R>
 __global__ void __launch_bounds__(256)
 k_coupling(Tiles tiles, const int *__restrict__ gate, int n, int K,
-           const double2 *__restrict__ Vt, const int *__restrict__ nbr,
-           const double2 *__restrict__ src, const double2 *__restrict__ in0, double sgn,
-           double2 *__restrict__ out)
+           const typename CT<R>::t *__restrict__ Vt, const int *__restrict__ nbr,
+           const typename CT<R>::t *__restrict__ src, const typename CT<R>::t *__restrict__ in0,
+           R sgn, typename CT<R>::t *__restrict__ out)
 {
+    using C2 = typename CT<R>::t;
     extern __shared__ int nb_s[];   // [kTileRows][K]
     const int tile = blockIdx.x;
     const int sys = tiles.sys[tile];
@@ -260,46 +278,49 @@ k_coupling(Tiles tiles, const int *__restrict__ gate, int n, int K,
     const int z = blockIdx.y * blockDim.x + threadIdx.x;
     if (r >= nrow || z >= n) return;
     const int *nb = nb_s + r * K;
-    double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
+    R ar = 0, ai = 0, br = 0, bi = 0;
     int t = 0;
     for (; t + 1 < K; t += 2) {
         const int j0 = nb[t], j1 = nb[t + 1];
-        const double2 v0 = __ldg(Vt + (size_t)t * n + z);
-        const double2 v1 = __ldg(Vt + (size_t)(t + 1) * n + z);
+        const C2 v0 = Vt[(size_t)t * n + z];
+        const C2 v1 = Vt[(size_t)(t + 1) * n + z];
         if (j0 >= 0) {
-            const double2 s0 = src[(size_t)j0 * n + z];
+            const C2 s0 = src[(size_t)j0 * n + z];
             ar = fma(v0.x, s0.x, ar); ar = fma(-v0.y, s0.y, ar);
             ai = fma(v0.x, s0.y, ai); ai = fma(v0.y, s0.x, ai);
         }
         if (j1 >= 0) {
-            const double2 s1 = src[(size_t)j1 * n + z];
+            const C2 s1 = src[(size_t)j1 * n + z];
             br = fma(v1.x, s1.x, br); br = fma(-v1.y, s1.y, br);
             bi = fma(v1.x, s1.y, bi); bi = fma(v1.y, s1.x, bi);
         }
     }
     if (t < K) {
         const int j0 = nb[t];
-        const double2 v0 = __ldg(Vt + (size_t)t * n + z);
+        const C2 v0 = Vt[(size_t)t * n + z];
         if (j0 >= 0) {
-            const double2 s0 = src[(size_t)j0 * n + z];
+            const C2 s0 = src[(size_t)j0 * n + z];
             ar = fma(v0.x, s0.x, ar); ar = fma(-v0.y, s0.y, ar);
             ai = fma(v0.x, s0.y, ai); ai = fma(v0.y, s0.x, ai);
         }
     }
     const size_t o = (size_t)(row0 + r) * n + z;
-    double2 base = in0 ? in0[o] : make_double2(0.0, 0.0);
-    out[o] = make_double2(base.x + sgn * (ar + br), base.y + sgn * (ai + bi));
+    C2 base = in0 ? in0[o] : mk2<R>(0, 0);
+    out[o] = mk2<R>(base.x + sgn * (ar + br), base.y + sgn * (ai + bi));
 }
 
 // ---------------------------------------------------------------------------
 // Arnoldi reductions.  partial[tile][i] = sum conj(Q_i) W over the tile for
-// i < nvec; slot nvec holds ||W||^2 when with_norm.  One warp per vector.
+// i < nvec; slot nvec holds ||W||^2 when with_norm.  One warp per vector;
+// FP64 accumulation for both precisions.
 // ---------------------------------------------------------------------------
+template <typename R>
 __global__ void __launch_bounds__(256)
-k_dots(Tiles tiles, const int *__restrict__ gate, int n, const double2 *__restrict__ Q,
-       size_t qstride, int nvec, const double2 *__restrict__ W, int with_norm,
+k_dots(Tiles tiles, const int *__restrict__ gate, int n, const typename CT<R>::t *__restrict__ Q,
+       size_t qstride, int nvec, const typename CT<R>::t *__restrict__ W, int with_norm,
        double2 *__restrict__ partial, int pstride)
 {
+    using C2 = typename CT<R>::t;
     const int tile = blockIdx.x;
     const int sys = tiles.sys[tile];
     if (gate && gate[sys] == 0) return;
@@ -310,18 +331,18 @@ k_dots(Tiles tiles, const int *__restrict__ gate, int n, const double2 *__restri
     for (int task = warp; task < ntask; task += (blockDim.x >> 5)) {
         double sr = 0.0, si = 0.0;
         if (task < nvec) {
-            const double2 *q = Q + (size_t)task * qstride + e0;
-            const double2 *w = W + e0;
+            const C2 *q = Q + (size_t)task * qstride + e0;
+            const C2 *w = W + e0;
             for (int e = lane; e < ne; e += 32) {
-                const double2 a = q[e], b = w[e];
-                sr = fma(a.x, b.x, sr); sr = fma(a.y, b.y, sr);
-                si = fma(a.x, b.y, si); si = fma(-a.y, b.x, si);
+                const C2 a = q[e], b = w[e];
+                sr = fma((double)a.x, (double)b.x, sr); sr = fma((double)a.y, (double)b.y, sr);
+                si = fma((double)a.x, (double)b.y, si); si = fma(-(double)a.y, (double)b.x, si);
             }
         } else {
-            const double2 *w = W + e0;
+            const C2 *w = W + e0;
             for (int e = lane; e < ne; e += 32) {
-                const double2 b = w[e];
-                sr = fma(b.x, b.x, sr); sr = fma(b.y, b.y, sr);
+                const C2 b = w[e];
+                sr = fma((double)b.x, (double)b.x, sr); sr = fma((double)b.y, (double)b.y, sr);
             }
         }
         sr = warp_sum(sr);
@@ -354,30 +375,37 @@ k_reduce_partials(const int *__restrict__ sys_tile0, int nsys, const int *__rest
     }
 }
 
-// dst = (W - sum_{i<nvec} Q_i coef[s][i]) * (scale ? scale[s] : 1)
-// (dst may alias W).  Grid: (tiles, chunks); 256 threads.
+// dst = (W - sum_{i<nvec} Q_i coef[s][i]) * (scale ? scale[s] : 1)      (sum_only = 0)
+// dst = sum_{i<nvec} Q_i coef[s][i]                                     (sum_only = 1)
+// (dst may alias W).  coef and scale are FP64; the arithmetic is in R.
+// Grid: (tiles, chunks); 256 threads.
+template <typename R>
 __global__ void __launch_bounds__(256)
-k_update(Tiles tiles, const int *__restrict__ gate, int n, const double2 *__restrict__ Q,
+k_update(Tiles tiles, const int *__restrict__ gate, int n, const typename CT<R>::t *__restrict__ Q,
          size_t qstride, int nvec, const int *__restrict__ nvec_sys,
-         const double2 *__restrict__ coef, int cstride, const double2 *W,
-         const double *__restrict__ scale, double2 *dst, int negate_sum_only)
+         const double2 *__restrict__ coef, int cstride, const typename CT<R>::t *W,
+         const double *__restrict__ scale, typename CT<R>::t *dst, int sum_only)
 {
-    __shared__ double2 cf[kMaxRestart + 1];
+    using C2 = typename CT<R>::t;
+    __shared__ C2 cf[kMaxRestart + 1];
     const int tile = blockIdx.x;
     const int sys = tiles.sys[tile];
     if (gate && gate[sys] == 0) return;
     int nv = nvec_sys ? nvec_sys[sys] : nvec;
-    for (int i = threadIdx.x; i < nv; i += blockDim.x) cf[i] = coef[(size_t)sys * cstride + i];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+        const double2 c = coef[(size_t)sys * cstride + i];
+        cf[i] = mk2<R>((R)c.x, (R)c.y);
+    }
     __syncthreads();
     const size_t e0 = (size_t)tiles.row0[tile] * n;
     const int ne = tiles.nrow[tile] * n;
-    const double sc = scale ? scale[sys] : 1.0;
+    const R sc = scale ? (R)scale[sys] : R(1);
     for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < ne; e += gridDim.y * blockDim.x) {
-        double2 acc = (W && !negate_sum_only) ? W[e0 + e] : make_double2(0.0, 0.0);
+        C2 acc = (W && !sum_only) ? W[e0 + e] : mk2<R>(0, 0);
         for (int i = 0; i < nv; ++i) {
-            const double2 q = Q[(size_t)i * qstride + e0 + e];
-            const double2 c = cf[i];
-            if (negate_sum_only) {
+            const C2 q = Q[(size_t)i * qstride + e0 + e];
+            const C2 c = cf[i];
+            if (sum_only) {
                 acc.x = fma(q.x, c.x, acc.x); acc.x = fma(-q.y, c.y, acc.x);
                 acc.y = fma(q.x, c.y, acc.y); acc.y = fma(q.y, c.x, acc.y);
             } else {
@@ -385,7 +413,44 @@ k_update(Tiles tiles, const int *__restrict__ gate, int n, const double2 *__rest
                 acc.y = fma(-q.x, c.y, acc.y); acc.y = fma(-q.y, c.x, acc.y);
             }
         }
-        dst[e0 + e] = make_double2(acc.x * sc, acc.y * sc);
+        dst[e0 + e] = mk2<R>(acc.x * sc, acc.y * sc);
+    }
+}
+
+// Mixed form: dst32 = src64 * scale[s]  (the normalised FP64 residual as the
+// first FP32 Krylov vector).
+__global__ void __launch_bounds__(256)
+k_convert_scaled(Tiles tiles, const int *__restrict__ gate, int n, const double2 *__restrict__ src,
+                 const double *__restrict__ scale, float2 *__restrict__ dst)
+{
+    const int tile = blockIdx.x;
+    const int sys = tiles.sys[tile];
+    if (gate && gate[sys] == 0) return;
+    const size_t e0 = (size_t)tiles.row0[tile] * n;
+    const int ne = tiles.nrow[tile] * n;
+    const double sc = scale[sys];
+    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < ne; e += gridDim.y * blockDim.x) {
+        const double2 v = src[e0 + e];
+        dst[e0 + e] = make_float2((float)(v.x * sc), (float)(v.y * sc));
+    }
+}
+
+// Mixed form: x64 += u32 (the FP32 correction of one refinement step).
+__global__ void __launch_bounds__(256)
+k_accumulate_f32(Tiles tiles, const int *__restrict__ gate, int n, const float2 *__restrict__ u,
+                 double2 *__restrict__ x)
+{
+    const int tile = blockIdx.x;
+    const int sys = tiles.sys[tile];
+    if (gate && gate[sys] == 0) return;
+    const size_t e0 = (size_t)tiles.row0[tile] * n;
+    const int ne = tiles.nrow[tile] * n;
+    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < ne; e += gridDim.y * blockDim.x) {
+        const float2 d = u[e0 + e];
+        double2 v = x[e0 + e];
+        v.x += (double)d.x;
+        v.y += (double)d.y;
+        x[e0 + e] = v;
     }
 }
 
@@ -404,6 +469,7 @@ struct GmresState {
     double *bnorm;    // [B]  ||b||
     double *resid;    // [B]  last true relative residual
     double *est;      // [B]  GMRES residual estimate (absolute)
+    double *beta0;    // [B]  residual norm at the start of the cycle
     int *active;      // [B]  iterating in this cycle
     int *kcyc;        // [B]  iterations done in this cycle
     int *iters;       // [B]  total iterations
@@ -415,7 +481,7 @@ struct GmresState {
 
 // Cycle start: norm of r = b - A x from the reduced partials (slot 0).
 __global__ void k_cycle_start(GmresState st, int nsys, int m, const double2 *__restrict__ nrm,
-                              int nstride, double rtol, int max_iter)
+                              int nstride, double rtol, int max_iter, int max_cycles)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsys) return;
@@ -435,7 +501,7 @@ __global__ void k_cycle_start(GmresState st, int nsys, int m, const double2 *__r
         st.status[s] = 0;
         return;
     }
-    if (st.iters[s] >= max_iter) {
+    if (st.iters[s] >= max_iter || (max_cycles > 0 && st.cycles[s] >= max_cycles)) {
         st.unfinished[s] = 0;
         st.status[s] = 2;
         return;
@@ -446,12 +512,17 @@ __global__ void k_cycle_start(GmresState st, int nsys, int m, const double2 *__r
     g[0] = make_double2(beta, 0.0);
     for (int i = 1; i <= m; ++i) g[i] = make_double2(0.0, 0.0);
     st.scale[s] = 1.0 / beta;
+    st.beta0[s] = beta;
     atomicAdd(st.counter, 1);
 }
 
 // Arnoldi step j: combine the two CGS passes, append column j of H, apply
-// the previous Givens rotations, make rotation j, update g.
-__global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rtol, int max_iter)
+// the previous Givens rotations, make rotation j, update g.  A system stops
+// iterating in this cycle when its residual estimate reaches
+// max(rtol ||b||, inner_rtol beta0) (inner_rtol > 0 only for the mixed
+// form, whose FP32 inner solve cannot go below its own rounding level).
+__global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rtol, int max_iter,
+                               double inner_rtol)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsys || !st.active[s]) return;
@@ -469,7 +540,6 @@ __global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rto
     }
     const double w2 = h2[j + 1].x;          // ||W'||^2 after the first pass
     const double beta = sqrt(fmax(w2 - proj2, 0.0));
-    // previous rotations
     for (int i = 0; i < j; ++i) {
         const double c = cs[i].x;
         const double2 sv = sn[i];
@@ -478,7 +548,6 @@ __global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rto
         H[i] = cadd(cscale(a, c), cmul(sv, b));
         H[i + 1] = csub(cscale(b, c), cmul(cconj(sv), a));
     }
-    // new rotation from (H[j], beta)
     const double2 a = H[j];
     const double aa = sqrt(cabs2(a));
     const double r = hypot(aa, beta);
@@ -492,7 +561,7 @@ __global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rto
         sv = make_double2(1.0, 0.0);
     } else {
         c = aa / r;
-        sv = cscale(cscale(a, 1.0 / aa), beta / r);   // (a/|a|) * conj(beta) / r, beta real
+        sv = cscale(cscale(a, 1.0 / aa), beta / r);   // (a/|a|) * beta / r, beta real
     }
     cs[j] = make_double2(c, 0.0);
     sn[j] = sv;
@@ -508,7 +577,7 @@ __global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rto
     st.scale[s] = (beta > 0.0) ? 1.0 / beta : 0.0;
     bool stop = false;
     if (!isfinite(est) || !isfinite(beta)) stop = true;
-    if (est <= rtol * st.bnorm[s]) stop = true;
+    if (est <= fmax(rtol * st.bnorm[s], inner_rtol * st.beta0[s])) stop = true;
     if (j + 1 >= m) stop = true;
     if (st.iters[s] >= max_iter) stop = true;
     if (beta <= 1e-300) stop = true;
@@ -554,13 +623,6 @@ __global__ void k_scale(double2 *p, size_t count, double sc)
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
          i += (size_t)gridDim.x * blockDim.x)
         p[i] = make_double2(p[i].x * sc, p[i].y * sc);
-}
-
-__global__ void k_fill_zero(double2 *p, size_t count)
-{
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
-         i += (size_t)gridDim.x * blockDim.x)
-        p[i] = make_double2(0.0, 0.0);
 }
 
 }  // namespace msc

@@ -29,7 +29,7 @@
 #include "../../include/multiscat_b200.h"
 #include "msc_common.cuh"
 #include "msc_eigh.hpp"
-#include "msc_kernels_fp64.cuh"
+#include "msc_kernels.cuh"
 
 namespace {
 
@@ -101,7 +101,14 @@ struct msc_plan {
     // solver state
     DevBuf<double2> X, W, U, TMP, Q, partial;
     DevBuf<double2> H, cs, sn, g, h1, h2, y;
-    DevBuf<double> scale, bnorm, resid, est;
+    DevBuf<double> scale, bnorm, resid, est, beta0;
+    // mixed form: FP32 copies of the operator data and the FP32 Krylov space
+    bool mixed = false;
+    double inner_rtol = 0.0;
+    int max_cycles = 0;
+    DevBuf<float> E32, ET32, lam32, en32, row_pkd32, row_fn32;
+    DevBuf<float2> Vt32, row_c32, Q32, W32, U32;
+    DevBuf<double2> R64;
     DevBuf<int> active, kcyc, iters, cycles, unfinished, status, counter;
     int *counter_host = nullptr;   // pinned
     cudaStream_t stream = nullptr;
@@ -133,7 +140,10 @@ struct msc_plan {
         partial.release(); H.release(); cs.release(); sn.release(); g.release(); h1.release();
         h2.release(); y.release(); scale.release(); bnorm.release(); resid.release();
         est.release(); active.release(); kcyc.release(); iters.release(); cycles.release();
-        unfinished.release(); status.release(); counter.release();
+        unfinished.release(); status.release(); counter.release(); beta0.release();
+        E32.release(); ET32.release(); lam32.release(); en32.release(); row_pkd32.release();
+        row_fn32.release(); Vt32.release(); row_c32.release(); Q32.release(); W32.release();
+        U32.release(); R64.release();
     }
 
     msc::Tiles tiles() const
@@ -144,7 +154,7 @@ struct msc_plan {
     {
         msc::GmresState s;
         s.H = H.p; s.cs = cs.p; s.sn = sn.p; s.g = g.p; s.h1 = h1.p; s.h2 = h2.p; s.y = y.p;
-        s.scale = scale.p; s.bnorm = bnorm.p; s.resid = resid.p; s.est = est.p;
+        s.scale = scale.p; s.bnorm = bnorm.p; s.resid = resid.p; s.est = est.p; s.beta0 = beta0.p;
         s.active = active.p; s.kcyc = kcyc.p; s.iters = iters.p; s.cycles = cycles.p;
         s.unfinished = unfinished.p; s.status = status.p; s.counter = counter.p;
         return s;
@@ -164,22 +174,65 @@ cudaError_t upload(DevBuf<T> &buf, const std::vector<T> &h)
 
 int block_inverse_rows(int n) { return n <= msc::kWideNz ? 8 : 4; }
 size_t smem_block_inverse(int n) { return (size_t)2 * n * 2 * block_inverse_rows(n) * sizeof(double); }
+void launch_block_inverse(msc_plan *p, const int *gate, const double2 *x, double2 *out, int acc,
+                          cudaStream_t st);
 size_t smem_residual(int n) { return (size_t)n * 2 * msc::kTileRows * sizeof(double); }
 size_t smem_coupling(int K) { return (size_t)msc::kTileRows * K * sizeof(int); }
 
-// --- kernel launch wrappers (all on plan->stream) ---------------------------
+// --- kernel launch wrappers ---------------------------------------------------
+
+template <typename R>
+struct OpData;   // operator data of one precision
+
+template <>
+struct OpData<double> {
+    static const double *E(msc_plan *p) { return p->E.p; }
+    static const double *ET(msc_plan *p) { return p->ET.p; }
+    static const double *lam(msc_plan *p) { return p->lam.p; }
+    static const double *en(msc_plan *p) { return p->en.p; }
+    static const double *pkd(msc_plan *p) { return p->row_pkd.p; }
+    static const double *fn(msc_plan *p) { return p->row_fn.p; }
+    static const double2 *c(msc_plan *p) { return p->row_c.p; }
+    static const double2 *Vt(msc_plan *p) { return p->Vt.p; }
+};
+
+template <>
+struct OpData<float> {
+    static const float *E(msc_plan *p) { return p->E32.p; }
+    static const float *ET(msc_plan *p) { return p->ET32.p; }
+    static const float *lam(msc_plan *p) { return p->lam32.p; }
+    static const float *en(msc_plan *p) { return p->en32.p; }
+    static const float *pkd(msc_plan *p) { return p->row_pkd32.p; }
+    static const float *fn(msc_plan *p) { return p->row_fn32.p; }
+    static const float2 *c(msc_plan *p) { return p->row_c32.p; }
+    static const float2 *Vt(msc_plan *p) { return p->Vt32.p; }
+};
+
+template <typename R>
+using C2 = typename msc::CT<R>::t;
+
+template <typename R>
+size_t smem_block_inverse_t(int n) { return (size_t)2 * n * 2 * block_inverse_rows(n) * sizeof(R); }
+
+template <typename R>
+void launch_block_inverse_t(msc_plan *p, const int *gate, const C2<R> *x, C2<R> *out, int acc,
+                            cudaStream_t st)
+{
+    using D = OpData<R>;
+    if (block_inverse_rows(p->n) == 8)
+        msc::k_block_inverse<8, R><<<p->ntiles, 256, smem_block_inverse_t<R>(p->n), st>>>(
+            p->tiles(), gate, p->n, D::E(p), D::ET(p), p->lam.p, p->en.p, p->row_pkd.p,
+            p->row_c.p, p->row_fn.p, x, out, acc);
+    else
+        msc::k_block_inverse<4, R><<<p->ntiles, 256, smem_block_inverse_t<R>(p->n), st>>>(
+            p->tiles(), gate, p->n, D::E(p), D::ET(p), p->lam.p, p->en.p, p->row_pkd.p,
+            p->row_c.p, p->row_fn.p, x, out, acc);
+}
 
 void launch_block_inverse(msc_plan *p, const int *gate, const double2 *x, double2 *out, int acc,
                           cudaStream_t st)
 {
-    if (block_inverse_rows(p->n) == 8)
-        msc::k_block_inverse<8><<<p->ntiles, 256, smem_block_inverse(p->n), st>>>(
-            p->tiles(), gate, p->n, p->E.p, p->ET.p, p->lam.p, p->en.p, p->row_pkd.p, p->row_c.p,
-            p->row_fn.p, x, out, acc);
-    else
-        msc::k_block_inverse<4><<<p->ntiles, 256, smem_block_inverse(p->n), st>>>(
-            p->tiles(), gate, p->n, p->E.p, p->ET.p, p->lam.p, p->en.p, p->row_pkd.p, p->row_c.p,
-            p->row_fn.p, x, out, acc);
+    launch_block_inverse_t<double>(p, gate, x, out, acc, st);
 }
 
 void launch_residual_diag(msc_plan *p, const int *gate, const double2 *x, double2 *out, int with_b,
@@ -190,21 +243,28 @@ void launch_residual_diag(msc_plan *p, const int *gate, const double2 *x, double
         p->sys_bspec.p, x, out, with_b);
 }
 
-void launch_coupling(msc_plan *p, const int *gate, const double2 *src, const double2 *in0,
-                     double sgn, double2 *out, cudaStream_t st)
+template <typename R>
+void launch_coupling_t(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
+                       C2<R> *out, cudaStream_t st)
 {
     dim3 grid(p->ntiles, (p->n + 31) / 32);
     dim3 block(32, msc::kTileRows);
-    msc::k_coupling<<<grid, block, smem_coupling(std::max(p->K, 1)), st>>>(
-        p->tiles(), gate, p->n, p->K, p->Vt.p, p->nbr.p, src, in0, sgn, out);
+    msc::k_coupling<R><<<grid, block, smem_coupling(std::max(p->K, 1)), st>>>(
+        p->tiles(), gate, p->n, p->K, OpData<R>::Vt(p), p->nbr.p, src, in0, sgn, out);
 }
 
-void launch_dots(msc_plan *p, const int *gate, int nvec, const double2 *W, int with_norm,
-                 cudaStream_t st)
+void launch_coupling(msc_plan *p, const int *gate, const double2 *src, const double2 *in0,
+                     double sgn, double2 *out, cudaStream_t st)
 {
-    msc::k_dots<<<p->ntiles, 256, 0, st>>>(p->tiles(), gate, p->n, p->Q.p,
-                                            (size_t)p->R * p->n, nvec, W, with_norm,
-                                            p->partial.p, p->pstride);
+    launch_coupling_t<double>(p, gate, src, in0, sgn, out, st);
+}
+
+template <typename R>
+void launch_dots_t(msc_plan *p, const int *gate, const C2<R> *Q, int nvec, const C2<R> *W,
+                   int with_norm, cudaStream_t st)
+{
+    msc::k_dots<R><<<p->ntiles, 256, 0, st>>>(p->tiles(), gate, p->n, Q, (size_t)p->R * p->n, nvec,
+                                               W, with_norm, p->partial.p, p->pstride);
 }
 
 void launch_reduce(msc_plan *p, const int *gate, int nslot, double2 *out, cudaStream_t st)
@@ -213,33 +273,30 @@ void launch_reduce(msc_plan *p, const int *gate, int nslot, double2 *out, cudaSt
                                                   p->pstride, nslot, out, p->m + 2);
 }
 
+dim3 elementwise_grid(msc_plan *p)
+{
+    return dim3(p->ntiles, (msc::kTileRows * p->n + 255) / 256);
+}
+
+template <typename R>
+void launch_update_t(msc_plan *p, const int *gate, const C2<R> *Q, int nvec, const int *nvec_sys,
+                     const double2 *coef, int cstride, const C2<R> *W, const double *scale,
+                     C2<R> *dst, int sum_only, cudaStream_t st)
+{
+    msc::k_update<R><<<elementwise_grid(p), 256, 0, st>>>(p->tiles(), gate, p->n, Q,
+                                                           (size_t)p->R * p->n, nvec, nvec_sys,
+                                                           coef, cstride, W, scale, dst, sum_only);
+}
+
 void launch_update(msc_plan *p, const int *gate, int nvec, const int *nvec_sys,
                    const double2 *coef, int cstride, const double2 *W, const double *scale,
                    double2 *dst, int sum_only, cudaStream_t st)
 {
-    int chunks = (msc::kTileRows * p->n + 255) / 256;
-    dim3 grid(p->ntiles, chunks);
-    msc::k_update<<<grid, 256, 0, st>>>(p->tiles(), gate, p->n, p->Q.p, (size_t)p->R * p->n,
-                                         nvec, nvec_sys, coef, cstride, W, scale, dst, sum_only);
+    launch_update_t<double>(p, gate, p->Q.p, nvec, nvec_sys, coef, cstride, W, scale, dst,
+                            sum_only, st);
 }
 
 int sys_blocks(int B) { return (B + 127) / 128; }
-
-// Cycle start: r = b - A x into Q0, its norm, activation, Q0 /= ||r||.
-void record_cycle_start(msc_plan *p, cudaStream_t st)
-{
-    double2 *Q0 = p->Q.p;
-    cudaMemsetAsync(p->counter.p, 0, sizeof(int), st);
-    launch_residual_diag(p, p->unfinished.p, p->X.p, p->TMP.p, 1, st);
-    launch_coupling(p, p->unfinished.p, p->X.p, p->TMP.p, -1.0, Q0, st);
-    launch_dots(p, p->unfinished.p, 0, Q0, 1, st);
-    launch_reduce(p, p->unfinished.p, 1, p->h2.p, st);
-    msc::k_cycle_start<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m, p->h2.p,
-                                                         p->m + 2, p->desc.rtol,
-                                                         p->desc.max_iterations);
-    launch_update(p, p->active.p, 0, nullptr, p->h1.p, p->m + 2, Q0, p->scale.p, Q0, 0, st);
-    cudaMemcpyAsync(p->counter_host, p->counter.p, sizeof(int), cudaMemcpyDeviceToHost, st);
-}
 
 cudaEvent_t tev_at(msc_plan *p, int kind, int slot, int which)
 {
@@ -252,38 +309,80 @@ void mark(msc_plan *p, int kind, int slot, int which, cudaStream_t st)
     cudaEventRecordWithFlags(tev_at(p, kind, slot, which), st, cudaEventRecordExternal);
 }
 
-// m Arnoldi steps (CGS2) and the solution update x += M (Q y).
-void record_cycle_iterations(msc_plan *p, cudaStream_t st)
+// Cycle start (both forms): r = b - A x in FP64, its norm, activation.
+// FP64 form: r lands in Q0 and is scaled in place.  Mixed form: r lands in
+// R64 and its normalised FP32 copy becomes the first inner Krylov vector, so
+// every cycle is one step of iterative refinement with an FP64 residual.
+void record_cycle_start(msc_plan *p, cudaStream_t st)
+{
+    double2 *r64 = p->mixed ? p->R64.p : p->Q.p;
+    cudaMemsetAsync(p->counter.p, 0, sizeof(int), st);
+    launch_residual_diag(p, p->unfinished.p, p->X.p, p->TMP.p, 1, st);
+    launch_coupling(p, p->unfinished.p, p->X.p, p->TMP.p, -1.0, r64, st);
+    launch_dots_t<double>(p, p->unfinished.p, p->Q.p, 0, r64, 1, st);
+    launch_reduce(p, p->unfinished.p, 1, p->h2.p, st);
+    msc::k_cycle_start<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m, p->h2.p,
+                                                         p->m + 2, p->desc.rtol,
+                                                         p->desc.max_iterations, p->max_cycles);
+    if (p->mixed) {
+        msc::k_convert_scaled<<<elementwise_grid(p), 256, 0, st>>>(p->tiles(), p->active.p, p->n,
+                                                                   r64, p->scale.p, p->Q32.p);
+    } else {
+        launch_update(p, p->active.p, 0, nullptr, p->h1.p, p->m + 2, r64, p->scale.p, r64, 0, st);
+    }
+    cudaMemcpyAsync(p->counter_host, p->counter.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+}
+
+// m Arnoldi steps (CGS2) in precision R and the solution update x += M (Q y).
+template <typename R>
+void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t st)
 {
     const size_t vs = (size_t)p->R * p->n;
     const bool tm = p->timing;
+    const double inner = p->mixed ? p->inner_rtol : 0.0;
     for (int j = 0; j < p->m; ++j) {
-        double2 *Qj = p->Q.p + (size_t)j * vs;
-        double2 *Qn = p->Q.p + (size_t)(j + 1) * vs;
+        C2<R> *Qj = Q + (size_t)j * vs;
+        C2<R> *Qn = Q + (size_t)(j + 1) * vs;
         if (tm) mark(p, 0, j, 0, st);
-        launch_block_inverse(p, p->active.p, Qj, p->U.p, 0, st);
+        launch_block_inverse_t<R>(p, p->active.p, Qj, U, 0, st);
         if (tm) mark(p, 0, j, 1, st);
         if (tm) mark(p, 1, j, 0, st);
-        launch_coupling(p, p->active.p, p->U.p, Qj, 1.0, p->W.p, st);
+        launch_coupling_t<R>(p, p->active.p, U, Qj, R(1), W, st);
         if (tm) mark(p, 1, j, 1, st);
-        launch_dots(p, p->active.p, j + 1, p->W.p, 0, st);
+        launch_dots_t<R>(p, p->active.p, Q, j + 1, W, 0, st);
         launch_reduce(p, p->active.p, j + 1, p->h1.p, st);
-        launch_update(p, p->active.p, j + 1, nullptr, p->h1.p, p->m + 2, p->W.p, nullptr, p->W.p,
-                      0, st);
-        launch_dots(p, p->active.p, j + 1, p->W.p, 1, st);
+        launch_update_t<R>(p, p->active.p, Q, j + 1, nullptr, p->h1.p, p->m + 2, W, nullptr, W, 0,
+                           st);
+        launch_dots_t<R>(p, p->active.p, Q, j + 1, W, 1, st);
         launch_reduce(p, p->active.p, j + 2, p->h2.p, st);
         msc::k_arnoldi_step<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m, j,
                                                               p->desc.rtol,
-                                                              p->desc.max_iterations);
-        launch_update(p, p->active.p, j + 1, nullptr, p->h2.p, p->m + 2, p->W.p, p->scale.p, Qn,
-                      0, st);
+                                                              p->desc.max_iterations, inner);
+        launch_update_t<R>(p, p->active.p, Q, j + 1, nullptr, p->h2.p, p->m + 2, W, p->scale.p, Qn,
+                           0, st);
     }
     msc::k_trisolve<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m);
-    launch_update(p, p->kcyc.p, 0, p->kcyc.p, p->y.p, p->m, nullptr, nullptr, p->U.p, 1, st);
+    launch_update_t<R>(p, p->kcyc.p, Q, 0, p->kcyc.p, p->y.p, p->m, nullptr, nullptr, U, 1, st);
     if (tm) mark(p, 0, p->m, 0, st);
-    launch_block_inverse(p, p->kcyc.p, p->U.p, p->X.p, 1, st);
+    if (p->mixed) {
+        launch_block_inverse_t<R>(p, p->kcyc.p, U, W, 0, st);
+    } else {
+        launch_block_inverse_t<R>(p, p->kcyc.p, U, reinterpret_cast<C2<R> *>(p->X.p), 1, st);
+    }
     if (tm) mark(p, 0, p->m, 1, st);
+    if (p->mixed) {
+        msc::k_accumulate_f32<<<elementwise_grid(p), 256, 0, st>>>(
+            p->tiles(), p->kcyc.p, p->n, reinterpret_cast<const float2 *>(W), p->X.p);
+    }
     cudaMemcpyAsync(p->kcyc_host, p->kcyc.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, st);
+}
+
+void record_cycle_iterations(msc_plan *p, cudaStream_t st)
+{
+    if (p->mixed)
+        record_iterations_t<float>(p, p->Q32.p, p->W32.p, p->U32.p, st);
+    else
+        record_iterations_t<double>(p, p->Q.p, p->W.p, p->U.p, st);
 }
 
 // Kernel nodes in a captured graph (launch accounting).
@@ -348,13 +447,23 @@ msc_status capture(msc_plan *p, void (*rec)(msc_plan *, cudaStream_t), cudaGraph
 
 msc_status set_kernel_attributes(int n, int K)
 {
-    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse<8, double>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_block_inverse(msc::kWideNz)));
-    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse<4, double>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_block_inverse(msc::kMaxNz)));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse<8, float>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_block_inverse(msc::kWideNz)));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_block_inverse<4, float>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_block_inverse(msc::kMaxNz)));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_coupling(msc::kMaxTaps)));
     MSC_CUDA(cudaFuncSetAttribute(msc::k_residual_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_residual(msc::kMaxNz)));
-    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_coupling(msc::kMaxTaps)));
     (void)n;
     (void)K;
@@ -434,15 +543,34 @@ msc_status finalize(msc_plan *p)
     MSC_CUDA(upload(p->sys_tile0, p->sys_tile0_h));
     MSC_CUDA(upload(p->row_sys, p->row_sys_h));
     MSC_CUDA(upload(p->bnorm, bn));
+    if (p->mixed) {
+        std::vector<float> pkd32(p->R), fn32(p->R);
+        std::vector<float2> c32(p->R);
+        for (int r = 0; r < p->R; ++r) {
+            pkd32[r] = (float)pkd[r];
+            fn32[r] = (float)fn[r];
+            c32[r] = make_float2((float)rc[r].x, (float)rc[r].y);
+        }
+        MSC_CUDA(upload(p->row_pkd32, pkd32));
+        MSC_CUDA(upload(p->row_fn32, fn32));
+        MSC_CUDA(upload(p->row_c32, c32));
+    }
 
     const size_t vs = (size_t)p->R * n;
     const int m = p->m;
     p->pstride = m + 2;
     MSC_CUDA(p->X.alloc(vs));
-    MSC_CUDA(p->W.alloc(vs));
-    MSC_CUDA(p->U.alloc(vs));
     MSC_CUDA(p->TMP.alloc(vs));
-    MSC_CUDA(p->Q.alloc(vs * (m + 1)));
+    if (p->mixed) {
+        MSC_CUDA(p->R64.alloc(vs));
+        MSC_CUDA(p->Q32.alloc(vs * (m + 1)));
+        MSC_CUDA(p->W32.alloc(vs));
+        MSC_CUDA(p->U32.alloc(vs));
+    } else {
+        MSC_CUDA(p->W.alloc(vs));
+        MSC_CUDA(p->U.alloc(vs));
+        MSC_CUDA(p->Q.alloc(vs * (m + 1)));
+    }
     MSC_CUDA(p->partial.alloc((size_t)p->ntiles * p->pstride));
     MSC_CUDA(p->H.alloc((size_t)p->B * (m + 1) * m));
     MSC_CUDA(p->cs.alloc((size_t)p->B * m));
@@ -453,6 +581,7 @@ msc_status finalize(msc_plan *p)
     MSC_CUDA(p->y.alloc((size_t)p->B * m));
     MSC_CUDA(p->scale.alloc(p->B));
     MSC_CUDA(p->resid.alloc(p->B));
+    MSC_CUDA(p->beta0.alloc(p->B));
     MSC_CUDA(p->est.alloc(p->B));
     MSC_CUDA(p->active.alloc(p->B));
     MSC_CUDA(p->kcyc.alloc(p->B));
@@ -494,8 +623,12 @@ msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc)
     if (desc->restart < 1 || desc->restart > msc::kMaxRestart || desc->max_iterations < 1 ||
         !(desc->rtol > 0.0))
         return fail(MSC_ERR_ARG, "bad solver options");
-    if (desc->precision != MSC_PRECISION_FP64)
-        return fail(MSC_ERR_NOT_BUILT, "only MSC_PRECISION_FP64 is available in this build");
+    if (desc->precision != MSC_PRECISION_FP64 && desc->precision != MSC_PRECISION_MIXED)
+        return fail(MSC_ERR_ARG, "unknown precision");
+    if (desc->precision == MSC_PRECISION_MIXED &&
+        (desc->inner_restart < 0 || desc->inner_restart > msc::kMaxRestart || desc->inner_rtol < 0.0 ||
+         desc->max_refinements < 0))
+        return fail(MSC_ERR_ARG, "bad mixed-precision options");
     msc_plan *p = new (std::nothrow) msc_plan();
     if (!p) return fail(MSC_ERR_CUDA, "host allocation failed");
     p->desc = *desc;
@@ -504,6 +637,12 @@ msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc)
     p->nky = desc->nky;
     p->B = desc->n_systems;
     p->m = desc->restart;
+    p->mixed = desc->precision == MSC_PRECISION_MIXED;
+    if (p->mixed) {
+        if (desc->inner_restart > 0) p->m = desc->inner_restart;
+        p->inner_rtol = desc->inner_rtol > 0.0 ? desc->inner_rtol : 1e-5;
+        p->max_cycles = desc->max_refinements > 0 ? desc->max_refinements : 30;
+    }
     p->sys.resize(p->B);
     msc_status st = set_kernel_attributes(p->n, 0);
     if (st != MSC_OK) { delete p; return st; }
@@ -578,6 +717,19 @@ msc_status msc_plan_set_potential(msc_plan *p, const double *potential_values, c
     } else {
         std::vector<double2> dummy(1, double2{0.0, 0.0});
         MSC_CUDA(upload(p->Vt, dummy));
+    }
+    if (p->mixed) {
+        auto to32 = [](const std::vector<double> &v) {
+            return std::vector<float>(v.begin(), v.end());
+        };
+        MSC_CUDA(upload(p->E32, to32(p->E_host)));
+        MSC_CUDA(upload(p->ET32, to32(ET)));
+        MSC_CUDA(upload(p->lam32, to32(p->lam_host)));
+        MSC_CUDA(upload(p->en32, to32(p->en_host)));
+        std::vector<float2> vt32(std::max<size_t>(p->Vt_host.size(), 1), make_float2(0.f, 0.f));
+        for (size_t i = 0; i < p->Vt_host.size(); ++i)
+            vt32[i] = make_float2((float)p->Vt_host[i].x, (float)p->Vt_host[i].y);
+        MSC_CUDA(upload(p->Vt32, vt32));
     }
     p->potential_set = true;
     return MSC_OK;
