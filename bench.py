@@ -164,7 +164,7 @@ def run_b200(args) -> None:
     torch.cuda.synchronize()
     iters = res.iterations.tolist()
 
-    plan.enable_kernel_timing(True)
+    plan.enable_kernel_timing(not args.no_kernel_timing)
     barrier()
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
@@ -249,6 +249,7 @@ def run_b200(args) -> None:
                        "l2": "working set (Krylov basis) exceeds the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
             "iterations": iters, "roofline": roof, "kernels": kernels,
+            "autotune": plan.tuning_report(),
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
             "gpu_launches": plan.launches_per_solve(res) * args.steps,
         }
@@ -348,6 +349,8 @@ def main() -> None:
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-kernel-timing", action="store_true",
+                    help="time the steps without the in-graph event pairs")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

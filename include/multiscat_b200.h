@@ -64,6 +64,9 @@ typedef struct {
     int32_t inner_restart;  /* mixed: inner FP32 restart length (0 = restart)   */
     double inner_rtol;      /* mixed: inner relative tolerance (0 = 1e-4)       */
     int32_t max_refinements;/* mixed: outer FP64 refinement steps (0 = 30)      */
+    int32_t flags;          /* bit 0: mixed form without the tcgen05 kernel;
+                               bit 1: keep the tcgen05 kernel even when the
+                               autotuner times the SIMT kernel faster          */
 } msc_plan_desc;
 
 typedef struct msc_plan msc_plan;
@@ -162,6 +165,18 @@ msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32_t n_z,
                                       const double *potential_values, const double *kinetic,
                                       const double *pkd, const double *wave_c, const double *x,
                                       double *y, void *stream);
+
+/* Mixed-precision plans: y = D^-1 x with the FP32 kernel the inner solve
+ * uses (tcgen05 BF16x3 when available), x and y complex FP32 packed rows. */
+msc_status msc_debug_apply_block_inverse_f32(msc_plan *plan, const float *x, float *y, void *stream);
+
+/* Tile width N of the tcgen05 block inverse the plan uses (0 = not used).
+ * Valid after the first msc_solve or debug call. */
+int msc_plan_uses_tensor_cores(const msc_plan *plan);
+
+/* JSON text of the autotuner's timings (microseconds per candidate kernel)
+ * and choices for this plan; owned by the plan, valid until the next call. */
+const char *msc_plan_tuning_report(msc_plan *plan);
 
 /* |S_G0|^2 per channel from psi[C][n_z] (device pointers), for one system. */
 msc_status msc_intensities(msc_plan *plan, int32_t s, const double *psi, double *intensities,

@@ -19,7 +19,8 @@ EXPORTED = (
     "msc_solve", "msc_plan_total_rows", "msc_run_multiscat", "msc_debug_apply_coupling",
     "msc_debug_apply_block_inverse", "msc_debug_apply_operator", "msc_intensities",
     "msc_last_error", "msc_version", "msc_plan_get_info", "msc_plan_set_kernel_timing",
-    "msc_plan_kernel_timing", "msc_apply_operator_noalloc",
+    "msc_plan_kernel_timing", "msc_apply_operator_noalloc", "msc_debug_apply_block_inverse_f32",
+    "msc_plan_uses_tensor_cores", "msc_plan_tuning_report",
 )
 
 MSC_OK = 0
@@ -48,6 +49,7 @@ class PlanDesc(ctypes.Structure):
         ("inner_restart", ctypes.c_int32),
         ("inner_rtol", ctypes.c_double),
         ("max_refinements", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
     ]
 
 
@@ -112,7 +114,7 @@ def load() -> ctypes.CDLL:
                                       ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                       ctypes.POINTER(ctypes.c_int)]
     for name in ("msc_debug_apply_coupling", "msc_debug_apply_block_inverse",
-                 "msc_debug_apply_operator"):
+                 "msc_debug_apply_operator", "msc_debug_apply_block_inverse_f32"):
         f = getattr(lib, name)
         f.restype = ctypes.c_int
         f.argtypes = [_vp, _vp, _vp, _vp]
@@ -127,6 +129,10 @@ def load() -> ctypes.CDLL:
     lib.msc_apply_operator_noalloc.restype = ctypes.c_int
     lib.msc_apply_operator_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    lib.msc_plan_tuning_report.restype = ctypes.c_char_p
+    lib.msc_plan_tuning_report.argtypes = [_vp]
+    lib.msc_plan_uses_tensor_cores.restype = ctypes.c_int
+    lib.msc_plan_uses_tensor_cores.argtypes = [_vp]
     lib.msc_last_error.restype = ctypes.c_char_p
     lib.msc_last_error.argtypes = []
     lib.msc_version.restype = ctypes.c_char_p

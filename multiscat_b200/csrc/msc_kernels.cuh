@@ -310,6 +310,148 @@ k_coupling(Tiles tiles, const int *__restrict__ gate, int n, int K,
 }
 
 // ---------------------------------------------------------------------------
+// Channel coupling with shared-memory halo tiles (the hot form of k_coupling).
+//
+// A block owns an 8 x BX patch of torus positions of ONE system and ZC
+// consecutive z.  It stages the patch plus a halo of HX (x) and HY (y)
+// positions -- the reach of the coupling taps -- for its z range in shared
+// memory (absent channels, i.e. positions outside a truncated channel set,
+// read as zero; positions wrap around the torus exactly as the reference's
+// modulo(G_j - G_i, n) does).  Each thread keeps one column of 8 + 2 HY halo
+// values in registers and produces 8 outputs along y for one (x, z):
+// for every tap (sdx, sdy) in the window it issues 8 complex FMAs from
+// registers, so a halo value loaded once serves up to 2 HY + 1 taps.
+//   out[r] = in0[r] + sgn * sum_t V_t(z) src[pos(r) - delta_t](z)
+// ---------------------------------------------------------------------------
+struct CouplingTiles {
+    const int *work;          // [nwork][3]: system, x0, y0
+    const int *pos_row;       // [B][nkx * nky]: row of each torus position, -1 if absent
+    const int *tap_window;    // [(2 HX + 1) * (2 HY + 1)]: tap index per signed offset, -1 if none
+    int nwork, nkx, nky, hx;  // hx = HX (runtime); HY is the template parameter
+    int ntaps;                // K
+};
+
+template <int HY, int BX, int ZC, int YS, typename R>
+__global__ void __launch_bounds__(BX * ZC * (8 / YS))
+k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
+                const typename CT<R>::t *__restrict__ Vt, const typename CT<R>::t *__restrict__ src,
+                const typename CT<R>::t *__restrict__ in0, R sgn, typename CT<R>::t *__restrict__ out)
+{
+    // YS outputs along y per thread; 8 / YS threads share one (x, z) column.
+    using C2 = typename CT<R>::t;
+    constexpr int BY = 8;
+    constexpr int HYW = BY + 2 * HY;
+    constexpr int WY = 2 * HY + 1;
+    constexpr int NT = BX * ZC * (BY / YS);
+    constexpr int CW = YS + 2 * HY;              // halo values one thread keeps per column
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int HX = ct.hx;
+    const int HXW = BX + 2 * HX;
+    const int nwin = (2 * HX + 1) * WY;
+    C2 *halo = reinterpret_cast<C2 *>(smem_raw);                              // [HXW][HYW][ZC]
+    C2 *vw = halo + (size_t)HXW * HYW * ZC;                                   // [window cell][ZC]
+    int *rows = reinterpret_cast<int *>(vw + (size_t)nwin * ZC);              // [HXW][HYW]
+    __shared__ int colany[BX];
+
+    const int w = blockIdx.x;
+    const int s = ct.work[3 * w];
+    if (gate && gate[s] == 0) return;
+    const int x0 = ct.work[3 * w + 1], y0 = ct.work[3 * w + 2];
+    const int z0 = blockIdx.y * ZC;
+    const int nkx = ct.nkx, nky = ct.nky;
+    const int *pr = ct.pos_row + (size_t)s * nkx * nky;
+    // tap values of this z range, one row per window cell (zero where no tap)
+    for (int i = threadIdx.x; i < nwin * ZC; i += NT) {
+        const int cell = i / ZC, z = z0 + (i % ZC);
+        const int t = ct.tap_window[cell];
+        vw[i] = (t >= 0 && z < n) ? Vt[(size_t)t * n + z] : mk2<R>(0, 0);
+    }
+    // source row of every halo position (absent channels: -1)
+    const int npos = HXW * HYW;
+    for (int pidx = threadIdx.x; pidx < npos; pidx += NT) {
+        const int hy = pidx % HYW, hx = pidx / HYW;
+        int gx = (x0 + hx - HX) % nkx;
+        if (gx < 0) gx += nkx;
+        int gy = (y0 + hy - HY) % nky;
+        if (gy < 0) gy += nky;
+        rows[pidx] = pr[gx * nky + gy];
+    }
+    if (threadIdx.x < BX) {
+        const int gx = x0 + threadIdx.x;
+        int any = 0;
+        if (gx < nkx)
+            for (int y = 0; y < BY && !any; ++y)
+                any = (y0 + y < nky) && pr[gx * nky + y0 + y] >= 0;
+        colany[threadIdx.x] = any;
+    }
+    __syncthreads();
+    constexpr int kU = 8;
+    const int total = npos * ZC;
+    for (int base = threadIdx.x; base < total; base += NT * kU) {
+        C2 v[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int idx = base + u * NT;
+            v[u] = mk2<R>(0, 0);
+            if (idx < total) {
+                const int row = rows[idx / ZC];
+                const int z = z0 + (idx % ZC);
+                if (row >= 0 && z < n) v[u] = src[(size_t)row * n + z];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int idx = base + u * NT;
+            if (idx < total) halo[idx] = v[u];
+        }
+    }
+    __syncthreads();
+
+    const int zl = threadIdx.x % ZC;
+    const int tx = (threadIdx.x / ZC) % BX;
+    const int ysub = threadIdx.x / (ZC * BX);      // which YS-slice of the 8 y outputs
+    const int z = z0 + zl;
+    if (x0 + tx >= nkx || z >= n || !colany[tx]) return;
+    R ar[YS], ai[YS];
+#pragma unroll
+    for (int y = 0; y < YS; ++y) {
+        ar[y] = 0;
+        ai[y] = 0;
+    }
+    for (int sdx = -HX; sdx <= HX; ++sdx) {
+        const int hx = tx - sdx + HX;
+        const C2 *colp = halo + ((size_t)hx * HYW + ysub * YS) * ZC + zl;
+        C2 col[CW];
+#pragma unroll
+        for (int i = 0; i < CW; ++i) col[i] = colp[(size_t)i * ZC];
+        const C2 *vrow = vw + (size_t)(sdx + HX) * WY * ZC + zl;
+#pragma unroll
+        for (int sdy = -HY; sdy <= HY; ++sdy) {
+            const C2 v = vrow[(sdy + HY) * ZC];
+#pragma unroll
+            for (int y = 0; y < YS; ++y) {
+                const C2 q = col[y - sdy + HY];
+                ar[y] = fma(v.x, q.x, fma(-v.y, q.y, ar[y]));
+                ai[y] = fma(v.x, q.y, fma(v.y, q.x, ai[y]));
+            }
+        }
+    }
+    const int gx = x0 + tx;
+#pragma unroll
+    for (int y = 0; y < YS; ++y) {
+        const int gy = y0 + ysub * YS + y;
+        if (gy < nky) {
+            const int row = pr[gx * nky + gy];
+            if (row >= 0) {
+                const size_t o = (size_t)row * n + z;
+                const C2 base = in0 ? in0[o] : mk2<R>(0, 0);
+                out[o] = mk2<R>(base.x + sgn * ar[y], base.y + sgn * ai[y]);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Arnoldi reductions.  partial[tile][i] = sum conj(Q_i) W over the tile for
 // i < nvec; slot nvec holds ||W||^2 when with_norm.  One warp per vector;
 // FP64 accumulation for both precisions.
@@ -521,11 +663,10 @@ __global__ void k_cycle_start(GmresState st, int nsys, int m, const double2 *__r
 // iterating in this cycle when its residual estimate reaches
 // max(rtol ||b||, inner_rtol beta0) (inner_rtol > 0 only for the mixed
 // form, whose FP32 inner solve cannot go below its own rounding level).
-__global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rtol, int max_iter,
+__device__ void arnoldi_givens(GmresState &st, int s, int m, int j, double rtol, int max_iter,
                                double inner_rtol)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nsys || !st.active[s]) return;
+    if (!st.active[s]) return;
     const int hs = m + 2;
     const double2 *h1 = st.h1 + (size_t)s * hs;
     const double2 *h2 = st.h2 + (size_t)s * hs;
@@ -584,6 +725,14 @@ __global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rto
     if (stop) st.active[s] = 0;
 }
 
+__global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rtol, int max_iter,
+                               double inner_rtol)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    arnoldi_givens(st, s, m, j, rtol, max_iter, inner_rtol);
+}
+
 // y = R^-1 g over the kcyc columns of this cycle.
 __global__ void k_trisolve(GmresState st, int nsys, int m)
 {
@@ -598,6 +747,193 @@ __global__ void k_trisolve(GmresState st, int nsys, int m)
         double2 acc = g[i];
         for (int l = i + 1; l < k; ++l) acc = csub(acc, cmul(H[(size_t)l * (m + 1) + i], y[l]));
         y[i] = cdiv(acc, H[(size_t)i * (m + 1) + i]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused Arnoldi step (CGS2), three launches per step:
+//   P1  h1 = Q^H w                                  (partials + last-block reduce)
+//   P2  w <- w - Q h1 ; h2 = Q^H w ; |w|^2 ; Givens  (partials + last-block reduce)
+//   P3  q_{j+1} = (w - Q h2) / beta                  (k_update)
+// Each block handles 1/split of a row tile; the block that finishes last for
+// a system (per-system arrival counter) sums that system's partials in a
+// fixed order, so results do not depend on scheduling.
+// ---------------------------------------------------------------------------
+struct ArnoldiArgs {
+    Tiles tiles;
+    const int *sys_tile0;   // [B + 1] first tile of each system
+    const int *gate;        // [B] active flags
+    int n;
+    int split;              // blocks per tile
+    size_t qstride;         // elements between basis vectors
+    double2 *partial;       // [ntiles * split][pstride]
+    int pstride;
+    int *counter;           // [B] arrival counters (left at 0)
+};
+
+constexpr int kProjGroup = 8;   // basis vectors per accumulation pass
+
+constexpr int kProjSlots = 2 * kProjGroup + 1;   // re/im per vector + |w|^2
+
+// Block sums of the accumulator slots in use: slots i < 2 gn, and slot
+// kProjSlots - 1 (the norm) when with_norm.  Results in red[slot].
+__device__ __forceinline__ void block_sum(double (&v)[kProjSlots], int gn, bool with_norm,
+                                          double *red_ws, double *red)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int i = 0; i < kProjSlots; ++i) {
+        const bool used = (i < 2 * gn) || (with_norm && i == kProjSlots - 1);
+        if (used) {
+            const double t = warp_sum(v[i]);
+            if (lane == 0) red_ws[warp * kProjSlots + i] = t;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < kProjSlots) {
+        const int i = threadIdx.x;
+        const bool used = (i < 2 * gn) || (with_norm && i == kProjSlots - 1);
+        double t = 0.0;
+        if (used)
+            for (int w = 0; w < nw; ++w) t += red_ws[w * kProjSlots + i];
+        red[i] = t;
+    }
+    __syncthreads();
+}
+
+template <typename R>
+__device__ __forceinline__ void elem_range(const ArnoldiArgs &a, int tile, int sub, size_t &e0, int &ne)
+{
+    const int tot = a.tiles.nrow[tile] * a.n;
+    const int per = (tot + a.split - 1) / a.split;
+    const int lo = min(tot, sub * per);
+    e0 = (size_t)a.tiles.row0[tile] * a.n + lo;
+    ne = min(tot, lo + per) - lo;
+}
+
+// Partial dot products of this block: slots [0, nvec) = Q_i^H w, slot nvec =
+// |w|^2 when with_norm.  Written to out[*].
+template <typename R>
+__device__ void block_project(const ArnoldiArgs &a, const typename CT<R>::t *Q, int nvec,
+                              const typename CT<R>::t *W, size_t e0, int ne, int with_norm,
+                              double2 *out)
+{
+    using C2 = typename CT<R>::t;
+    __shared__ double red_ws[8 * kProjSlots];
+    __shared__ double red[kProjSlots];
+    const int ngroups = (nvec > 0) ? (nvec + kProjGroup - 1) / kProjGroup : (with_norm ? 1 : 0);
+    for (int gi = 0; gi < ngroups; ++gi) {
+        const int g0 = gi * kProjGroup;
+        const int gn = min(kProjGroup, nvec - g0);
+        const bool norm_here = with_norm && (gi == ngroups - 1);
+        double acc[kProjSlots];
+#pragma unroll
+        for (int i = 0; i < kProjSlots; ++i) acc[i] = 0.0;
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const C2 w = W[e0 + e];
+#pragma unroll
+            for (int i = 0; i < kProjGroup; ++i) {
+                if (i < gn) {
+                    const C2 q = Q[(size_t)(g0 + i) * a.qstride + e0 + e];
+                    acc[2 * i] = fma((double)q.x, (double)w.x, fma((double)q.y, (double)w.y, acc[2 * i]));
+                    acc[2 * i + 1] = fma((double)q.x, (double)w.y, fma(-(double)q.y, (double)w.x, acc[2 * i + 1]));
+                }
+            }
+            if (norm_here)
+                acc[kProjSlots - 1] = fma((double)w.x, (double)w.x, fma((double)w.y, (double)w.y, acc[kProjSlots - 1]));
+        }
+        block_sum(acc, gn, norm_here, red_ws, red);
+        if (threadIdx.x < gn) out[g0 + threadIdx.x] = make_double2(red[2 * threadIdx.x], red[2 * threadIdx.x + 1]);
+        if (norm_here && threadIdx.x == 0) out[nvec] = make_double2(red[kProjSlots - 1], 0.0);
+    }
+}
+
+// Last-arriving block of system s sums the system's partials into dst[0..nslot).
+__device__ __forceinline__ bool last_block_reduce(const ArnoldiArgs &a, int s, int nslot, double2 *dst)
+{
+    __shared__ int is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nblocks = (a.sys_tile0[s + 1] - a.sys_tile0[s]) * a.split;
+        const int prev = atomicAdd(&a.counter[s], 1);
+        is_last = (prev == nblocks - 1);
+        if (is_last) a.counter[s] = 0;
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    const int b0 = a.sys_tile0[s] * a.split, b1 = a.sys_tile0[s + 1] * a.split;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = warp; i < nslot; i += (blockDim.x >> 5)) {
+        double sr = 0.0, si = 0.0;
+        for (int b = b0 + lane; b < b1; b += 32) {
+            const double2 v = __ldcg(a.partial + (size_t)b * a.pstride + i);
+            sr += v.x;
+            si += v.y;
+        }
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (lane == 0) dst[i] = make_double2(sr, si);
+    }
+    __syncthreads();
+    return true;
+}
+
+// P1: h1 = Q^H w
+template <typename R>
+__global__ void __launch_bounds__(256)
+k_arnoldi_p1(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
+             const typename CT<R>::t *__restrict__ W, double2 *__restrict__ h1, int hstride)
+{
+    const int tile = blockIdx.x / a.split, sub = blockIdx.x - tile * a.split;
+    const int s = a.tiles.sys[tile];
+    if (a.gate && a.gate[s] == 0) return;
+    size_t e0;
+    int ne;
+    elem_range<R>(a, tile, sub, e0, ne);
+    block_project<R>(a, Q, nvec, W, e0, ne, 0, a.partial + (size_t)blockIdx.x * a.pstride);
+    last_block_reduce(a, s, nvec, h1 + (size_t)s * hstride);
+}
+
+__device__ void arnoldi_givens(GmresState &st, int s, int m, int j, double rtol, int max_iter,
+                               double inner_rtol);
+
+// P2: w <- w - Q h1 ; h2 = Q^H w, |w|^2 ; then the Givens step of the system.
+template <typename R>
+__global__ void __launch_bounds__(256)
+k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
+             typename CT<R>::t *__restrict__ W, GmresState st, int m, int j, double rtol,
+             int max_iter, double inner_rtol)
+{
+    using C2 = typename CT<R>::t;
+    __shared__ C2 cf[kMaxRestart + 1];
+    const int tile = blockIdx.x / a.split, sub = blockIdx.x - tile * a.split;
+    const int s = a.tiles.sys[tile];
+    if (a.gate && a.gate[s] == 0) return;
+    const int hs = m + 2;
+    for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
+        const double2 c = st.h1[(size_t)s * hs + i];
+        cf[i] = mk2<R>((R)c.x, (R)c.y);
+    }
+    __syncthreads();
+    size_t e0;
+    int ne;
+    elem_range<R>(a, tile, sub, e0, ne);
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        C2 w = W[e0 + e];
+        for (int i = 0; i < nvec; ++i) {
+            const C2 q = Q[(size_t)i * a.qstride + e0 + e];
+            const C2 c = cf[i];
+            w.x = fma(-q.x, c.x, fma(q.y, c.y, w.x));
+            w.y = fma(-q.x, c.y, fma(-q.y, c.x, w.y));
+        }
+        W[e0 + e] = w;
+    }
+    __syncthreads();
+    block_project<R>(a, Q, nvec, W, e0, ne, 1, a.partial + (size_t)blockIdx.x * a.pstride);
+    if (last_block_reduce(a, s, nvec + 1, st.h2 + (size_t)s * hs)) {
+        if (threadIdx.x == 0) arnoldi_givens(st, s, m, j, rtol, max_iter, inner_rtol);
     }
 }
 

@@ -24,12 +24,14 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/multiscat_b200.h"
 #include "msc_common.cuh"
 #include "msc_eigh.hpp"
 #include "msc_kernels.cuh"
+#include "msc_tc.cuh"
 
 namespace {
 
@@ -109,8 +111,24 @@ struct msc_plan {
     DevBuf<float> E32, ET32, lam32, en32, row_pkd32, row_fn32;
     DevBuf<float2> Vt32, row_c32, Q32, W32, U32;
     DevBuf<double2> R64;
+    // tcgen05 block inverse (mixed form)
+    bool use_tc = false;
+    int tc_n = 0, tc_tile_rows = 0, tc_ntiles = 0, tc_grid = 0;
+    size_t tc_smem = 0;
+    DevBuf<__nv_bfloat16> e_img;
+    DevBuf<int> tc_error;
     DevBuf<int> active, kcyc, iters, cycles, unfinished, status, counter;
     int *counter_host = nullptr;   // pinned
+    int split = 1;                 // Arnoldi blocks per row tile
+    // halo-tiled coupling
+    bool use_halo = false;             // halo tables built (taps reach <= 8)
+    int halo32 = 0, halo64 = 0;    // autotuned coupling kind per precision (0 nbr, 1/2 halo)
+    int halo_hx = 0, halo_hy = 0, nwork = 0;
+    // autotuning record: microseconds per candidate
+    std::vector<std::pair<std::string, float>> tune_log;
+    std::string tune_report;
+    DevBuf<int> work, pos_row, tap_window;
+    DevBuf<int> sys_counter;       // per-system arrival counters of the fused Arnoldi kernels
     cudaStream_t stream = nullptr;
     cudaGraphExec_t g_start = nullptr, g_iter = nullptr;
     int pstride = 0;
@@ -141,9 +159,10 @@ struct msc_plan {
         h2.release(); y.release(); scale.release(); bnorm.release(); resid.release();
         est.release(); active.release(); kcyc.release(); iters.release(); cycles.release();
         unfinished.release(); status.release(); counter.release(); beta0.release();
+        sys_counter.release(); work.release(); pos_row.release(); tap_window.release();
         E32.release(); ET32.release(); lam32.release(); en32.release(); row_pkd32.release();
         row_fn32.release(); Vt32.release(); row_c32.release(); Q32.release(); W32.release();
-        U32.release(); R64.release();
+        U32.release(); R64.release(); e_img.release(); tc_error.release();
     }
 
     msc::Tiles tiles() const
@@ -214,11 +233,47 @@ using C2 = typename msc::CT<R>::t;
 template <typename R>
 size_t smem_block_inverse_t(int n) { return (size_t)2 * n * 2 * block_inverse_rows(n) * sizeof(R); }
 
+void launch_block_inverse_tc(msc_plan *p, const int *gate, const float2 *x, float2 *out,
+                             cudaStream_t st)
+{
+    msc::tc::TcParams prm;
+    prm.n = p->n;
+    prm.kp = (p->n + 15) / 16 * 16;
+    prm.mt = (p->n + 127) / 128;
+    prm.rows = p->R;
+    prm.tile_rows = p->tc_tile_rows;
+    prm.ntiles = p->tc_ntiles;
+    prm.e_img = p->e_img.p;
+    prm.lam = p->lam.p;
+    prm.en = p->en.p;
+    prm.row_pkd = p->row_pkd.p;
+    prm.row_fn = p->row_fn.p;
+    prm.row_c = p->row_c.p;
+    prm.row_sys = p->row_sys.p;
+    prm.gate = gate;
+    prm.x = x;
+    prm.out = out;
+    prm.error = p->tc_error.p;
+    switch (p->tc_n) {
+    case 16: msc::tc::k_block_inverse_tc<16><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
+    case 32: msc::tc::k_block_inverse_tc<32><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
+    case 64: msc::tc::k_block_inverse_tc<64><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
+    case 128: msc::tc::k_block_inverse_tc<128><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
+    default: msc::tc::k_block_inverse_tc<256><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
+    }
+}
+
 template <typename R>
 void launch_block_inverse_t(msc_plan *p, const int *gate, const C2<R> *x, C2<R> *out, int acc,
                             cudaStream_t st)
 {
     using D = OpData<R>;
+    if constexpr (std::is_same<R, float>::value) {
+        if (p->use_tc && !acc) {
+            launch_block_inverse_tc(p, gate, x, out, st);
+            return;
+        }
+    }
     if (block_inverse_rows(p->n) == 8)
         msc::k_block_inverse<8, R><<<p->ntiles, 256, smem_block_inverse_t<R>(p->n), st>>>(
             p->tiles(), gate, p->n, D::E(p), D::ET(p), p->lam.p, p->en.p, p->row_pkd.p,
@@ -243,10 +298,49 @@ void launch_residual_diag(msc_plan *p, const int *gate, const double2 *x, double
         p->sys_bspec.p, x, out, with_b);
 }
 
+constexpr int kHaloBX = 8;
+template <typename R> constexpr int halo_zc() { return std::is_same<R, float>::value ? 32 : 16; }
+
+size_t halo_smem(int hx, int hy, int zc, size_t elem)
+{
+    return (size_t)(kHaloBX + 2 * hx) * (8 + 2 * hy) * zc * elem +
+           (size_t)(2 * hx + 1) * (2 * hy + 1) * zc * elem +
+           (size_t)(kHaloBX + 2 * hx) * (8 + 2 * hy) * sizeof(int);
+}
+
+template <int HY, int YS, typename R>
+void launch_halo(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
+                 C2<R> *out, cudaStream_t st)
+{
+    constexpr int ZC = halo_zc<R>();
+    msc::CouplingTiles ct{p->work.p, p->pos_row.p, p->tap_window.p, p->nwork, p->nkx, p->nky,
+                          p->halo_hx, p->K};
+    dim3 grid(p->nwork, (p->n + ZC - 1) / ZC);
+    msc::k_coupling_halo<HY, kHaloBX, ZC, YS, R>
+        <<<grid, kHaloBX * ZC * (8 / YS), halo_smem(p->halo_hx, HY, ZC, sizeof(C2<R>)), st>>>(
+            ct, gate, p->n, OpData<R>::Vt(p), src, in0, sgn, out);
+}
+
+template <int YS, typename R>
+void launch_halo_ys(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
+                    C2<R> *out, cudaStream_t st)
+{
+    switch (p->halo_hy) {
+    case 1: launch_halo<1, YS, R>(p, gate, src, in0, sgn, out, st); return;
+    case 2: launch_halo<2, YS, R>(p, gate, src, in0, sgn, out, st); return;
+    case 4: launch_halo<4, YS, R>(p, gate, src, in0, sgn, out, st); return;
+    default: launch_halo<8, YS, R>(p, gate, src, in0, sgn, out, st); return;
+    }
+}
+
 template <typename R>
 void launch_coupling_t(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
                        C2<R> *out, cudaStream_t st)
 {
+    // coupling kind per precision: 0 neighbour table, 1 halo (8 y/thread), 2 halo (4 y/thread)
+    const int kind = p->use_halo ? (std::is_same<R, float>::value ? p->halo32 : p->halo64) : 0;
+    if (kind == 1) { launch_halo_ys<8, R>(p, gate, src, in0, sgn, out, st); return; }
+    if (kind == 2) { launch_halo_ys<4, R>(p, gate, src, in0, sgn, out, st); return; }
     dim3 grid(p->ntiles, (p->n + 31) / 32);
     dim3 block(32, msc::kTileRows);
     msc::k_coupling<R><<<grid, block, smem_coupling(std::max(p->K, 1)), st>>>(
@@ -297,6 +391,21 @@ void launch_update(msc_plan *p, const int *gate, int nvec, const int *nvec_sys,
 }
 
 int sys_blocks(int B) { return (B + 127) / 128; }
+
+msc::ArnoldiArgs arnoldi_args(msc_plan *p, const int *gate)
+{
+    msc::ArnoldiArgs a;
+    a.tiles = p->tiles();
+    a.sys_tile0 = p->sys_tile0.p;
+    a.gate = gate;
+    a.n = p->n;
+    a.split = p->split;
+    a.qstride = (size_t)p->R * p->n;
+    a.partial = p->partial.p;
+    a.pstride = p->pstride;
+    a.counter = p->sys_counter.p;
+    return a;
+}
 
 cudaEvent_t tev_at(msc_plan *p, int kind, int slot, int which)
 {
@@ -349,15 +458,11 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
         if (tm) mark(p, 1, j, 0, st);
         launch_coupling_t<R>(p, p->active.p, U, Qj, R(1), W, st);
         if (tm) mark(p, 1, j, 1, st);
-        launch_dots_t<R>(p, p->active.p, Q, j + 1, W, 0, st);
-        launch_reduce(p, p->active.p, j + 1, p->h1.p, st);
-        launch_update_t<R>(p, p->active.p, Q, j + 1, nullptr, p->h1.p, p->m + 2, W, nullptr, W, 0,
-                           st);
-        launch_dots_t<R>(p, p->active.p, Q, j + 1, W, 1, st);
-        launch_reduce(p, p->active.p, j + 2, p->h2.p, st);
-        msc::k_arnoldi_step<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m, j,
-                                                              p->desc.rtol,
-                                                              p->desc.max_iterations, inner);
+        const msc::ArnoldiArgs aa = arnoldi_args(p, p->active.p);
+        const unsigned nblk = (unsigned)(p->ntiles * p->split);
+        msc::k_arnoldi_p1<R><<<nblk, 256, 0, st>>>(aa, Q, j + 1, W, p->h1.p, p->m + 2);
+        msc::k_arnoldi_p2<R><<<nblk, 256, 0, st>>>(aa, Q, j + 1, W, p->state(), p->m, j,
+                                                   p->desc.rtol, p->desc.max_iterations, inner);
         launch_update_t<R>(p, p->active.p, Q, j + 1, nullptr, p->h2.p, p->m + 2, W, p->scale.p, Qn,
                            0, st);
     }
@@ -461,12 +566,247 @@ msc_status set_kernel_attributes(int n, int K)
                                   (int)smem_block_inverse(msc::kMaxNz)));
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_coupling(msc::kMaxTaps)));
+#define MSC_HALO_ATTR(HY, R)                                                                     \
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_halo<HY, kHaloBX, halo_zc<R>(), 8, R>,        \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                  (int)std::min<size_t>(halo_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448))); \
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_halo<HY, kHaloBX, halo_zc<R>(), 4, R>,        \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                  (int)std::min<size_t>(halo_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448)));
+    MSC_HALO_ATTR(1, float)
+    MSC_HALO_ATTR(2, float)
+    MSC_HALO_ATTR(4, float)
+    MSC_HALO_ATTR(8, float)
+    MSC_HALO_ATTR(1, double)
+    MSC_HALO_ATTR(2, double)
+    MSC_HALO_ATTR(4, double)
+    MSC_HALO_ATTR(8, double)
+#undef MSC_HALO_ATTR
     MSC_CUDA(cudaFuncSetAttribute(msc::k_residual_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_residual(msc::kMaxNz)));
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_coupling(msc::kMaxTaps)));
     (void)n;
     (void)K;
+    return MSC_OK;
+}
+
+// Shared memory the tensor-core kernel needs for tile width N (bytes of the
+// dynamic part), including the bytes its padded M tiles may read past E.
+size_t tc_smem_bytes(int n, int N)
+{
+    const size_t kp = (size_t)(n + 15) / 16 * 16;
+    const size_t kb = kp / 8, mt = (size_t)(n + 127) / 128;
+    const size_t part = kp * kp * 2, sz = kb * 128;
+    const size_t read1 = (16 * mt - 1) * 128 + (kb - 1) * sz + 128;
+    const size_t read2 = (16 * mt - 1) * sz + (kb - 1) * 128 + 128;
+    const size_t need = std::max(2 * part + 4 * (size_t)N * kp, part + std::max(read1, read2));
+    return (need + 1023) / 1024 * 1024 + 1024;
+}
+
+template <int N>
+cudaError_t tc_set_smem(size_t bytes)
+{
+    return cudaFuncSetAttribute(msc::tc::k_block_inverse_tc<N>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int N>
+size_t tc_static_smem()
+{
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, msc::tc::k_block_inverse_tc<N>) != cudaSuccess) return 1u << 30;
+    return a.sharedSizeBytes;
+}
+
+size_t tc_static_for(int N)
+{
+    switch (N) {
+    case 16: return tc_static_smem<16>();
+    case 32: return tc_static_smem<32>();
+    case 64: return tc_static_smem<64>();
+    case 128: return tc_static_smem<128>();
+    default: return tc_static_smem<256>();
+    }
+}
+
+// Decide whether the mixed form uses the tcgen05 block inverse and with what
+// tile width; build the BF16 hi/lo image of E in the kernel's smem order.
+msc_status setup_tensor_core(msc_plan *p)
+{
+    p->use_tc = false;
+    if (!p->mixed || (p->desc.flags & 1) || p->n > 256) return MSC_OK;
+    int dev = 0, sms = 0, cc_major = 0, cc_minor = 0, optin = 0;
+    MSC_CUDA(cudaGetDevice(&dev));
+    MSC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MSC_CUDA(cudaDeviceGetAttribute(&cc_major, cudaDevAttrComputeCapabilityMajor, dev));
+    MSC_CUDA(cudaDeviceGetAttribute(&cc_minor, cudaDevAttrComputeCapabilityMinor, dev));
+    MSC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (cc_major != 10 || cc_minor != 0) return MSC_OK;   // tcgen05 path is built for sm_100a
+    const int n = p->n, mt = (n + 127) / 128;
+    int chosen = 0;
+    for (int N = 16; N <= 256; N *= 2) {
+        if (2 * mt * N > 512) break;
+        if (tc_smem_bytes(n, N) + tc_static_for(N) > (size_t)optin) break;
+        const int tiles = (p->R + N / 2 - 1) / (N / 2);
+        chosen = N;
+        if (tiles <= sms) break;   // enough tiles for every SM already at this width
+    }
+    if (chosen == 0) return MSC_OK;
+    p->tc_n = chosen;
+    p->tc_tile_rows = chosen / 2;
+    p->tc_ntiles = (p->R + p->tc_tile_rows - 1) / p->tc_tile_rows;
+    p->tc_grid = std::min(p->tc_ntiles, sms);
+    p->tc_smem = tc_smem_bytes(n, chosen);
+    {
+        // TMEM: CTAs resident on one SM must fit in its 512 columns, so pad
+        // the shared-memory request until no more than 512 / ncols CTAs fit.
+        int ncols = 32;
+        while (ncols < 2 * mt * chosen) ncols <<= 1;
+        const size_t max_ctas = 512 / (size_t)ncols;
+        const size_t sm_bytes = 233472;   // 228 KB of shared memory per SM
+        const size_t floor_bytes = sm_bytes / (max_ctas + 1) + 1024;
+        p->tc_smem = std::max(p->tc_smem, floor_bytes);
+        if (p->tc_smem + tc_static_for(chosen) > (size_t)optin) return MSC_OK;
+    }
+    // every width up to `chosen` may be picked by the autotuner; all launch
+    // with the same (largest) shared-memory request
+    for (int N = 16; N <= chosen; N *= 2) {
+        cudaError_t e = cudaSuccess;
+        switch (N) {
+        case 16: e = tc_set_smem<16>(p->tc_smem); break;
+        case 32: e = tc_set_smem<32>(p->tc_smem); break;
+        case 64: e = tc_set_smem<64>(p->tc_smem); break;
+        case 128: e = tc_set_smem<128>(p->tc_smem); break;
+        default: e = tc_set_smem<256>(p->tc_smem); break;
+        }
+        if (e != cudaSuccess) return fail(MSC_ERR_CUDA, std::string("tc smem attribute: ") + cudaGetErrorString(e));
+    }
+    // E image: [hi|lo][z/8][k/8][z%8][k%8], zero padded to kp x kp
+    const int kp = (n + 15) / 16 * 16, kb = kp / 8;
+    std::vector<__nv_bfloat16> img((size_t)2 * kp * kp, __float2bfloat16(0.f));
+    for (int z = 0; z < n; ++z)
+        for (int k = 0; k < n; ++k) {
+            const double v = p->E_host[(size_t)z * n + k];
+            const __nv_bfloat16 hi = __float2bfloat16_rn((float)v);
+            const __nv_bfloat16 lo = __float2bfloat16_rn((float)(v - (double)__bfloat162float(hi)));
+            const size_t off = ((size_t)(z / 8) * kb + k / 8) * 64 + (z % 8) * 8 + (k % 8);
+            img[off] = hi;
+            img[(size_t)kp * kp + off] = lo;
+        }
+    MSC_CUDA(upload(p->e_img, img));
+    MSC_CUDA(p->tc_error.alloc(1));
+    MSC_CUDA(cudaMemset(p->tc_error.p, 0, sizeof(int)));
+    p->use_tc = true;
+    return MSC_OK;
+}
+
+// Device time of one call of `f` on the plan's stream (mean of 3 after a warm-up).
+template <typename F>
+float time_launch(msc_plan *p, F f)
+{
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    f(p->stream);
+    cudaEventRecord(a, p->stream);
+    for (int i = 0; i < 3; ++i) f(p->stream);
+    cudaEventRecord(b, p->stream);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms * 1000.f / 3.f;
+}
+
+// Autotuner: time the kernel variants this plan can use on its own data
+// and keep the fastest.  Coupling: halo tiles vs neighbour table, for each
+// precision the solve uses.  Mixed form: tcgen05 tile width N (and the SIMT
+// FP32 kernel).  Runs once per plan, before the solve graphs are captured.
+msc_status autotune(msc_plan *p)
+{
+    const size_t vs = (size_t)p->R * p->n;
+    MSC_CUDA(cudaMemsetAsync(p->X.p, 0, vs * sizeof(double2), p->stream));
+    MSC_CUDA(cudaMemsetAsync(p->TMP.p, 0, vs * sizeof(double2), p->stream));
+    const char *kind_name[3] = {"neighbour", "halo_y8", "halo_y4"};
+    if (p->use_halo) {
+        float best = 0.f;
+        int best_k = 0;
+        for (int k = 0; k < 3; ++k) {
+            p->halo64 = k;
+            const float t = time_launch(p, [&](cudaStream_t st) {
+                launch_coupling_t<double>(p, nullptr, p->X.p, p->TMP.p, -1.0, p->TMP.p, st);
+            });
+            p->tune_log.push_back({std::string("coupling64_") + kind_name[k] + "_us", t});
+            if (k == 0 || t < best) {
+                best = t;
+                best_k = k;
+            }
+        }
+        p->halo64 = best_k;
+    }
+    if (p->mixed) {
+        float2 *a = p->Q32.p, *b = p->W32.p, *c = p->U32.p;
+        MSC_CUDA(cudaMemsetAsync(a, 0, vs * sizeof(float2), p->stream));
+        MSC_CUDA(cudaMemsetAsync(c, 0, vs * sizeof(float2), p->stream));
+        if (p->use_halo) {
+            float best = 0.f;
+            int best_k = 0;
+            for (int k = 0; k < 3; ++k) {
+                p->halo32 = k;
+                const float t = time_launch(p, [&](cudaStream_t st) {
+                    launch_coupling_t<float>(p, nullptr, a, c, 1.0f, b, st);
+                });
+                p->tune_log.push_back({std::string("coupling32_") + kind_name[k] + "_us", t});
+                if (k == 0 || t < best) {
+                    best = t;
+                    best_k = k;
+                }
+            }
+            p->halo32 = best_k;
+        }
+        if (p->use_tc) {
+            int sms = 0, dev = 0;
+            MSC_CUDA(cudaGetDevice(&dev));
+            MSC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            const int best_n0 = p->tc_n;
+            int best_n = 0;
+            float best_t = 0.f;
+            p->use_tc = false;
+            const float t_simt = time_launch(p, [&](cudaStream_t st) {
+                launch_block_inverse_t<float>(p, nullptr, a, b, 0, st);
+            });
+            p->tune_log.push_back({"block_inverse32_simt_us", t_simt});
+            p->use_tc = true;
+            for (int N = 16; N <= best_n0; N *= 2) {
+                p->tc_n = N;
+                p->tc_tile_rows = N / 2;
+                p->tc_ntiles = (p->R + N / 2 - 1) / (N / 2);
+                p->tc_grid = std::min(p->tc_ntiles, sms);
+                const float t = time_launch(p, [&](cudaStream_t st) {
+                    launch_block_inverse_t<float>(p, nullptr, a, b, 0, st);
+                });
+                p->tune_log.push_back({"block_inverse32_tc_N" + std::to_string(N) + "_us", t});
+                if (best_n == 0 || t < best_t) {
+                    best_n = N;
+                    best_t = t;
+                }
+            }
+            int tc_err = 0;
+            MSC_CUDA(cudaMemcpy(&tc_err, p->tc_error.p, sizeof(int), cudaMemcpyDeviceToHost));
+            if (tc_err) return fail(MSC_ERR_CUDA, "tensor-core block inverse timed out during tuning");
+            if (t_simt < best_t && !(p->desc.flags & 2)) {
+                p->use_tc = false;
+            } else {
+                p->tc_n = best_n;
+                p->tc_tile_rows = best_n / 2;
+                p->tc_ntiles = (p->R + best_n / 2 - 1) / (best_n / 2);
+                p->tc_grid = std::min(p->tc_ntiles, sms);
+            }
+        }
+    }
+    MSC_CUDA(cudaGetLastError());
     return MSC_OK;
 }
 
@@ -537,6 +877,56 @@ msc_status finalize(msc_plan *p)
     MSC_CUDA(upload(p->sys_aspec, aspec));
     MSC_CUDA(upload(p->sys_spec_row, spec_row));
     MSC_CUDA(upload(p->nbr, nbr));
+    {
+        // Halo-tiled coupling: signed tap reach, tap window, position->row
+        // tables and the list of 8 x kHaloBX position patches that hold
+        // channels of each system.
+        int hx = 0, hy = 0;
+        std::vector<std::pair<int, int>> sgn(p->K);
+        for (int t = 0; t < p->K; ++t) {
+            int dx = p->taps[t].first, dy = p->taps[t].second;
+            if (dx > p->nkx / 2) dx -= p->nkx;
+            if (dy > p->nky / 2) dy -= p->nky;
+            sgn[t] = {dx, dy};
+            hx = std::max(hx, std::abs(dx));
+            hy = std::max(hy, std::abs(dy));
+        }
+        int hyt = 1;
+        while (hyt < hy) hyt <<= 1;
+        p->use_halo = (hx <= 8 && hyt <= 8 &&
+                       halo_smem(hx, hyt, 16, sizeof(double2)) <= 225 * 1024 &&
+                       halo_smem(hx, hyt, 32, sizeof(float2)) <= 225 * 1024);
+        if (p->use_halo) {
+            p->halo_hx = hx;
+            p->halo_hy = hyt;
+            const int wy = 2 * hyt + 1;
+            std::vector<int> win((size_t)(2 * hx + 1) * wy, -1);
+            for (int t = 0; t < p->K; ++t)
+                win[(size_t)(sgn[t].first + hx) * wy + (sgn[t].second + hyt)] = t;
+            const int npos = p->nkx * p->nky;
+            std::vector<int> pr((size_t)p->B * npos, -1), wl;
+            const int nbx = (p->nkx + kHaloBX - 1) / kHaloBX, nby = (p->nky + 7) / 8;
+            for (int s2 = 0; s2 < p->B; ++s2) {
+                const SystemHost &sh = p->sys[s2];
+                std::vector<char> occ((size_t)nbx * nby, 0);
+                for (int j = 0; j < sh.C; ++j) {
+                    pr[(size_t)s2 * npos + sh.ix[j] * p->nky + sh.iy[j]] = p->sys_row0_h[s2] + j;
+                    occ[(size_t)(sh.ix[j] / kHaloBX) * nby + sh.iy[j] / 8] = 1;
+                }
+                for (int bx = 0; bx < nbx; ++bx)
+                    for (int by = 0; by < nby; ++by)
+                        if (occ[(size_t)bx * nby + by]) {
+                            wl.push_back(s2);
+                            wl.push_back(bx * kHaloBX);
+                            wl.push_back(by * 8);
+                        }
+            }
+            p->nwork = (int)(wl.size() / 3);
+            MSC_CUDA(upload(p->tap_window, win));
+            MSC_CUDA(upload(p->pos_row, pr));
+            MSC_CUDA(upload(p->work, wl));
+        }
+    }
     MSC_CUDA(upload(p->tile_row0, p->tile_row0_h));
     MSC_CUDA(upload(p->tile_nrow, p->tile_nrow_h));
     MSC_CUDA(upload(p->tile_sys, p->tile_sys_h));
@@ -571,7 +961,16 @@ msc_status finalize(msc_plan *p)
         MSC_CUDA(p->U.alloc(vs));
         MSC_CUDA(p->Q.alloc(vs * (m + 1)));
     }
-    MSC_CUDA(p->partial.alloc((size_t)p->ntiles * p->pstride));
+    {
+        // Enough Arnoldi blocks to fill the GPU (about 600 blocks of 256
+        // threads), without splitting a tile below 256 elements per block.
+        const int tile_elems = msc::kTileRows * n;
+        const int max_split = std::max(1, tile_elems / 256);
+        p->split = std::max(1, std::min(max_split, (600 + p->ntiles - 1) / p->ntiles));
+    }
+    MSC_CUDA(p->partial.alloc((size_t)p->ntiles * p->split * p->pstride));
+    MSC_CUDA(p->sys_counter.alloc(p->B));
+    MSC_CUDA(cudaMemset(p->sys_counter.p, 0, p->B * sizeof(int)));
     MSC_CUDA(p->H.alloc((size_t)p->B * (m + 1) * m));
     MSC_CUDA(p->cs.alloc((size_t)p->B * m));
     MSC_CUDA(p->sn.alloc((size_t)p->B * m));
@@ -594,6 +993,14 @@ msc_status finalize(msc_plan *p)
     MSC_CUDA(cudaMemset(p->h1.p, 0, p->h1.count * sizeof(double2)));
     MSC_CUDA(cudaMemset(p->y.p, 0, p->y.count * sizeof(double2)));
 
+    {
+        msc_status tst = setup_tensor_core(p);
+        if (tst != MSC_OK) return tst;
+    }
+    {
+        msc_status tst = autotune(p);
+        if (tst != MSC_OK) return tst;
+    }
     MSC_CUDA(cudaMallocHost(&p->kcyc_host, p->B * sizeof(int)));
     for (int s = 0; s < p->B; ++s) p->kcyc_host[s] = 0;
     p->tev.resize((size_t)2 * (m + 1) * 2);
@@ -825,6 +1232,11 @@ msc_status msc_solve(msc_plan *p, double *psi_out, double *intensities_out, msc_
     p->launches_last = launches;
     p->cycles_last = cycle;
     MSC_CUDA(cudaGetLastError());
+    if (p->use_tc) {
+        int tc_err = 0;
+        MSC_CUDA(cudaMemcpy(&tc_err, p->tc_error.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (tc_err) return fail(MSC_ERR_CUDA, "tensor-core block inverse timed out on an mbarrier wait");
+    }
     if (psi_out)
         MSC_CUDA(cudaMemcpyAsync(psi_out, p->X.p, vs * sizeof(double2), cudaMemcpyDeviceToDevice, ps));
     if (intensities_out) {
@@ -938,6 +1350,45 @@ msc_status msc_debug_apply_operator(msc_plan *p, const double *x, double *y, voi
     MSC_CUDA(cudaGetLastError());
     return MSC_OK;
 }
+
+const char *msc_plan_tuning_report(msc_plan *p)
+{
+    if (!p) return "";
+    std::string r = "{";
+    for (size_t i = 0; i < p->tune_log.size(); ++i) {
+        if (i) r += ", ";
+        r += "\"" + p->tune_log[i].first + "\": " + std::to_string(p->tune_log[i].second);
+    }
+    if (!r.empty() && r.size() > 1) r += ", ";
+    const char *kn[3] = {"neighbour", "halo_y8", "halo_y4"};
+    r += "\"chosen\": \"coupling64=" + std::string(p->use_halo ? kn[p->halo64] : kn[0]) +
+         ",coupling32=" + std::string(p->use_halo ? kn[p->halo32] : kn[0]) +
+         ",block_inverse32=" + (p->use_tc ? "tc_N" + std::to_string(p->tc_n) : std::string("simt")) +
+         "\"}";
+    p->tune_report = r;
+    return p->tune_report.c_str();
+}
+
+msc_status msc_debug_apply_block_inverse_f32(msc_plan *p, const float *x, float *y, void *stream)
+{
+    if (!p || !x || !y) return fail(MSC_ERR_ARG, "null argument");
+    if (!p->mixed) return fail(MSC_ERR_ARG, "plan is not a mixed-precision plan");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    launch_block_inverse_t<float>(p, nullptr, reinterpret_cast<const float2 *>(x),
+                                  reinterpret_cast<float2 *>(y), 0, s);
+    MSC_CUDA(cudaGetLastError());
+    if (p->use_tc) {
+        int tc_err = 0;
+        MSC_CUDA(cudaMemcpyAsync(&tc_err, p->tc_error.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MSC_CUDA(cudaStreamSynchronize(s));
+        if (tc_err) return fail(MSC_ERR_CUDA, "tensor-core block inverse timed out on an mbarrier wait");
+    }
+    return MSC_OK;
+}
+
+int msc_plan_uses_tensor_cores(const msc_plan *p) { return (p && p->use_tc) ? p->tc_n : 0; }
 
 msc_status msc_intensities(msc_plan *p, int32_t s, const double *psi, double *intensities, void *stream)
 {

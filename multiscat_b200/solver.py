@@ -97,7 +97,7 @@ class ScatteringPlan:
     def __init__(self, potential_values, kinetic, systems: list[SystemSpec], *,
                  rtol: float = 1e-10, restart: int = 30, max_iterations: int = 2000,
                  precision: str = "fp64", inner_rtol: float = 0.0, inner_restart: int = 0,
-                 max_refinements: int = 0):
+                 max_refinements: int = 0, tensor_cores: bool | None = None):
         self._lib = nat.load()
         v = np.ascontiguousarray(np.asarray(potential_values), dtype=np.complex128)
         nkx, nky, nz = v.shape
@@ -116,6 +116,8 @@ class ScatteringPlan:
         desc.inner_restart = inner_restart
         desc.inner_rtol = inner_rtol
         desc.max_refinements = max_refinements
+        # tensor_cores: None = autotuned, True = always tcgen05, False = never
+        desc.flags = {None: 0, True: 2, False: 1}[tensor_cores]
         self._plan = ctypes.c_void_p()
         nat.check("msc_plan_create", self._lib.msc_plan_create(ctypes.byref(self._plan),
                                                               ctypes.byref(desc)))
@@ -209,6 +211,20 @@ class ScatteringPlan:
 
     def apply_operator(self, x: torch.Tensor) -> torch.Tensor:
         return self._debug("msc_debug_apply_operator", x)
+
+    def apply_block_inverse_f32(self, x: torch.Tensor) -> torch.Tensor:
+        """D^-1 x with the mixed form's FP32 kernel (x: complex64 [R, nz])."""
+        return self._debug("msc_debug_apply_block_inverse_f32", x)
+
+    def tuning_report(self) -> dict:
+        """Autotuner timings (us) and the kernel variants it chose."""
+        import json
+        return json.loads(self._lib.msc_plan_tuning_report(self._plan).decode())
+
+    @property
+    def tensor_core_tile(self) -> int:
+        """Tile width N of the tcgen05 block inverse (0 when it is not used)."""
+        return int(self._lib.msc_plan_uses_tensor_cores(self._plan))
 
 
 def full_grid_system(pkd, wave_a, wave_b, wave_c) -> SystemSpec:

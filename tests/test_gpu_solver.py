@@ -263,3 +263,43 @@ def test_mixed_batched_subsets_match_oracle_and_fp64():
                                    atol=MIXED_TOL)
     mixed.close()
     fp64.close()
+
+
+# ---------------------------------------------------------------------------
+# tcgen05 BF16x3 block inverse (mixed form) against the FP64 kernel.  BF16x3
+# keeps ~16 bits per operand, so the tolerance is 2e-4 relative to the
+# largest entry of the output row set.
+# ---------------------------------------------------------------------------
+TC_TOL = 2e-4
+
+
+@pytest.mark.parametrize("which", ["cfg0", "cfg1", "cfg2"])
+def test_tensor_core_block_inverse_matches_fp64(which):
+    if which == "cfg0":
+        case = cfg0_case()
+        systems = [case.system()]
+    elif which == "cfg1":
+        case = cfg1_case()
+        systems = [case.system()]
+    else:
+        case, systems = cfg2_batch(n_solves=5, seed=3)
+    mixed = ScatteringPlan(case.v, case.t, systems, precision="mixed", tensor_cores=True)
+    simt = ScatteringPlan(case.v, case.t, systems, precision="mixed", tensor_cores=False)
+    rows = mixed.total_rows
+    rng = np.random.default_rng(17)
+    x = rng.standard_normal((rows, case.v.shape[2])) + 1j * rng.standard_normal((rows, case.v.shape[2]))
+    x32 = torch.as_tensor(x.astype(np.complex64), device="cuda")
+    y_tc = mixed.apply_block_inverse_f32(x32).cpu().numpy()
+    assert mixed.tensor_core_tile > 0, "tcgen05 path not selected"
+    y_simt = simt.apply_block_inverse_f32(x32).cpu().numpy()
+    assert simt.tensor_core_tile == 0
+    scale = np.abs(y_simt).max()
+    np.testing.assert_allclose(y_tc, y_simt, rtol=0, atol=TC_TOL * scale)
+    if len(systems) == 1:
+        fp64 = ScatteringPlan(case.v, case.t, systems)
+        y64 = fp64.apply_block_inverse(torch.as_tensor(x32.cpu().numpy().astype(np.complex128),
+                                                       device="cuda")).cpu().numpy()
+        np.testing.assert_allclose(y_tc, y64, rtol=0, atol=TC_TOL * scale)
+        fp64.close()
+    mixed.close()
+    simt.close()
