@@ -196,9 +196,11 @@ msc_status msc_plan_get_info(const msc_plan *plan, msc_plan_info *info);
 
 /* Kernel timing (measurement only).  When enabled, the solve graphs carry
  * CUDA event pairs around every Arnoldi-step launch of kernel kind k
- * (0 = block-diagonal inverse, 1 = channel coupling) and msc_solve adds the
- * device time of the launches that did work.  msc_plan_kernel_timing copies
- * ms[2] and launches[2] accumulated since the previous call and resets them. */
+ * (0 = block-diagonal inverse, 1 = channel coupling, 2 = first projection,
+ * 3 = update + second projection + Givens, 4 = normalisation) and msc_solve
+ * adds the device time of the launches that did work.
+ * msc_plan_kernel_timing copies ms[5] and launches[5] accumulated since the
+ * previous call and resets them. */
 msc_status msc_plan_set_kernel_timing(msc_plan *plan, int enable);
 msc_status msc_plan_kernel_timing(msc_plan *plan, double *ms, int64_t *launches);
 

@@ -19,7 +19,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <tuple>
 #include <map>
 #include <mutex>
 #include <new>
@@ -134,9 +136,10 @@ struct msc_plan {
     int pstride = 0;
     // measurement
     bool timing = false;
-    std::vector<cudaEvent_t> tev;        // [2 kinds][m + 1 slots][start, stop]
-    double t_ms[2] = {0.0, 0.0};
-    int64_t t_launches[2] = {0, 0};
+    static constexpr int kKinds = 5;      // block inverse, coupling, projection 1, projection 2, normalize
+    std::vector<cudaEvent_t> tev;        // [kKinds][m + 1 slots][start, stop]
+    double t_ms[kKinds] = {};
+    int64_t t_launches[kKinds] = {};
     int *kcyc_host = nullptr;            // pinned [B]
     int64_t launches_last = 0;
     int cycles_last = 0;
@@ -460,11 +463,17 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
         if (tm) mark(p, 1, j, 1, st);
         const msc::ArnoldiArgs aa = arnoldi_args(p, p->active.p);
         const unsigned nblk = (unsigned)(p->ntiles * p->split);
+        if (tm) mark(p, 2, j, 0, st);
         msc::k_arnoldi_p1<R><<<nblk, 256, 0, st>>>(aa, Q, j + 1, W, p->h1.p, p->m + 2);
+        if (tm) mark(p, 2, j, 1, st);
+        if (tm) mark(p, 3, j, 0, st);
         msc::k_arnoldi_p2<R><<<nblk, 256, 0, st>>>(aa, Q, j + 1, W, p->state(), p->m, j,
                                                    p->desc.rtol, p->desc.max_iterations, inner);
+        if (tm) mark(p, 3, j, 1, st);
+        if (tm) mark(p, 4, j, 0, st);
         launch_update_t<R>(p, p->active.p, Q, j + 1, nullptr, p->h2.p, p->m + 2, W, p->scale.p, Qn,
                            0, st);
+        if (tm) mark(p, 4, j, 1, st);
     }
     msc::k_trisolve<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m);
     launch_update_t<R>(p, p->kcyc.p, Q, 0, p->kcyc.p, p->y.p, p->m, nullptr, nullptr, U, 1, st);
@@ -511,7 +520,7 @@ void accumulate_timing(msc_plan *p)
     int maxk = 0;
     for (int s = 0; s < p->B; ++s) maxk = std::max(maxk, p->kcyc_host[s]);
     if (maxk == 0) return;
-    for (int kind = 0; kind < 2; ++kind) {
+    for (int kind = 0; kind < msc_plan::kKinds; ++kind) {
         for (int j = 0; j < maxk; ++j) {
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, tev_at(p, kind, j, 0), tev_at(p, kind, j, 1)) == cudaSuccess) {
@@ -724,7 +733,87 @@ float time_launch(msc_plan *p, F f)
 // and keep the fastest.  Coupling: halo tiles vs neighbour table, for each
 // precision the solve uses.  Mixed form: tcgen05 tile width N (and the SIMT
 // FP32 kernel).  Runs once per plan, before the solve graphs are captured.
+struct TuneKey {
+    int n, R, K, nkx, nky, B, mixed, hx, hy, tcmax, flags;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(n, R, K, nkx, nky, B, mixed, hx, hy, tcmax, flags) <
+               std::tie(o.n, o.R, o.K, o.nkx, o.nky, o.B, o.mixed, o.hx, o.hy, o.tcmax, o.flags);
+    }
+};
+struct TuneChoice {
+    int halo64, halo32, use_tc, tc_n;
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, TuneChoice> g_tune_cache;
+
+msc_status autotune_measure(msc_plan *p);
+
+void apply_tc_width(msc_plan *p, int N)
+{
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    p->tc_n = N;
+    p->tc_tile_rows = N / 2;
+    p->tc_ntiles = (p->R + N / 2 - 1) / (N / 2);
+    p->tc_grid = std::min(p->tc_ntiles, sms);
+}
+
+// Autotuner front end: reuse the choices of an earlier plan of the same
+// shape (same sizes, batch, tap reach and options), else measure.
+// MSC_TUNE="c64=K,c32=K,bi=N" fixes the choices (K: 0 neighbour table,
+// 1 halo 8 y/thread, 2 halo 4 y/thread; N: tcgen05 tile width, 0 = SIMT).
+// Profiling runs use it so that a profiler's overhead cannot change what the
+// autotuner picks.
+bool tune_from_env(msc_plan *p)
+{
+    const char *env = std::getenv("MSC_TUNE");
+    if (!env || !*env) return false;
+    int c64 = p->halo64, c32 = p->halo32, bi = p->use_tc ? p->tc_n : 0;
+    std::sscanf(env, "c64=%d,c32=%d,bi=%d", &c64, &c32, &bi);
+    p->halo64 = p->use_halo ? std::max(0, std::min(2, c64)) : 0;
+    p->halo32 = p->use_halo ? std::max(0, std::min(2, c32)) : 0;
+    if (p->use_tc) {
+        if (bi == 0) {
+            p->use_tc = false;
+        } else {
+            int N = 16;
+            while (N < bi && N < p->tc_n) N *= 2;
+            apply_tc_width(p, N);
+        }
+    }
+    p->tune_log.push_back({"from_MSC_TUNE", 1.f});
+    return true;
+}
+
 msc_status autotune(msc_plan *p)
+{
+    if (tune_from_env(p)) return MSC_OK;
+    const TuneKey key{p->n, p->R, p->K, p->nkx, p->nky, p->B, p->mixed ? 1 : 0, p->halo_hx,
+                      p->halo_hy, p->use_tc ? p->tc_n : 0, p->desc.flags};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            p->halo64 = it->second.halo64;
+            p->halo32 = it->second.halo32;
+            if (p->use_tc) {
+                p->use_tc = it->second.use_tc != 0;
+                if (p->use_tc) apply_tc_width(p, it->second.tc_n);
+            }
+            p->tune_log.push_back({"cached", 1.f});
+            return MSC_OK;
+        }
+    }
+    msc_status st = autotune_measure(p);
+    if (st != MSC_OK) return st;
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = TuneChoice{p->halo64, p->halo32, p->use_tc ? 1 : 0, p->tc_n};
+    return MSC_OK;
+}
+
+msc_status autotune_measure(msc_plan *p)
 {
     const size_t vs = (size_t)p->R * p->n;
     MSC_CUDA(cudaMemsetAsync(p->X.p, 0, vs * sizeof(double2), p->stream));
@@ -1003,7 +1092,7 @@ msc_status finalize(msc_plan *p)
     }
     MSC_CUDA(cudaMallocHost(&p->kcyc_host, p->B * sizeof(int)));
     for (int s = 0; s < p->B; ++s) p->kcyc_host[s] = 0;
-    p->tev.resize((size_t)2 * (m + 1) * 2);
+    p->tev.resize((size_t)msc_plan::kKinds * (m + 1) * 2);
     for (cudaEvent_t &e : p->tev) MSC_CUDA(cudaEventCreate(&e));
     msc_status st = capture(p, record_cycle_start, &p->g_start, &p->launches_start);
     if (st != MSC_OK) return st;
@@ -1011,6 +1100,35 @@ msc_status finalize(msc_plan *p)
     if (st != MSC_OK) return st;
     p->finalized = true;
     return MSC_OK;
+}
+
+// Process-wide caches.  Sweeps build many plans over one potential (new
+// beams, same z grid): the H0 eigen-decomposition and the autotuner's
+// choices are reused instead of recomputed.
+struct EigenEntry {
+    std::vector<double> H, lam, E;
+};
+std::mutex g_cache_mutex;
+std::vector<EigenEntry> g_eigen_cache;   // few entries, most recent last
+
+bool eigen_cache_lookup(const std::vector<double> &H, std::vector<double> &lam, std::vector<double> &E)
+{
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    for (const EigenEntry &e : g_eigen_cache)
+        if (e.H.size() == H.size() && std::memcmp(e.H.data(), H.data(), H.size() * sizeof(double)) == 0) {
+            lam = e.lam;
+            E = e.E;
+            return true;
+        }
+    return false;
+}
+
+void eigen_cache_store(const std::vector<double> &H, const std::vector<double> &lam,
+                       const std::vector<double> &E)
+{
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    if (g_eigen_cache.size() >= 8) g_eigen_cache.erase(g_eigen_cache.begin());
+    g_eigen_cache.push_back({H, lam, E});
 }
 
 }  // namespace
@@ -1087,10 +1205,13 @@ msc_status msc_plan_set_potential(msc_plan *p, const double *potential_values, c
     }
     for (double hv : H)
         if (!std::isfinite(hv)) return fail(MSC_ERR_NONFINITE, "non-finite kinetic or V00");
-    p->lam_host.resize(n);
-    p->E_host.resize((size_t)n * n);
-    if (msc::symmetric_eigh(n, H.data(), p->lam_host.data(), p->E_host.data()) != 0)
-        return fail(MSC_ERR_EIGEN, "eigensolver did not converge");
+    if (!eigen_cache_lookup(H, p->lam_host, p->E_host)) {
+        p->lam_host.resize(n);
+        p->E_host.resize((size_t)n * n);
+        if (msc::symmetric_eigh(n, H.data(), p->lam_host.data(), p->E_host.data()) != 0)
+            return fail(MSC_ERR_EIGEN, "eigensolver did not converge");
+        eigen_cache_store(H, p->lam_host, p->E_host);
+    }
     p->en_host.resize(n);
     for (int k = 0; k < n; ++k) p->en_host[k] = p->E_host[(size_t)(n - 1) * n + k];
     std::vector<double> ET((size_t)n * n);
@@ -1292,15 +1413,17 @@ msc_status msc_plan_set_kernel_timing(msc_plan *p, int enable)
     const bool want = enable != 0;
     if (want == p->timing) return MSC_OK;
     p->timing = want;
-    p->t_ms[0] = p->t_ms[1] = 0.0;
-    p->t_launches[0] = p->t_launches[1] = 0;
+    for (int k = 0; k < msc_plan::kKinds; ++k) {
+        p->t_ms[k] = 0.0;
+        p->t_launches[k] = 0;
+    }
     return capture(p, record_cycle_iterations, &p->g_iter, &p->launches_iter);
 }
 
 msc_status msc_plan_kernel_timing(msc_plan *p, double *ms, int64_t *launches)
 {
     if (!p || !ms || !launches) return fail(MSC_ERR_ARG, "null argument");
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < msc_plan::kKinds; ++k) {
         ms[k] = p->t_ms[k];
         launches[k] = p->t_launches[k];
         p->t_ms[k] = 0.0;

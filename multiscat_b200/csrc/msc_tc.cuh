@@ -19,9 +19,10 @@
 // CTA.  The B operands (x, then yt) are staged per tile of channels by the
 // threads themselves (FP32 -> BF16 hi/lo, re/im de-interleaved).
 //
-// Execution.  Persistent CTAs (one per SM, 128 threads = 4 warps).  Per tile:
+// Execution.  Persistent CTAs (one per SM, 256 threads = 8 warps).  Per tile:
 // stage B, one thread issues the MMAs and commits to an mbarrier, all warps
-// read the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31),
+// read the accumulator with tcgen05.ld (warp w owns TMEM lanes
+// 32 (w % 4)..32 (w % 4) + 31 and the column half w / 4),
 // form the Sherman-Morrison scalars and yt (pkd + lam in FP64), stage yt as
 // the next B operand, second GEMM, store u.  Every mbarrier wait is bounded;
 // on time-out the kernel records an error code, stops issuing work and still
@@ -35,7 +36,7 @@
 namespace msc {
 namespace tc {
 
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;   // 8 warps: warp w reads TMEM lanes 32 (w % 4).., columns half w / 4
 constexpr long long kSpinLimit = 1ll << 26;   // polls before a wait is declared hung
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -199,11 +200,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar_e, bar_mma;
     __shared__ uint32_t tmem_base_s;
-    __shared__ float sm_part[4][2][N];        // Sherman-Morrison partial sums [warp][M tile][col]
+    __shared__ float sm_part[8][2][N];        // Sherman-Morrison partial sums [warp][M tile][col]
     __shared__ float2 beta_s[TR];
     __shared__ double pkd_s[TR];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int lq = warp & 3;                              // TMEM lane quarter of this warp
+    constexpr int HALF = (N >= 32) ? N / 2 : N;           // columns per warp group
+    const int c_begin = (N >= 32) ? (warp >> 2) * HALF : 0;
+    const bool epi = (N >= 32) || warp < 4;               // N = 16: warps 4-7 sit out the epilogues
     const int n = prm.n, kp = prm.kp, mt_count = prm.mt;
     const int kb = kp >> 3;                               // 8-blocks along z and k
     const uint32_t part_bytes = (uint32_t)kp * kp * 2u;   // one of E_hi / E_lo
@@ -323,14 +328,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         if (!__syncthreads_and(ok)) { ok = false; break; }
 
         // ---- epilogue 1a: Sherman-Morrison sums s_j = sum_k en_k xt_kj / (pkd_j + lam_k)
-        for (int m = 0; m < mt_count; ++m) {
-            const int k = m * 128 + warp * 32 + lane;
+        for (int m = 0; m < mt_count && epi; ++m) {
+            const int k = m * 128 + lq * 32 + lane;
             const bool valid = k < n;
             const double lam_k = valid ? prm.lam[k] : 0.0;
             const float en_k = valid ? (float)prm.en[k] : 0.f;
-            for (int c0 = 0; c0 < N; c0 += 16) {
+            for (int c0 = c_begin; c0 < c_begin + HALF; c0 += 16) {
                 float v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(m * N + c0), v);
+                tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + c0), v);
 #pragma unroll
                 for (int c = 0; c < 16; c += 2) {
                     const int j = (c0 + c) >> 1;
@@ -354,8 +359,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
             double2 b = make_double2(0.0, 0.0);
             if (j < nrow) {
                 double sr = 0.0, si = 0.0;   // fixed summation order: deterministic
+                const int wg = (N >= 32) ? ((2 * j) / HALF) * 4 : 0;   // warps that own column 2j
                 for (int m = 0; m < mt_count; ++m)
-                    for (int w = 0; w < 4; ++w) {
+                    for (int w = wg; w < wg + 4; ++w) {
                         sr += sm_part[w][m][2 * j];
                         si += sm_part[w][m][2 * j + 1];
                     }
@@ -369,15 +375,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
 
         // ---- epilogue 1b: yt = (xt + beta en) / (pkd + lam) as the B operand of GEMM 2
         // (rows = 2 TR columns, K = k; rows k >= kp are never read, k in [n, kp) are zero)
-        for (int m = 0; m < mt_count; ++m) {
-            const int k = m * 128 + warp * 32 + lane;
+        for (int m = 0; m < mt_count && epi; ++m) {
+            const int k = m * 128 + lq * 32 + lane;
             const bool valid = k < n;
             const bool stage = k < kp;
             const double lam_k = valid ? prm.lam[k] : 0.0;
             const float en_k = valid ? (float)prm.en[k] : 0.f;
-            for (int c0 = 0; c0 < N; c0 += 16) {
+            for (int c0 = c_begin; c0 < c_begin + HALF; c0 += 16) {
                 float v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(m * N + c0), v);
+                tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + c0), v);
                 if (!stage) continue;
 #pragma unroll
                 for (int c = 0; c < 16; c += 2) {
@@ -435,11 +441,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         if (!__syncthreads_and(ok)) { ok = false; break; }
 
         // ---- epilogue 2: u rows to global (z contiguous across lanes)
-        for (int m = 0; m < mt_count; ++m) {
-            const int z = m * 128 + warp * 32 + lane;
-            for (int c0 = 0; c0 < N; c0 += 16) {
+        for (int m = 0; m < mt_count && epi; ++m) {
+            const int z = m * 128 + lq * 32 + lane;
+            for (int c0 = c_begin; c0 < c_begin + HALF; c0 += 16) {
                 float v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((mt_count + m) * N + c0), v);
+                tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)((mt_count + m) * N + c0), v);
                 if (z < n) {
 #pragma unroll
                     for (int c = 0; c < 16; c += 2) {

@@ -187,11 +187,12 @@ class ScatteringPlan:
                   self._lib.msc_plan_set_kernel_timing(self._plan, 1 if on else 0))
 
     def kernel_timing(self) -> dict:
-        ms = (ctypes.c_double * 2)()
-        cnt = (ctypes.c_int64 * 2)()
+        ms = (ctypes.c_double * 5)()
+        cnt = (ctypes.c_int64 * 5)()
         nat.check("msc_plan_kernel_timing", self._lib.msc_plan_kernel_timing(self._plan, ms, cnt))
-        return {"block_inverse": {"ms": ms[0], "launches": cnt[0]},
-                "coupling": {"ms": ms[1], "launches": cnt[1]}}
+        names = ("block_inverse", "coupling", "arnoldi_project", "arnoldi_update_project",
+                 "arnoldi_normalize")
+        return {k: {"ms": ms[i], "launches": cnt[i]} for i, k in enumerate(names)}
 
     # debug operators on one full-grid system (x, y: complex128 [C, nz] cuda tensors)
     def _debug(self, name: str, x: torch.Tensor) -> torch.Tensor:
