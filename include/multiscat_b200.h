@@ -66,7 +66,11 @@ typedef struct {
     int32_t max_refinements;/* mixed: outer FP64 refinement steps (0 = 30)      */
     int32_t flags;          /* bit 0: mixed form without the tcgen05 kernel;
                                bit 1: keep the tcgen05 kernel even when the
-                               autotuner times the SIMT kernel faster          */
+                               autotuner times the SIMT kernel faster;
+                               bit 2: mixed form with ONE Gram-Schmidt pass
+                               (Pythagorean norm) in the inner solve instead
+                               of two; fewer bytes per iteration, but on
+                               ill-conditioned batches more iterations        */
 } msc_plan_desc;
 
 typedef struct msc_plan msc_plan;
@@ -203,6 +207,53 @@ msc_status msc_plan_get_info(const msc_plan *plan, msc_plan_info *info);
  * previous call and resets them. */
 msc_status msc_plan_set_kernel_timing(msc_plan *plan, int enable);
 msc_status msc_plan_kernel_timing(msc_plan *plan, double *ms, int64_t *launches);
+
+/* ---- Adjoint differentiation (no counterpart in the reference, which has
+ * no derivatives; the operator transposed is the one of
+ * multiscat_gmres.f90:452-687 / _scipy.py:336-354).
+ *
+ * Forward:  A psi = u,  S_G = 2i b_G psi_G(z_n) + delta_{G,spec} a_spec.
+ * For a real loss L(S) with gamma_G = dL/dRe S_G + i dL/dIm S_G:
+ *   1. msc_plan_set_adjoint(plan, 1)                     operator -> A^H
+ *   2. msc_plan_set_adjoint_rhs(plan, psi, dL/dI, dL/dS)  u_G = -i gamma_G conj(b_G)
+ *   3. msc_solve(plan, lambda, NULL, ...)                 A^H lambda = u
+ *   4. msc_potential_gradient(plan, psi, lambda, ...)     dL/dV
+ *   5. msc_plan_set_adjoint(plan, 0); msc_plan_set_boundary_rhs(plan, NULL, ...)
+ * The plan keeps its eigenbasis, tuning and graphs throughout. */
+
+/* Select the operator the plan solves with: 0 = A, 1 = A^H (coupling taps
+ * conj(V_{-d}) at offset d and c_G -> conj(c_G); D's eigenbasis is real and
+ * unchanged).  Synchronises the device; no work of the plan may be in
+ * flight.  msc_debug_apply_operator follows the selection. */
+msc_status msc_plan_set_adjoint(msc_plan *plan, int32_t adjoint);
+int msc_plan_is_adjoint(const msc_plan *plan);
+
+/* Right-hand side on the outer boundary: rhs complex [total_rows] (plan row
+ * order) is the source at z_n of each channel row; every other entry of the
+ * right-hand side is zero.  rhs = NULL restores the scattering source
+ * (b_spec at each system's specular row).  on_device != 0: rhs is a device
+ * pointer read in order on `stream`.  Per-system norms are recomputed; a
+ * system whose right-hand side is zero solves to psi = 0 at once. */
+msc_status msc_plan_set_boundary_rhs(msc_plan *plan, const double *rhs, int32_t on_device,
+                                     void *stream);
+
+/* Adjoint right-hand side u_G = -i gamma_G conj(b_G) at z_n with
+ * gamma = 2 dl_dintensity[G] S_G + dl_damplitude[G], S from psi (the
+ * forward solution, complex [total_rows][n_z]).  Device pointers, in order on
+ * `stream`; dl_dintensity (double [total_rows]) or dl_damplitude (complex
+ * [total_rows]) may be NULL. */
+msc_status msc_plan_set_adjoint_rhs(msc_plan *plan, const double *psi, const double *dl_dintensity,
+                                    const double *dl_damplitude, void *stream);
+
+/* dL/dV for the potential layout [nkx][nky][n_z] (complex, device), from
+ * psi and lambda (device, complex [total_rows][n_z]), summed over the plan's
+ * systems: grad[d][z] = -2 conj(K_d(z)) for d != 0 and -2 Re K_0(z) for
+ * d = 0 (only Re V_0 enters), K_d(z) = sum_G conj(lambda_G(z)) psi_{G-d}(z),
+ * in the (dL/dRe + i dL/dIm) convention.  half_x/half_y >= 0 restrict d to
+ * |dx| <= half_x, |dy| <= half_y (signed torus offsets; entries outside are
+ * written as 0); -1 = every offset of the torus. */
+msc_status msc_potential_gradient(msc_plan *plan, const double *psi, const double *lambda,
+                                  int32_t half_x, int32_t half_y, double *grad, void *stream);
 
 /* Human-readable text of the last error on this thread. */
 const char *msc_last_error(void);

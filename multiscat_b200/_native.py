@@ -20,7 +20,9 @@ EXPORTED = (
     "msc_debug_apply_block_inverse", "msc_debug_apply_operator", "msc_intensities",
     "msc_last_error", "msc_version", "msc_plan_get_info", "msc_plan_set_kernel_timing",
     "msc_plan_kernel_timing", "msc_apply_operator_noalloc", "msc_debug_apply_block_inverse_f32",
-    "msc_plan_uses_tensor_cores", "msc_plan_tuning_report",
+    "msc_plan_uses_tensor_cores", "msc_plan_tuning_report", "msc_plan_set_adjoint",
+    "msc_plan_is_adjoint", "msc_plan_set_boundary_rhs", "msc_plan_set_adjoint_rhs",
+    "msc_potential_gradient",
 )
 
 MSC_OK = 0
@@ -133,6 +135,16 @@ def load() -> ctypes.CDLL:
     lib.msc_plan_tuning_report.argtypes = [_vp]
     lib.msc_plan_uses_tensor_cores.restype = ctypes.c_int
     lib.msc_plan_uses_tensor_cores.argtypes = [_vp]
+    lib.msc_plan_set_adjoint.restype = ctypes.c_int
+    lib.msc_plan_set_adjoint.argtypes = [_vp, ctypes.c_int32]
+    lib.msc_plan_is_adjoint.restype = ctypes.c_int
+    lib.msc_plan_is_adjoint.argtypes = [_vp]
+    lib.msc_plan_set_boundary_rhs.restype = ctypes.c_int
+    lib.msc_plan_set_boundary_rhs.argtypes = [_vp, _vp, ctypes.c_int32, _vp]
+    lib.msc_plan_set_adjoint_rhs.restype = ctypes.c_int
+    lib.msc_plan_set_adjoint_rhs.argtypes = [_vp, _vp, _vp, _vp, _vp]
+    lib.msc_potential_gradient.restype = ctypes.c_int
+    lib.msc_potential_gradient.argtypes = [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp]
     lib.msc_last_error.restype = ctypes.c_char_p
     lib.msc_last_error.argtypes = []
     lib.msc_version.restype = ctypes.c_char_p

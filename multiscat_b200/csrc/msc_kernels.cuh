@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(256)
 k_residual_diag(Tiles tiles, const int *__restrict__ gate, int n,
                 const double *__restrict__ Tm, const double *__restrict__ v00,
                 const double *__restrict__ row_pkd, const double2 *__restrict__ row_c,
-                const int *__restrict__ sys_spec_row, const double2 *__restrict__ sys_bspec,
+                const double2 *__restrict__ row_rhs,
                 const double2 *__restrict__ x, double2 *__restrict__ out, int with_b)
 {
     constexpr int TR = kTileRows;
@@ -201,8 +201,6 @@ k_residual_diag(Tiles tiles, const int *__restrict__ gate, int n,
     if (gate && gate[sys] == 0) return;
     const int row0 = tiles.row0[tile];
     const int nrow = tiles.nrow[tile];
-    const int spec_row = sys_spec_row[sys];
-    const double2 bspec = sys_bspec[sys];
 
     for (int idx = threadIdx.x; idx < TR * n; idx += blockDim.x) {
         int r = idx / n, z = idx - r * n;
@@ -242,7 +240,7 @@ k_residual_diag(Tiles tiles, const int *__restrict__ gate, int n,
                 double2 d = make_double2(acc[2 * rr] + diag * xz.x, acc[2 * rr + 1] + diag * xz.y);
                 if (z == n - 1) d = csub(d, cmul(row_c[row], xz));
                 double2 o = make_double2(-d.x, -d.y);
-                if (with_b && row == spec_row && z == n - 1) o = cadd(o, bspec);
+                if (with_b && z == n - 1) o = cadd(o, row_rhs[row]);
                 out[(size_t)row * n + z] = o;
             }
         }
@@ -631,6 +629,12 @@ __global__ void k_cycle_start(GmresState st, int nsys, int m, const double2 *__r
     st.kcyc[s] = 0;
     if (!st.unfinished[s]) return;
     const double beta = sqrt(fmax(nrm[(size_t)s * nstride].x, 0.0));
+    if (beta == 0.0) {                  // exact (also: zero right-hand side)
+        st.resid[s] = 0.0;
+        st.unfinished[s] = 0;
+        st.status[s] = 0;
+        return;
+    }
     const double rel = beta / st.bnorm[s];
     st.resid[s] = rel;
     if (!isfinite(beta)) {
@@ -664,8 +668,10 @@ __global__ void k_cycle_start(GmresState st, int nsys, int m, const double2 *__r
 // max(rtol ||b||, inner_rtol beta0) (inner_rtol > 0 only for the mixed
 // form, whose FP32 inner solve cannot go below its own rounding level).
 __device__ void arnoldi_givens(GmresState &st, int s, int m, int j, double rtol, int max_iter,
-                               double inner_rtol)
+                               double inner_rtol, bool use_h1 = true)
 {
+    // use_h1 = false: one Gram-Schmidt pass (h2 holds the projections and
+    // h2[j+1] the squared norm of w before projection; beta by Pythagoras).
     if (!st.active[s]) return;
     const int hs = m + 2;
     const double2 *h1 = st.h1 + (size_t)s * hs;
@@ -676,7 +682,7 @@ __device__ void arnoldi_givens(GmresState &st, int s, int m, int j, double rtol,
     double2 *g = st.g + (size_t)s * (m + 1);
     double proj2 = 0.0;
     for (int i = 0; i <= j; ++i) {
-        H[i] = cadd(h1[i], h2[i]);
+        H[i] = use_h1 ? cadd(h1[i], h2[i]) : h2[i];
         proj2 += cabs2(h2[i]);
     }
     const double w2 = h2[j + 1].x;          // ||W'||^2 after the first pass
@@ -900,11 +906,14 @@ __device__ void arnoldi_givens(GmresState &st, int s, int m, int j, double rtol,
                                double inner_rtol);
 
 // P2: w <- w - Q h1 ; h2 = Q^H w, |w|^2 ; then the Givens step of the system.
+// With cgs2 = 0 (single Gram-Schmidt pass) there is no h1 and no update:
+// h2 = Q^H w and |w|^2 come from the unprojected w and the Givens step takes
+// beta^2 = |w|^2 - |h2|^2.
 template <typename R>
 __global__ void __launch_bounds__(256)
 k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
              typename CT<R>::t *__restrict__ W, GmresState st, int m, int j, double rtol,
-             int max_iter, double inner_rtol)
+             int max_iter, double inner_rtol, int cgs2)
 {
     using C2 = typename CT<R>::t;
     __shared__ C2 cf[kMaxRestart + 1];
@@ -912,14 +921,15 @@ k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
     const int s = a.tiles.sys[tile];
     if (a.gate && a.gate[s] == 0) return;
     const int hs = m + 2;
+    size_t e0;
+    int ne;
+    elem_range<R>(a, tile, sub, e0, ne);
+    if (cgs2) {
     for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
         const double2 c = st.h1[(size_t)s * hs + i];
         cf[i] = mk2<R>((R)c.x, (R)c.y);
     }
     __syncthreads();
-    size_t e0;
-    int ne;
-    elem_range<R>(a, tile, sub, e0, ne);
     for (int e = threadIdx.x; e < ne; e += blockDim.x) {
         C2 w = W[e0 + e];
         for (int i = 0; i < nvec; ++i) {
@@ -931,9 +941,10 @@ k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
         W[e0 + e] = w;
     }
     __syncthreads();
+    }   // cgs2
     block_project<R>(a, Q, nvec, W, e0, ne, 1, a.partial + (size_t)blockIdx.x * a.pstride);
     if (last_block_reduce(a, s, nvec + 1, st.h2 + (size_t)s * hs)) {
-        if (threadIdx.x == 0) arnoldi_givens(st, s, m, j, rtol, max_iter, inner_rtol);
+        if (threadIdx.x == 0) arnoldi_givens(st, s, m, j, rtol, max_iter, inner_rtol, cgs2 != 0);
     }
 }
 
@@ -952,6 +963,129 @@ __global__ void k_intensities(int nrows, int row_offset, int n, const int *__res
     double2 amp = cmul(make_double2(0.0, 2.0), cmul(b, p));
     if (row + row_offset == sys_spec_row[s]) amp = cadd(amp, sys_aspec[s]);
     out[row] = cabs2(amp);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint (no counterpart in the reference, which has no derivatives).
+//
+// Forward:  A psi = u_fwd,  S_G = 2i b_G psi_G(z_n) + delta_{G,spec} a_spec.
+// For a real loss L with gamma_G = dL/dS_G in the (Re + i Im) convention,
+// dL = Re sum conj(gamma_G) dS_G = 2 Re <u, d psi> with the outer-boundary
+// vector u_G(z_n) = -i gamma_G conj(b_G).  With A^H lambda = u and
+// d psi = -A^{-1} (dA) psi:  dL = -2 Re <lambda, (dA) psi>.
+// ---------------------------------------------------------------------------
+
+// u_G = -i gamma_G conj(b_G),  gamma_G = 2 dl_di[G] S_G + dl_ds[G]
+// (either input may be null).
+__global__ void k_adjoint_rhs(int nrows, int n, const int *__restrict__ row_sys,
+                              const int *__restrict__ sys_spec_row,
+                              const double2 *__restrict__ sys_aspec,
+                              const double2 *__restrict__ row_b, const double2 *__restrict__ psi,
+                              const double *__restrict__ dl_di, const double2 *__restrict__ dl_ds,
+                              double2 *__restrict__ rhs)
+{
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= nrows) return;
+    const double2 b = row_b[row];
+    double2 gamma = make_double2(0.0, 0.0);
+    if (dl_di) {
+        const int s = row_sys[row];
+        const double2 p = psi[(size_t)row * n + (n - 1)];
+        double2 amp = cmul(make_double2(0.0, 2.0), cmul(b, p));
+        if (row == sys_spec_row[s]) amp = cadd(amp, sys_aspec[s]);
+        gamma = cscale(amp, 2.0 * dl_di[row]);
+    }
+    if (dl_ds) gamma = cadd(gamma, dl_ds[row]);
+    rhs[row] = cmul(make_double2(0.0, -1.0), cmul(gamma, cconj(b)));
+}
+
+// bnorm[s] = || rhs restricted to system s ||  (one block per system, fixed
+// summation order).
+__global__ void __launch_bounds__(256)
+k_system_norms(const int *__restrict__ sys_row0, const double2 *__restrict__ rhs,
+               double *__restrict__ bnorm)
+{
+    __shared__ double ws[8];
+    const int s = blockIdx.x;
+    double acc = 0.0;
+    for (int r = sys_row0[s] + threadIdx.x; r < sys_row0[s + 1]; r += blockDim.x)
+        acc += cabs2(rhs[r]);
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+        bnorm[s] = sqrt(t);
+    }
+}
+
+// dL/dV_D(z) for every torus offset D = (dx, dy) in a window, summed over the
+// systems of the plan (they share V):
+//   K_D(z) = sum_s sum_{G in s, G - D in s} conj(lambda_G(z)) psi_{G-D}(z)
+//   grad[D][z] = -2 conj(K_D(z))   (D != 0: the coupling uses V_D, complex)
+//   grad[0][z] = -2 Re K_0(z)       (only Re V_0 enters the diagonal)
+// in the (dL/dRe + i dL/dIm) convention.  A per-z correlation of lambda with
+// psi over the channel torus ("outer product" restricted to its diagonals).
+// Layout: grad [nkx][nky][n], the potential's own layout.
+// Grid: x = window offsets / (8 warps * kGradPerWarp), y = z / 32.  Lane = z,
+// so psi / lambda rows ([row][z]) are read coalesced; each (D, z) is summed by
+// one thread in a fixed order.
+constexpr int kGradPerWarp = 4;
+
+__global__ void __launch_bounds__(256)
+k_potential_gradient(int nkx, int nky, int n, int nsys, const int *__restrict__ sys_row0,
+                     const int *__restrict__ row_pos, const int *__restrict__ pos_map,
+                     int wx, int wy, int hx, int hy, const double2 *__restrict__ psi,
+                     const double2 *__restrict__ lam, double2 *__restrict__ grad)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int z = blockIdx.y * 32 + lane;
+    const int nwin = wx * wy;
+    const int d0 = (blockIdx.x * 8 + warp) * kGradPerWarp;
+    if (d0 >= nwin) return;
+    int dx[kGradPerWarp], dy[kGradPerWarp];
+    double2 acc[kGradPerWarp];
+#pragma unroll
+    for (int k = 0; k < kGradPerWarp; ++k) {
+        const int d = min(d0 + k, nwin - 1);
+        const int ux = d / wy, uy = d - ux * wy;
+        dx[k] = ((ux - hx) % nkx + nkx) % nkx;
+        dy[k] = ((uy - hy) % nky + nky) % nky;
+        acc[k] = make_double2(0.0, 0.0);
+    }
+    const int ntor = nkx * nky;
+    const bool zok = z < n;
+    for (int s = 0; s < nsys; ++s) {
+        const int *map = pos_map + (size_t)s * ntor;
+        for (int r = sys_row0[s]; r < sys_row0[s + 1]; ++r) {
+            const double2 l = zok ? lam[(size_t)r * n + z] : make_double2(0.0, 0.0);
+            const int pos = row_pos[r];
+            const int ix = pos / nky, iy = pos - ix * nky;
+#pragma unroll
+            for (int k = 0; k < kGradPerWarp; ++k) {
+                int sx = ix - dx[k];
+                sx += (sx < 0) ? nkx : 0;
+                int sy = iy - dy[k];
+                sy += (sy < 0) ? nky : 0;
+                const int r2 = __ldg(map + sx * nky + sy);
+                if (r2 >= 0 && zok) {
+                    const double2 q = psi[(size_t)r2 * n + z];
+                    // conj(l) * q
+                    acc[k].x = fma(l.x, q.x, fma(l.y, q.y, acc[k].x));
+                    acc[k].y = fma(l.x, q.y, fma(-l.y, q.x, acc[k].y));
+                }
+            }
+        }
+    }
+    if (!zok) return;
+#pragma unroll
+    for (int k = 0; k < kGradPerWarp; ++k) {
+        if (d0 + k >= nwin) break;
+        const size_t o = ((size_t)dx[k] * nky + dy[k]) * n + z;
+        grad[o] = (dx[k] == 0 && dy[k] == 0) ? make_double2(-2.0 * acc[k].x, 0.0)
+                                             : make_double2(-2.0 * acc[k].x, 2.0 * acc[k].y);
+    }
 }
 
 __global__ void k_scale(double2 *p, size_t count, double sc)

@@ -93,14 +93,19 @@ struct msc_plan {
     std::vector<double> T_host, v00_host, lam_host, E_host, en_host;
     std::vector<std::pair<int, int>> taps;     // (dx, dy) storage offsets
     std::vector<double2> Vt_host;              // [K][n]
+    std::vector<double2> Vt_adj_host;          // [K][n] taps of A^H: conj(V_{-d}) at offset d
     int K = 0;
+    bool adjoint = false;                      // operator in use: A (false) or A^H (true)
     std::vector<SystemHost> sys;
     // rows / tiles
     int R = 0, ntiles = 0;
     std::vector<int> tile_row0_h, tile_nrow_h, tile_sys_h, sys_tile0_h, sys_row0_h, row_sys_h;
     // device data
     DevBuf<double> E, ET, Tm, lam, en, v00, row_pkd, row_fn;
-    DevBuf<double2> Vt, row_c, row_b, sys_bspec, sys_aspec;
+    DevBuf<double2> Vt, row_c, row_b, row_rhs, sys_aspec;
+    std::vector<double2> row_c_h, rhs_default_h;   // c per row; default right-hand side
+    DevBuf<int> row_pos, pos_map;                  // gradient tables (built on first use)
+    DevBuf<int> sys_row0;                          // [B + 1] first row of each system
     DevBuf<int> nbr, tile_row0, tile_nrow, tile_sys, sys_tile0, sys_spec_row, row_sys;
     // solver state
     DevBuf<double2> X, W, U, TMP, Q, partial;
@@ -108,6 +113,7 @@ struct msc_plan {
     DevBuf<double> scale, bnorm, resid, est, beta0;
     // mixed form: FP32 copies of the operator data and the FP32 Krylov space
     bool mixed = false;
+    bool cgs1_inner = false;       // single Gram-Schmidt pass in the FP32 inner solve
     double inner_rtol = 0.0;
     int max_cycles = 0;
     DevBuf<float> E32, ET32, lam32, en32, row_pkd32, row_fn32;
@@ -155,7 +161,8 @@ struct msc_plan {
         if (stream) cudaStreamDestroy(stream);
         E.release(); ET.release(); Tm.release(); lam.release(); en.release(); v00.release();
         row_pkd.release(); row_fn.release(); Vt.release(); row_c.release(); row_b.release();
-        sys_bspec.release(); sys_aspec.release(); nbr.release(); tile_row0.release();
+        row_rhs.release(); sys_aspec.release(); row_pos.release(); pos_map.release();
+        sys_row0.release(); nbr.release(); tile_row0.release();
         tile_nrow.release(); tile_sys.release(); sys_tile0.release(); sys_spec_row.release();
         row_sys.release(); X.release(); W.release(); U.release(); TMP.release(); Q.release();
         partial.release(); H.release(); cs.release(); sn.release(); g.release(); h1.release();
@@ -190,6 +197,16 @@ cudaError_t upload(DevBuf<T> &buf, const std::vector<T> &h)
 {
     cudaError_t e = buf.alloc(h.size());
     if (e != cudaSuccess) return e;
+    if (h.empty()) return cudaSuccess;
+    return cudaMemcpy(buf.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+// Overwrite an allocated buffer in place (device pointers captured in the
+// solve graphs stay valid).
+template <typename T>
+cudaError_t refill(DevBuf<T> &buf, const std::vector<T> &h)
+{
+    if (h.size() != buf.count) return cudaErrorInvalidValue;
     if (h.empty()) return cudaSuccess;
     return cudaMemcpy(buf.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
@@ -297,8 +314,8 @@ void launch_residual_diag(msc_plan *p, const int *gate, const double2 *x, double
                           cudaStream_t st)
 {
     msc::k_residual_diag<<<p->ntiles, 256, smem_residual(p->n), st>>>(
-        p->tiles(), gate, p->n, p->Tm.p, p->v00.p, p->row_pkd.p, p->row_c.p, p->sys_spec_row.p,
-        p->sys_bspec.p, x, out, with_b);
+        p->tiles(), gate, p->n, p->Tm.p, p->v00.p, p->row_pkd.p, p->row_c.p, p->row_rhs.p, x, out,
+        with_b);
 }
 
 constexpr int kHaloBX = 8;
@@ -463,12 +480,19 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
         if (tm) mark(p, 1, j, 1, st);
         const msc::ArnoldiArgs aa = arnoldi_args(p, p->active.p);
         const unsigned nblk = (unsigned)(p->ntiles * p->split);
-        if (tm) mark(p, 2, j, 0, st);
-        msc::k_arnoldi_p1<R><<<nblk, 256, 0, st>>>(aa, Q, j + 1, W, p->h1.p, p->m + 2);
-        if (tm) mark(p, 2, j, 1, st);
+        // Two Gram-Schmidt passes; the mixed form may opt into one pass with
+        // the Pythagorean norm (the FP64 true residual of the next refinement
+        // step absorbs the loss of orthogonality, at the price of iterations).
+        const int cgs2 = p->cgs1_inner ? 0 : 1;
+        if (cgs2) {
+            if (tm) mark(p, 2, j, 0, st);
+            msc::k_arnoldi_p1<R><<<nblk, 256, 0, st>>>(aa, Q, j + 1, W, p->h1.p, p->m + 2);
+            if (tm) mark(p, 2, j, 1, st);
+        }
         if (tm) mark(p, 3, j, 0, st);
         msc::k_arnoldi_p2<R><<<nblk, 256, 0, st>>>(aa, Q, j + 1, W, p->state(), p->m, j,
-                                                   p->desc.rtol, p->desc.max_iterations, inner);
+                                                   p->desc.rtol, p->desc.max_iterations, inner,
+                                                   cgs2);
         if (tm) mark(p, 3, j, 1, st);
         if (tm) mark(p, 4, j, 0, st);
         launch_update_t<R>(p, p->active.p, Q, j + 1, nullptr, p->h2.p, p->m + 2, W, p->scale.p, Qn,
@@ -957,12 +981,17 @@ msc_status finalize(msc_plan *p)
     }
     std::vector<double> bn(p->B);
     for (int s = 0; s < p->B; ++s) bn[s] = std::sqrt(msc::cabs2(bspec[s]));
+    // right-hand side: the scattering source b_spec at z_n of each specular row
+    p->rhs_default_h.assign(p->R, double2{0.0, 0.0});
+    for (int s = 0; s < p->B; ++s) p->rhs_default_h[spec_row[s]] = bspec[s];
+    p->row_c_h = rc;
 
     MSC_CUDA(upload(p->row_pkd, pkd));
     MSC_CUDA(upload(p->row_fn, fn));
     MSC_CUDA(upload(p->row_c, rc));
     MSC_CUDA(upload(p->row_b, rb));
-    MSC_CUDA(upload(p->sys_bspec, bspec));
+    MSC_CUDA(upload(p->row_rhs, p->rhs_default_h));
+    MSC_CUDA(upload(p->sys_row0, p->sys_row0_h));
     MSC_CUDA(upload(p->sys_aspec, aspec));
     MSC_CUDA(upload(p->sys_spec_row, spec_row));
     MSC_CUDA(upload(p->nbr, nbr));
@@ -1166,6 +1195,7 @@ msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc)
     if (p->mixed) {
         if (desc->inner_restart > 0) p->m = desc->inner_restart;
         p->inner_rtol = desc->inner_rtol > 0.0 ? desc->inner_rtol : 1e-5;
+        p->cgs1_inner = (desc->flags & 4) != 0;
         p->max_cycles = desc->max_refinements > 0 ? desc->max_refinements : 30;
     }
     p->sys.resize(p->B);
@@ -1217,19 +1247,30 @@ msc_status msc_plan_set_potential(msc_plan *p, const double *potential_values, c
     std::vector<double> ET((size_t)n * n);
     for (int z = 0; z < n; ++z)
         for (int k = 0; k < n; ++k) ET[(size_t)k * n + z] = p->E_host[(size_t)z * n + k];
-    // coupling taps: every nonzero V_G with G != 0
+    // coupling taps: every offset d != 0 with V_d or V_{-d} nonzero (the set is
+    // closed under d -> -d so that A^H, whose tap at d is conj(V_{-d}), runs on
+    // the same offsets and tables)
     p->taps.clear();
     p->Vt_host.clear();
+    p->Vt_adj_host.clear();
+    auto nonzero = [&](int dx, int dy) {
+        const double2 *v = V + ((size_t)dx * nky + dy) * n;
+        for (int k = 0; k < n; ++k)
+            if (v[k].x != 0.0 || v[k].y != 0.0) return true;
+        return false;
+    };
     for (int dx = 0; dx < nkx; ++dx)
         for (int dy = 0; dy < nky; ++dy) {
             if (dx == 0 && dy == 0) continue;
+            const int mx = (nkx - dx) % nkx, my = (nky - dy) % nky;
+            if (!nonzero(dx, dy) && !nonzero(mx, my)) continue;
             const double2 *v = V + ((size_t)dx * nky + dy) * n;
-            bool nz = false;
-            for (int k = 0; k < n && !nz; ++k) nz = (v[k].x != 0.0 || v[k].y != 0.0);
-            if (!nz) continue;
+            const double2 *vm = V + ((size_t)mx * nky + my) * n;
             p->taps.emplace_back(dx, dy);
             p->Vt_host.insert(p->Vt_host.end(), v, v + n);
+            for (int k = 0; k < n; ++k) p->Vt_adj_host.push_back(msc::cconj(vm[k]));
         }
+    p->adjoint = false;
     p->K = (int)p->taps.size();
     if (p->K > msc::kMaxTaps) return fail(MSC_ERR_DIMS, "too many nonzero coupling taps");
     for (const double2 &v : p->Vt_host)
@@ -1513,6 +1554,119 @@ msc_status msc_debug_apply_block_inverse_f32(msc_plan *p, const float *x, float 
 
 int msc_plan_uses_tensor_cores(const msc_plan *p) { return (p && p->use_tc) ? p->tc_n : 0; }
 
+// ---------------------------------------------------------------------------
+// Adjoint solves and the potential gradient (no counterpart in the reference;
+// the operator they transpose is the one of multiscat_gmres.f90:452-687).
+// ---------------------------------------------------------------------------
+msc_status msc_plan_set_adjoint(msc_plan *p, int32_t adjoint)
+{
+    if (!p) return fail(MSC_ERR_ARG, "null plan");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    const bool want = adjoint != 0;
+    if (want == p->adjoint) return MSC_OK;
+    // nothing of this plan may be in flight while its operator data changes
+    MSC_CUDA(cudaDeviceSynchronize());
+    const std::vector<double2> &vt = want ? p->Vt_adj_host : p->Vt_host;
+    std::vector<double2> rc = p->row_c_h;
+    if (want)
+        for (double2 &c : rc) c = msc::cconj(c);
+    if (p->K > 0) MSC_CUDA(refill(p->Vt, vt));
+    MSC_CUDA(refill(p->row_c, rc));
+    if (p->mixed) {
+        if (p->K > 0) {
+            std::vector<float2> vt32(vt.size());
+            for (size_t i = 0; i < vt.size(); ++i) vt32[i] = make_float2((float)vt[i].x, (float)vt[i].y);
+            MSC_CUDA(refill(p->Vt32, vt32));
+        }
+        std::vector<float2> c32(rc.size());
+        for (size_t i = 0; i < rc.size(); ++i) c32[i] = make_float2((float)rc[i].x, (float)rc[i].y);
+        MSC_CUDA(refill(p->row_c32, c32));
+    }
+    p->adjoint = want;
+    return MSC_OK;
+}
+
+int msc_plan_is_adjoint(const msc_plan *p) { return (p && p->adjoint) ? 1 : 0; }
+
+msc_status msc_plan_set_boundary_rhs(msc_plan *p, const double *rhs, int32_t on_device, void *stream)
+{
+    if (!p) return fail(MSC_ERR_ARG, "null plan");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    cudaStream_t us = reinterpret_cast<cudaStream_t>(stream);
+    const size_t bytes = (size_t)p->R * sizeof(double2);
+    if (!rhs)
+        MSC_CUDA(cudaMemcpyAsync(p->row_rhs.p, p->rhs_default_h.data(), bytes, cudaMemcpyHostToDevice, us));
+    else
+        MSC_CUDA(cudaMemcpyAsync(p->row_rhs.p, rhs, bytes,
+                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, us));
+    msc::k_system_norms<<<p->B, 256, 0, us>>>(p->sys_row0.p, p->row_rhs.p, p->bnorm.p);
+    MSC_CUDA(cudaGetLastError());
+    if (!on_device || !rhs) MSC_CUDA(cudaStreamSynchronize(us));
+    return MSC_OK;
+}
+
+msc_status msc_plan_set_adjoint_rhs(msc_plan *p, const double *psi, const double *dl_dintensity,
+                                    const double *dl_damplitude, void *stream)
+{
+    if (!p) return fail(MSC_ERR_ARG, "null plan");
+    if (dl_dintensity && !psi) return fail(MSC_ERR_ARG, "dl_dintensity needs psi");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    cudaStream_t us = reinterpret_cast<cudaStream_t>(stream);
+    msc::k_adjoint_rhs<<<(p->R + 255) / 256, 256, 0, us>>>(
+        p->R, p->n, p->row_sys.p, p->sys_spec_row.p, p->sys_aspec.p, p->row_b.p,
+        reinterpret_cast<const double2 *>(psi), dl_dintensity,
+        reinterpret_cast<const double2 *>(dl_damplitude), p->row_rhs.p);
+    MSC_CUDA(cudaGetLastError());
+    msc::k_system_norms<<<p->B, 256, 0, us>>>(p->sys_row0.p, p->row_rhs.p, p->bnorm.p);
+    MSC_CUDA(cudaGetLastError());
+    return MSC_OK;
+}
+
+msc_status msc_potential_gradient(msc_plan *p, const double *psi, const double *lambda,
+                                  int32_t half_x, int32_t half_y, double *grad, void *stream)
+{
+    if (!p || !psi || !lambda || !grad) return fail(MSC_ERR_ARG, "null argument");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    const int nkx = p->nkx, nky = p->nky, n = p->n, ntor = nkx * nky;
+    if (!p->pos_map.p) {
+        std::vector<int> pos(p->R), map((size_t)p->B * ntor, -1);
+        for (int s = 0; s < p->B; ++s) {
+            const SystemHost &sh = p->sys[s];
+            const int r0 = p->sys_row0_h[s];
+            for (int j = 0; j < sh.C; ++j) {
+                const int q = sh.ix[j] * nky + sh.iy[j];
+                pos[r0 + j] = q;
+                map[(size_t)s * ntor + q] = r0 + j;
+            }
+        }
+        MSC_CUDA(upload(p->row_pos, pos));
+        MSC_CUDA(upload(p->pos_map, map));
+    }
+    int wx = nkx, hx = 0, wy = nky, hy = 0;
+    if (half_x >= 0 && 2 * half_x + 1 < nkx) {
+        wx = 2 * half_x + 1;
+        hx = half_x;
+    }
+    if (half_y >= 0 && 2 * half_y + 1 < nky) {
+        wy = 2 * half_y + 1;
+        hy = half_y;
+    }
+    cudaStream_t us = reinterpret_cast<cudaStream_t>(stream);
+    MSC_CUDA(cudaMemsetAsync(grad, 0, (size_t)ntor * n * sizeof(double2), us));
+    const int per_block = 8 * msc::kGradPerWarp;
+    dim3 grid((wx * wy + per_block - 1) / per_block, (n + 31) / 32);
+    msc::k_potential_gradient<<<grid, 256, 0, us>>>(
+        nkx, nky, n, p->B, p->sys_row0.p, p->row_pos.p, p->pos_map.p, wx, wy, hx, hy,
+        reinterpret_cast<const double2 *>(psi), reinterpret_cast<const double2 *>(lambda),
+        reinterpret_cast<double2 *>(grad));
+    MSC_CUDA(cudaGetLastError());
+    return MSC_OK;
+}
+
 msc_status msc_intensities(msc_plan *p, int32_t s, const double *psi, double *intensities, void *stream)
 {
     if (!p || !psi || !intensities) return fail(MSC_ERR_ARG, "null argument");
@@ -1653,13 +1807,11 @@ k_noalloc_scan_taps(int nkx, int nky, int n, const double2 *__restrict__ V, int 
     if (threadIdx.x == 0) *count = base;
 }
 
-// Tap values, neighbour table, row tiles and the (unused) right-hand-side
-// slots for one full-grid system.
+// Tap values, neighbour table and row tiles for one full-grid system.
 __global__ void k_noalloc_tables(int nkx, int nky, int n, int K, const double2 *__restrict__ V,
                                  const int2 *__restrict__ taps, double2 *__restrict__ Vt,
                                  int *__restrict__ nbr, int *__restrict__ tile_row0,
-                                 int *__restrict__ tile_nrow, int *__restrict__ tile_sys, int ntiles,
-                                 int *__restrict__ spec_row, double2 *__restrict__ bspec)
+                                 int *__restrict__ tile_nrow, int *__restrict__ tile_sys, int ntiles)
 {
     const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -1679,10 +1831,6 @@ __global__ void k_noalloc_tables(int nkx, int nky, int n, int K, const double2 *
         tile_row0[i] = (int)i * msc::kTileRows;
         tile_nrow[i] = min(msc::kTileRows, C - (int)i * msc::kTileRows);
         tile_sys[i] = 0;
-    }
-    if (tid == 0) {
-        spec_row[0] = 0;
-        bspec[0] = make_double2(0.0, 0.0);
     }
 }
 
@@ -1736,8 +1884,6 @@ extern "C" msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32
     const size_t o_t0 = off;     off += round256(sizeof(int) * (size_t)ntiles);
     const size_t o_tn = off;     off += round256(sizeof(int) * (size_t)ntiles);
     const size_t o_ts = off;     off += round256(sizeof(int) * (size_t)ntiles);
-    const size_t o_spec = off;   off += round256(sizeof(int));
-    const size_t o_bspec = off;  off += round256(sizeof(double2));
     const size_t o_tmp = off;    off += round256(sizeof(double2) * (size_t)C * n);
     if (off > kNoAllocScratchBytes)
         return fail(MSC_ERR_DIMS, "problem needs " + std::to_string(off) +
@@ -1755,8 +1901,6 @@ extern "C" msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32
     int *t0 = reinterpret_cast<int *>(base + o_t0);
     int *tn = reinterpret_cast<int *>(base + o_tn);
     int *ts = reinterpret_cast<int *>(base + o_ts);
-    int *spec = reinterpret_cast<int *>(base + o_spec);
-    double2 *bspec = reinterpret_cast<double2 *>(base + o_bspec);
     double2 *tmp = reinterpret_cast<double2 *>(base + o_tmp);
     const double2 *V = reinterpret_cast<const double2 *>(potential_values);
 
@@ -1766,12 +1910,11 @@ extern "C" msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32
     MSC_CUDA(cudaMemcpyAsync(&K, count, sizeof(int), cudaMemcpyDeviceToHost, s));
     MSC_CUDA(cudaStreamSynchronize(s));
     if (K < 0 || K > kmax) return fail(MSC_ERR_CUDA, "tap scan returned an invalid count");
-    k_noalloc_tables<<<256, 256, 0, s>>>(nkx, nky, n, K, V, taps, Vt, nbr, t0, tn, ts, ntiles, spec,
-                                         bspec);
+    k_noalloc_tables<<<256, 256, 0, s>>>(nkx, nky, n, K, V, taps, Vt, nbr, t0, tn, ts, ntiles);
     MSC_CUDA(cudaGetLastError());
     const msc::Tiles tiles{t0, tn, ts, ntiles};
     msc::k_residual_diag<<<ntiles, 256, smem_residual(n), s>>>(
-        tiles, nullptr, n, kinetic, v00, pkd, reinterpret_cast<const double2 *>(wave_c), spec, bspec,
+        tiles, nullptr, n, kinetic, v00, pkd, reinterpret_cast<const double2 *>(wave_c), nullptr,
         reinterpret_cast<const double2 *>(x), tmp, 0);
     MSC_CUDA(cudaGetLastError());
     dim3 grid(ntiles, (n + 31) / 32);

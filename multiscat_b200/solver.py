@@ -97,7 +97,8 @@ class ScatteringPlan:
     def __init__(self, potential_values, kinetic, systems: list[SystemSpec], *,
                  rtol: float = 1e-10, restart: int = 30, max_iterations: int = 2000,
                  precision: str = "fp64", inner_rtol: float = 0.0, inner_restart: int = 0,
-                 max_refinements: int = 0, tensor_cores: bool | None = None):
+                 max_refinements: int = 0, tensor_cores: bool | None = None,
+                 inner_gram_schmidt_passes: int = 2):
         self._lib = nat.load()
         v = np.ascontiguousarray(np.asarray(potential_values), dtype=np.complex128)
         nkx, nky, nz = v.shape
@@ -118,6 +119,11 @@ class ScatteringPlan:
         desc.max_refinements = max_refinements
         # tensor_cores: None = autotuned, True = always tcgen05, False = never
         desc.flags = {None: 0, True: 2, False: 1}[tensor_cores]
+        # mixed form: Gram-Schmidt passes of the FP32 inner Arnoldi step (1 or 2)
+        if inner_gram_schmidt_passes not in (1, 2):
+            raise ValueError("inner_gram_schmidt_passes must be 1 or 2")
+        if inner_gram_schmidt_passes == 1:
+            desc.flags |= 4
         self._plan = ctypes.c_void_p()
         nat.check("msc_plan_create", self._lib.msc_plan_create(ctypes.byref(self._plan),
                                                               ctypes.byref(desc)))
@@ -168,6 +174,68 @@ class ScatteringPlan:
             cycles=np.array([r.refinements for r in res]),
             status=np.array([r.status for r in res]),
             residual=np.array([r.residual for r in res]))
+
+    # ---- adjoint differentiation -------------------------------------------------
+    def set_adjoint(self, on: bool) -> None:
+        """Solve with A^H (True) or A (False); eigenbasis, tuning and graphs are kept."""
+        nat.check("msc_plan_set_adjoint", self._lib.msc_plan_set_adjoint(self._plan, 1 if on else 0))
+
+    @property
+    def adjoint(self) -> bool:
+        return bool(self._lib.msc_plan_is_adjoint(self._plan))
+
+    def set_boundary_rhs(self, rhs: torch.Tensor | None) -> None:
+        """Outer-boundary right-hand side per row (complex128 [total_rows], cuda),
+        or None for the scattering source b_spec at each specular row."""
+        stream = torch.cuda.current_stream().cuda_stream
+        if rhs is None:
+            st = self._lib.msc_plan_set_boundary_rhs(self._plan, None, 0, ctypes.c_void_p(stream))
+        else:
+            rhs = _device_rows(rhs, torch.complex128, self.total_rows)
+            st = self._lib.msc_plan_set_boundary_rhs(self._plan, ctypes.c_void_p(rhs.data_ptr()), 1,
+                                                     ctypes.c_void_p(stream))
+            self._rhs_keepalive = rhs
+        nat.check("msc_plan_set_boundary_rhs", st)
+
+    def solve_adjoint(self, psi: torch.Tensor, dl_dintensity: torch.Tensor | None = None,
+                      dl_damplitude: torch.Tensor | None = None, *,
+                      raise_on_error: bool = True) -> SolveResult:
+        """lambda with A^H lambda = u, u_G(z_n) = -i gamma_G conj(b_G),
+        gamma = 2 dL/dI_G S_G + dL/dS_G (S from psi).  lambda is in ``.psi``.
+        The plan returns to the forward operator and source afterwards."""
+        stream = torch.cuda.current_stream().cuda_stream
+        psi = psi.contiguous()
+        di = None if dl_dintensity is None else _device_rows(dl_dintensity, torch.float64,
+                                                             self.total_rows)
+        ds = None if dl_damplitude is None else _device_rows(dl_damplitude, torch.complex128,
+                                                             self.total_rows)
+        self.set_adjoint(True)
+        try:
+            nat.check("msc_plan_set_adjoint_rhs", self._lib.msc_plan_set_adjoint_rhs(
+                self._plan, ctypes.c_void_p(psi.data_ptr()),
+                None if di is None else ctypes.c_void_p(di.data_ptr()),
+                None if ds is None else ctypes.c_void_p(ds.data_ptr()), ctypes.c_void_p(stream)))
+            res = self.solve(raise_on_error=raise_on_error)
+        finally:
+            self.set_adjoint(False)
+            self.set_boundary_rhs(None)
+        res.intensities = None
+        return res
+
+    def potential_gradient(self, psi: torch.Tensor, lam: torch.Tensor,
+                           window: tuple[int, int] | None = None) -> torch.Tensor:
+        """dL/dV (complex128 [nkx, nky, nz], dL/dRe + i dL/dIm) from the forward
+        solution psi and the adjoint solution lam; window = (half_x, half_y)
+        restricts the offsets computed (others are 0)."""
+        psi = psi.contiguous()
+        lam = lam.contiguous()
+        grad = torch.empty((self.nkx, self.nky, self.nz), dtype=torch.complex128, device=psi.device)
+        hx, hy = (-1, -1) if window is None else window
+        stream = torch.cuda.current_stream().cuda_stream
+        nat.check("msc_potential_gradient", self._lib.msc_potential_gradient(
+            self._plan, ctypes.c_void_p(psi.data_ptr()), ctypes.c_void_p(lam.data_ptr()), hx, hy,
+            ctypes.c_void_p(grad.data_ptr()), ctypes.c_void_p(stream)))
+        return grad
 
     def info(self) -> "nat.PlanInfo":
         inf = nat.PlanInfo()
@@ -226,6 +294,14 @@ class ScatteringPlan:
     def tensor_core_tile(self) -> int:
         """Tile width N of the tcgen05 block inverse (0 when it is not used)."""
         return int(self._lib.msc_plan_uses_tensor_cores(self._plan))
+
+
+def _device_rows(t, dtype, rows: int) -> torch.Tensor:
+    t = torch.as_tensor(t).to(device=torch.device("cuda", torch.cuda.current_device()),
+                              dtype=dtype).contiguous()
+    if t.numel() != rows:
+        raise ValueError(f"expected {rows} rows, got {t.numel()}")
+    return t
 
 
 def full_grid_system(pkd, wave_a, wave_b, wave_c) -> SystemSpec:

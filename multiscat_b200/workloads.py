@@ -15,6 +15,9 @@ All in natural units (1/Angstrom^2, Angstrom), He-4 (4.0026 u) unless stated:
   phi ~ U(0, 45) deg; each beam keeps the channels with
   pkd <= (2m/hbar^2) * 200 meV (the ``n_channels``-style truncation by pkd)
   out of a 32 x 32 coupling torus, giving uneven channel counts.
+- ``cfg3_problem``: cfg1's system with the loss L = sum_open w_G |S_G|^2,
+  w_G ~ U(0, 1) (seeded) on the open channels, and the potential as a
+  differentiable function of (D, alpha, h) for adjoint gradients.
 - ``cfg4_batch``: square a = 2.54 A, h = 0.25 A, modes |m|,|n| <= 8 from a
   128 x 128 cell grid; 81 x 81 channels; 300 nodes on [-2, 14] A;
   E = 100 meV, theta = 45 deg, 16 azimuths phi = 3k deg.
@@ -95,6 +98,50 @@ def cfg1_case(nz: int = 200, nk: int = 41) -> Case:
     pkd, wa, wb, wc = _beam(factor, 64.0, math.radians(30.0), 0.0, a1, a2, nk, nk, w, z0, z1 - z0)
     return Case(f"cfg1: hexagonal {nk}x{nk}x{nz}", v, sa.kinetic_matrix(nodes, w), pkd, wa, wb,
                 wc, nodes, w)
+
+
+@dataclass
+class AdjointProblem:
+    """Loss L = sum_G w_G |S_G|^2 over one system and its potential builder."""
+    case: Case
+    weights: np.ndarray          # [C] (0 on closed channels)
+    a1: np.ndarray
+    a2: np.ndarray
+    h: float
+    k_max: int
+    n_cell: int
+    factor: float
+    params: dict = field(default_factory=dict)
+
+    def potential(self, depth=D_MORSE, alpha=ALPHA_MORSE, h=None, device=None) -> torch.Tensor:
+        """V (complex128 [nk, nk, nz], 1/A^2) as a torch function of (D meV, alpha 1/A, h A)."""
+        h = self.h if h is None else h
+        nk = self.case.pkd.shape[0]
+        v = sa.corrugated_morse_fourier(self.case.nodes, self.a1, self.a2,
+                                        sa.hexagonal_xi(self.a1, self.a2, h), depth, alpha,
+                                        self.n_cell, self.k_max, nk, nk, device=device)
+        return v * self.factor
+
+
+def cfg3_problem(nz: int = 200, nk: int = 41, seed: int = 0) -> AdjointProblem:
+    """cfg1's hexagonal system; w_G ~ U(0, 1) from default_rng(seed) on the
+    open channels (pkd < 0) in the row-major channel order, 0 elsewhere."""
+    factor = sa.natural_units_factor(sa.HE4_MASS)
+    z0, z1 = -1.5, 12.0
+    nodes, w = sa.lobatto_rule(z0, z1, nz)
+    a = 3.16
+    a1, a2 = np.array([a, 0.0]), np.array([0.5 * a, 0.5 * math.sqrt(3.0) * a])
+    h = 0.2
+    v = (sa.corrugated_morse_fourier(nodes, a1, a2, sa.hexagonal_xi(a1, a2, h), D_MORSE,
+                                     ALPHA_MORSE, 64, 4, nk, nk) * factor).numpy()
+    pkd, wa, wb, wc = _beam(factor, 64.0, math.radians(30.0), 0.0, a1, a2, nk, nk, w, z0, z1 - z0)
+    case = Case(f"cfg3: hexagonal {nk}x{nk}x{nz}, weighted-intensity loss", v,
+                sa.kinetic_matrix(nodes, w), pkd, wa, wb, wc, nodes, w)
+    rng = np.random.default_rng(seed)
+    draws = rng.uniform(0.0, 1.0, pkd.size)
+    weights = np.where(pkd.ravel() < 0.0, draws, 0.0)
+    return AdjointProblem(case, weights, a1, a2, h, 4, 64, factor,
+                          {"depth": D_MORSE, "alpha": ALPHA_MORSE, "h": h})
 
 
 def cfg2_batch(n_solves: int = 512, seed: int = 0, nz: int = 150, torus: int = 32,

@@ -15,6 +15,11 @@ Writes
   ``n_channels`` truncation) of two seeded beams over the same potential.
 - ``oracle_cfg1.json`` (with --cfg1, minutes of CPU): oracle intensities of
   the 41x41-channel hexagonal case at precision 1e-10.
+- ``oracle_cfg3_fd.json`` (with --cfg3, minutes of CPU on all cores): central
+  finite differences, through the oracle, of L = sum_open w_G |S_G|^2 on the
+  cfg1 system (w_G ~ U(0,1), seed 0) with respect to D, alpha, h (relative
+  step 1e-5, potential from the oracle's own numpy builder) and to Re/Im of a
+  few single Fourier components V_G(z_k) (step 1e-3 max(|V_G(z_k)|, 1)).
 
 The GPU box has no reference tree; the tests read only these files.
 """
@@ -91,9 +96,114 @@ def oracle_subsets() -> None:
     (HERE / "oracle_subsets.json").write_text(json.dumps(res))
 
 
+# ---------------------------------------------------------------------------
+# cfg3: finite differences of the weighted-intensity loss through the oracle
+# ---------------------------------------------------------------------------
+CFG3_COMPONENTS = [  # (ix, iy, z index, "re" | "im"); z nodes 40-55 lie at -0.2..0.9 A
+    (1, 0, 45, "re"), (1, 0, 45, "im"), (40, 1, 40, "re"), (2, 39, 40, "im"),
+    (0, 0, 55, "re"),
+]
+
+
+def _component_step(v, ix, iy, k) -> float:
+    """1e-3 of max(|V_G(z_k)|, 1/A^2): one node's component moves L by only
+    ~1e-4 per unit, so a 1e-5 step would leave the loss difference near the
+    solver's own error; the central-difference truncation error at 1e-3 is
+    ~1e-7 relative."""
+    return 1e-3 * max(abs(v[ix, iy, k]), 1.0)
+CFG3_EPS = 0.5e-13
+
+
+def _cfg3_setup():
+    from multiscat_b200.workloads import cfg3_problem
+    pr = cfg3_problem()
+    c = pr.case
+    hex_xi = _hex_xi_numpy(pr.a1, pr.a2)
+    return pr, c, hex_xi
+
+
+def _hex_xi_numpy(a1, a2):
+    b1, b2 = inputs.reciprocal_vectors(np.asarray(a1), np.asarray(a2))
+    b3 = b1 + b2
+
+    def make(h):
+        def fn(x, y):
+            return (h / 3.0) * (np.cos(b1[0] * x + b1[1] * y) + np.cos(b2[0] * x + b2[1] * y) +
+                                np.cos(b3[0] * x + b3[1] * y))
+        return fn
+    return make
+
+
+def _cfg3_potential(pr, hex_xi, depth, alpha, h):
+    nk = pr.case.pkd.shape[0]
+    v = inputs.corrugated_morse_fourier(pr.case.nodes, pr.a1, pr.a2, hex_xi(h), depth, alpha,
+                                        pr.n_cell, pr.k_max, nk, nk)
+    return v * pr.factor
+
+
+def _cfg3_loss(v):
+    pr, c, _ = _cfg3_setup()
+    sx, sy = solver.full_grid_channels(*v.shape[:2])
+    psi, info, iters, _ = solver.solve_channels(
+        v, sx, sy, c.pkd.ravel(), c.wc.ravel(), 0, c.wb.ravel()[0], c.t, eps=CFG3_EPS)
+    inten = inputs.intensities(psi, c.wa.ravel(), c.wb.ravel())
+    return float(np.dot(pr.weights, inten)), int(info), int(iters)
+
+
+def _cfg3_job(job):
+    sys.path.insert(0, str(ROOT))
+    pr, c, hex_xi = _cfg3_setup()
+    kind, key, sign = job
+    p = dict(pr.params)
+    if kind == "param":
+        p[key] = p[key] * (1.0 + sign * 1e-5)
+        v = _cfg3_potential(pr, hex_xi, p["depth"], p["alpha"], p["h"])
+    elif kind == "base":
+        v = _cfg3_potential(pr, hex_xi, p["depth"], p["alpha"], p["h"])
+    else:
+        v = _cfg3_potential(pr, hex_xi, p["depth"], p["alpha"], p["h"])
+        ix, iy, k, part = key
+        step = _component_step(v, ix, iy, k)
+        v[ix, iy, k] += sign * step * (1.0 if part == "re" else 1.0j)
+    return job, _cfg3_loss(v)
+
+
+def oracle_cfg3_fd() -> None:
+    import multiprocessing as mp
+    t0 = time.time()
+    pr, c, hex_xi = _cfg3_setup()
+    v0 = _cfg3_potential(pr, hex_xi, pr.params["depth"], pr.params["alpha"], pr.params["h"])
+    jobs = [("base", None, 0)]
+    for k in ("depth", "alpha", "h"):
+        jobs += [("param", k, +1), ("param", k, -1)]
+    for comp in CFG3_COMPONENTS:
+        jobs += [("comp", comp, +1), ("comp", comp, -1)]
+    with mp.get_context("spawn").Pool(min(len(jobs), 8)) as pool:
+        res = dict(((j[0], j[1], j[2]), r) for j, r in pool.map(_cfg3_job, jobs))
+    out = {"case": c.name, "oracle_eps": CFG3_EPS, "relative_step": 1e-5,
+           "loss": res[("base", None, 0)][0], "params": {}, "components": [],
+           "max_iterations": max(r[2] for r in res.values()),
+           "all_converged": all(r[1] == 0 for r in res.values())}
+    for k in ("depth", "alpha", "h"):
+        step = 1e-5 * pr.params[k]
+        out["params"][k] = {"value": pr.params[k], "step": step,
+                            "dL": (res[("param", k, 1)][0] - res[("param", k, -1)][0]) / (2 * step)}
+    for comp in CFG3_COMPONENTS:
+        ix, iy, k, part = comp
+        step = _component_step(v0, ix, iy, k)
+        out["components"].append({"ix": ix, "iy": iy, "z": k, "part": part, "step": step,
+                                  "dL": (res[("comp", comp, 1)][0] - res[("comp", comp, -1)][0]) /
+                                        (2 * step)})
+    out["seconds"] = time.time() - t0
+    (HERE / "oracle_cfg3_fd.json").write_text(json.dumps(out, indent=1))
+    print("cfg3 fd", json.dumps(out))
+
+
 if __name__ == "__main__":
     wolken_files()
     oracle_case(cfg0_case(), 12, "oracle_cfg0.json")
     oracle_subsets()
     if "--cfg1" in sys.argv:
         oracle_case(cfg1_case(), 10, "oracle_cfg1.json")
+    if "--cfg3" in sys.argv:
+        oracle_cfg3_fd()

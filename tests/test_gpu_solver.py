@@ -230,13 +230,15 @@ def test_mixed_cfg0_matches_oracle(cfg0):
     plan.close()
 
 
-def test_mixed_cfg1_matches_oracle():
+@pytest.mark.parametrize("passes", [1, 2])
+def test_mixed_cfg1_matches_oracle(passes):
     path = GOLDEN / "oracle_cfg1.json"
     if not path.exists():
         pytest.skip("oracle_cfg1.json not generated")
     golden = json.loads(path.read_text())
     case = cfg1_case()
-    plan = ScatteringPlan(case.v, case.t, [case.system()], rtol=1e-10, precision="mixed")
+    plan = ScatteringPlan(case.v, case.t, [case.system()], rtol=1e-10, precision="mixed",
+                          inner_gram_schmidt_passes=passes)
     res = plan.solve()
     inten = res.intensities.cpu().numpy()
     assert res.status[0] == 0
@@ -245,14 +247,16 @@ def test_mixed_cfg1_matches_oracle():
     plan.close()
 
 
-def test_mixed_batched_subsets_match_oracle_and_fp64():
+@pytest.mark.parametrize("passes", [1, 2])
+def test_mixed_batched_subsets_match_oracle_and_fp64(passes):
     golden = json.loads((GOLDEN / "oracle_subsets.json").read_text())
     systems = []
     case = None
     for rec in golden:
         case, sys_list = cfg2_batch(n_solves=2, seed=rec["seed"])
         systems.append(sys_list[0])
-    mixed = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed")
+    mixed = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed",
+                           inner_gram_schmidt_passes=passes)
     fp64 = ScatteringPlan(case.v, case.t, systems, rtol=1e-10)
     rm = mixed.solve()
     rf = fp64.solve()
@@ -303,3 +307,26 @@ def test_tensor_core_block_inverse_matches_fp64(which):
         fp64.close()
     mixed.close()
     simt.close()
+
+
+# ---------------------------------------------------------------------------
+# cfg4 shape: 81 x 81 channels, 300 nodes, |m|,|n| <= 8 (288 taps, halo 8),
+# several azimuths batched.  No oracle here (the CPU restatement would need
+# tens of GB); the check is mixed vs the plain FP64 form, plus flux.
+# ---------------------------------------------------------------------------
+def test_cfg4_batch_mixed_matches_fp64():
+    from multiscat_b200.workloads import cfg4_batch
+    case, systems = cfg4_batch(n_azimuths=4)
+    fp64 = ScatteringPlan(case.v, case.t, systems, rtol=1e-10)
+    r64 = fp64.solve()
+    assert (r64.status == 0).all()
+    fp64.close()
+    mixed = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed")
+    rm = mixed.solve()
+    assert (rm.status == 0).all()
+    d = (rm.intensities - r64.intensities).abs().max().item()
+    assert d <= MIXED_TOL, d
+    for s in range(len(systems)):
+        inten = r64.system_intensities(s).cpu().numpy()
+        assert abs(inten.sum() - 1.0) <= 1e-8
+    mixed.close()

@@ -147,3 +147,19 @@ def test_golden_oracle_fixtures_are_converged():
     for rec in json.loads((GOLDEN / "oracle_subsets.json").read_text()):
         assert rec["info"] == 0
         assert abs(rec["flux"] - 1.0) < 1e-11
+
+
+def test_cfg3_fd_fixture_consistent_with_cfg1_fixture():
+    """The oracle FD fixture's base loss is sum_G w_G I_G of the cfg1 oracle
+    intensities (same system, independent runs at 1e-10 and 5e-14)."""
+    path = GOLDEN / "oracle_cfg3_fd.json"
+    if not path.exists():
+        pytest.skip("oracle_cfg3_fd.json not generated")
+    from multiscat_b200.workloads import cfg3_problem
+    fd = json.loads(path.read_text())
+    cfg1 = json.loads((GOLDEN / "oracle_cfg1.json").read_text())
+    w = cfg3_problem().weights
+    assert fd["all_converged"]
+    assert abs(float(np.dot(w, cfg1["intensities"])) - fd["loss"]) < 1e-8
+    for rec in list(fd["params"].values()) + fd["components"]:
+        assert math.isfinite(rec["dL"])
