@@ -337,6 +337,71 @@ def secondary_measurements(args, case, systems, plan, inten, value, torch, strea
                          "iterations": int(p.solve().iterations[0])}
             p.close()
         out["cfg1_single_solve"] = {"workload": c1.name, **res}
+    out["cfg3_adjoint"] = adjoint_measurement(torch, stream)
+    out["cfg4_batch"] = cfg4_measurement(args, torch, stream)
+    return out
+
+
+def adjoint_measurement(torch, stream) -> dict:
+    """cfg3: forward + adjoint backward of L = sum w |S|^2 w.r.t. (D, alpha, h)
+    through the torch potential builder; gradient error vs the oracle's
+    central finite differences (tests/golden/oracle_cfg3_fd.json)."""
+    from multiscat_b200.adjoint import scattering_intensities
+    from multiscat_b200.workloads import cfg3_problem
+    pr = cfg3_problem()
+    ref_path = ROOT / "tests" / "golden" / "oracle_cfg3_fd.json"
+    ref = json.loads(ref_path.read_text()) if ref_path.exists() else None
+    w = torch.as_tensor(pr.weights, device="cuda")
+    out = {"workload": pr.case.name}
+    for prec, rtol in (("fp64", 1e-12), ("mixed", 1e-12)):
+        def step():
+            p = {k: torch.tensor(v, dtype=torch.float64, device="cuda", requires_grad=True)
+                 for k, v in pr.params.items()}
+            v = pr.potential(p["depth"], p["alpha"], p["h"], device="cuda")
+            loss = (w * scattering_intensities(v, pr.case.t, [pr.case.system()], rtol=rtol,
+                                               precision=prec)).sum()
+            loss.backward()
+            return {k: float(t.grad) for k, t in p.items()}
+        for _ in range(2):
+            g = step()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(3):
+            g = step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+        rec = {"forward_backward_ms": start.elapsed_time(stop) / 3, "grads": g}
+        if ref:
+            rec["max_rel_err_vs_oracle_fd"] = max(abs(g[k] / ref["params"][k]["dL"] - 1.0)
+                                                  for k in g)
+        out[prec] = rec
+    out["what"] = ("plan build + forward solve + A^H solve + gradient kernel + torch builder "
+                   "backward, per step; bar: 1e-5 relative vs finite differences")
+    return out
+
+
+def cfg4_measurement(args, torch, stream) -> dict:
+    """cfg4: 16 azimuths of the 81 x 81 x 300 square system (288 taps), batched,
+    mixed vs plain FP64; accuracy of the mixed form against FP64."""
+    from multiscat_b200 import ScatteringPlan
+    from multiscat_b200.workloads import cfg4_batch
+    case, systems = cfg4_batch()
+    out = {"workload": case.name, "systems": len(systems),
+           "rows": int(sum(s.pkd.size for s in systems))}
+    inten = {}
+    for prec in ("mixed", "fp64"):
+        p = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, restart=args.restart,
+                           precision=prec)
+        r = p.solve()
+        ms = timed_steps(p, 1, stream, torch)
+        inten[prec] = r.intensities
+        out[prec] = {"solves_per_s": len(systems) / (ms / 1e3), "ms": ms,
+                     "iterations_max": int(r.iterations.max()),
+                     "all_converged": bool((r.status == 0).all())}
+        p.close()
+    out["max_abs_dI_mixed_vs_fp64"] = float((inten["mixed"] - inten["fp64"]).abs().max())
+    out["mixed_over_fp64"] = out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]
     return out
 
 
