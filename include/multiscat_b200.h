@@ -62,7 +62,7 @@ typedef struct {
     double rtol;            /* stop when ||b - A psi|| <= rtol ||b|| (per system)*/
     int32_t precision;      /* msc_precision                                    */
     int32_t inner_restart;  /* mixed: inner FP32 restart length (0 = restart)   */
-    double inner_rtol;      /* mixed: inner relative tolerance (0 = 1e-4)       */
+    double inner_rtol;      /* mixed: inner relative tolerance (0 = 1e-5)       */
     int32_t max_refinements;/* mixed: outer FP64 refinement steps (0 = 30)      */
     int32_t flags;          /* bit 0: mixed form without the tcgen05 kernel;
                                bit 1: keep the tcgen05 kernel even when the
@@ -87,13 +87,22 @@ typedef struct {
 /* Create a plan on the current CUDA device.  Allocates all device memory
  * the solve needs; *plan is NULL on failure. */
 msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc);
+
+/* Destroy a plan (synchronises the device).  Its device memory goes back to
+ * a memory pool the library keeps per device, so that the next plan (a new
+ * batch of beams, a new potential) gets its buffers without cudaMalloc; up
+ * to 32 GiB of unused pool memory stays reserved. */
 msc_status msc_plan_destroy(msc_plan *plan);
+
+/* Return the current device's unused pool memory to the driver (for callers
+ * that share the GPU with another allocator, e.g. between phases). */
+msc_status msc_release_cached_memory(void);
 
 /* Set the potential (host arrays, C order):
  *   potential_values  complex [nkx][nky][n_z]  V_G(z_k) in 1/Angstrom^2
  *   kinetic           double  [n_z][n_z]       positive Lobatto kinetic T
  * Builds H0 = T + diag Re V_00, its eigen-decomposition (FP64) and the
- * coupling taps (all nonzero V_G with G != 0).
+ * coupling taps (every offset G != 0 with V_G or V_-G nonzero).
  * Replaces build_preconditioner, multiscat_gmres.f90:226-273. */
 msc_status msc_plan_set_potential(msc_plan *plan, const double *potential_values,
                                   const double *kinetic);

@@ -28,6 +28,7 @@ from .solver import (
     SystemSpec,
     channel_subset_system,
     full_grid_system,
+    release_cached_memory,
     run_multiscat_fortran,
 )
 
@@ -35,5 +36,5 @@ __all__ = [
     "OptimizationConfig", "ScatteringCondition", "ScatteringMetadata", "UnitSystem",
     "get_scattering_matrices", "get_scattering_matrix", "momentum_from_angles", "natural_arrays",
     "ScatteringPlan", "SolveResult", "SystemSpec", "channel_subset_system", "full_grid_system",
-    "run_multiscat_fortran",
+    "release_cached_memory", "run_multiscat_fortran",
 ]

@@ -1088,6 +1088,43 @@ k_potential_gradient(int nkx, int nky, int n, int nsys, const int *__restrict__ 
     }
 }
 
+// Plan set-up on the device, one thread per channel row:
+//   fn[row]  = sum_k E[n-1,k]^2 / (pkd_row + lam_k)   (Sherman-Morrison factor
+//              of the block inverse, multiscat_gmres.f90:226-273)
+//   nbr[row][t] = row of the same system at position G - d_t, or -1
+// pos_map [B][nkx*nky] gives the row of each torus position per system.
+__global__ void k_row_tables(int nrows, int n, int ntaps, int nkx, int nky,
+                             const int *__restrict__ row_pos, const int *__restrict__ row_sys,
+                             const int *__restrict__ pos_map, const int2 *__restrict__ taps,
+                             const double *__restrict__ row_pkd, const double *__restrict__ en,
+                             const double *__restrict__ lam, double *__restrict__ fn,
+                             float *__restrict__ fn32, int *__restrict__ nbr)
+{
+    const int ntor = nkx * nky;
+    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < nrows;
+         row += gridDim.x * blockDim.x) {
+        const double pkd = row_pkd[row];
+        double f = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double e = en[k];
+            f += e * e / (pkd + lam[k]);
+        }
+        fn[row] = f;
+        if (fn32) fn32[row] = (float)f;
+        if (!nbr) continue;
+        const int pos = row_pos[row];
+        const int ix = pos / nky, iy = pos - ix * nky;
+        const int *map = pos_map + (size_t)row_sys[row] * ntor;
+        for (int t = 0; t < ntaps; ++t) {
+            int sx = ix - taps[t].x;
+            sx += (sx < 0) ? nkx : 0;
+            int sy = iy - taps[t].y;
+            sy += (sy < 0) ? nky : 0;
+            nbr[(size_t)row * ntaps + t] = map[sx * nky + sy];
+        }
+    }
+}
+
 __global__ void k_scale(double2 *p, size_t count, double sc)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -53,20 +54,66 @@ msc_status fail(msc_status st, const std::string &msg)
         }                                                                               \
     } while (0)
 
+// Plan memory comes from a memory pool owned by the library, one per device.
+// A destroyed plan's buffers go back to the pool and later plans reuse them
+// without cudaMalloc / cudaFree (a multi-GB cudaFree synchronises the device
+// and unmaps, tens of ms); up to kPoolKeepBytes of unused memory stays
+// reserved until msc_release_cached_memory.
+constexpr int kPoolMaxDevices = 64;
+constexpr uint64_t kPoolKeepBytes = 32ull << 30;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pool[kPoolMaxDevices] = {};
+
+cudaError_t plan_pool(cudaMemPool_t *out)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kPoolMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool;
+        e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = kPoolKeepBytes;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+        g_pool[dev] = pool;
+    }
+    *out = g_pool[dev];
+    return cudaSuccess;
+}
+
 template <typename T>
 struct DevBuf {
     T *p = nullptr;
     size_t count = 0;
+    // Allocation and release are ordered on the legacy stream; alloc waits
+    // for the allocation, and the plan synchronises the device before it
+    // releases anything that work may still use.
     cudaError_t alloc(size_t c)
     {
         release();
         count = c;
         if (c == 0) return cudaSuccess;
-        return cudaMalloc(&p, c * sizeof(T));
+        cudaMemPool_t pool;
+        cudaError_t e = plan_pool(&pool);
+        if (e != cudaSuccess) return e;
+        e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&p), c * sizeof(T), pool, 0);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            count = 0;
+            return e;
+        }
+        return cudaStreamSynchronize(0);
     }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, 0);
         p = nullptr;
         count = 0;
     }
@@ -104,7 +151,7 @@ struct msc_plan {
     DevBuf<double> E, ET, Tm, lam, en, v00, row_pkd, row_fn;
     DevBuf<double2> Vt, row_c, row_b, row_rhs, sys_aspec;
     std::vector<double2> row_c_h, rhs_default_h;   // c per row; default right-hand side
-    DevBuf<int> row_pos, pos_map;                  // gradient tables (built on first use)
+    DevBuf<int> row_pos, pos_map;                  // [R] torus position; [B][nkx*nky] row or -1
     DevBuf<int> sys_row0;                          // [B + 1] first row of each system
     DevBuf<int> nbr, tile_row0, tile_nrow, tile_sys, sys_tile0, sys_spec_row, row_sys;
     // solver state
@@ -135,7 +182,8 @@ struct msc_plan {
     // autotuning record: microseconds per candidate
     std::vector<std::pair<std::string, float>> tune_log;
     std::string tune_report;
-    DevBuf<int> work, pos_row, tap_window;
+    DevBuf<int> work, tap_window;
+    DevBuf<int2> taps_d;                      // [K] tap offsets (dx, dy)
     DevBuf<int> sys_counter;       // per-system arrival counters of the fused Arnoldi kernels
     cudaStream_t stream = nullptr;
     cudaGraphExec_t g_start = nullptr, g_iter = nullptr;
@@ -169,7 +217,7 @@ struct msc_plan {
         h2.release(); y.release(); scale.release(); bnorm.release(); resid.release();
         est.release(); active.release(); kcyc.release(); iters.release(); cycles.release();
         unfinished.release(); status.release(); counter.release(); beta0.release();
-        sys_counter.release(); work.release(); pos_row.release(); tap_window.release();
+        sys_counter.release(); work.release(); tap_window.release(); taps_d.release();
         E32.release(); ET32.release(); lam32.release(); en32.release(); row_pkd32.release();
         row_fn32.release(); Vt32.release(); row_c32.release(); Q32.release(); W32.release();
         U32.release(); R64.release(); e_img.release(); tc_error.release();
@@ -333,7 +381,7 @@ void launch_halo(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in
                  C2<R> *out, cudaStream_t st)
 {
     constexpr int ZC = halo_zc<R>();
-    msc::CouplingTiles ct{p->work.p, p->pos_row.p, p->tap_window.p, p->nwork, p->nkx, p->nky,
+    msc::CouplingTiles ct{p->work.p, p->pos_map.p, p->tap_window.p, p->nwork, p->nkx, p->nky,
                           p->halo_hx, p->K};
     dim3 grid(p->nwork, (p->n + ZC - 1) / ZC);
     msc::k_coupling_halo<HY, kHaloBX, ZC, YS, R>
@@ -924,9 +972,32 @@ msc_status autotune_measure(msc_plan *p)
 }
 
 // Build rows, tiles, neighbour tables; upload everything; allocate state.
+// Set-up phase timer: MSC_PROFILE_SETUP=1 prints the wall time of each plan
+// set-up phase (device synchronised at the marks) to stderr.
+struct SetupTimer {
+    bool on = false;
+    std::chrono::steady_clock::time_point t0;
+    SetupTimer()
+    {
+        const char *e = std::getenv("MSC_PROFILE_SETUP");
+        on = e && e[0] == '1';
+        t0 = std::chrono::steady_clock::now();
+    }
+    void mark(const char *what)
+    {
+        if (!on) return;
+        cudaDeviceSynchronize();
+        const auto t = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "msc setup %-22s %8.2f ms\n", what,
+                     std::chrono::duration<double, std::milli>(t - t0).count());
+        t0 = t;
+    }
+};
+
 msc_status finalize(msc_plan *p)
 {
     if (p->finalized) return MSC_OK;
+    SetupTimer tm;
     if (!p->potential_set) return fail(MSC_ERR_ARG, "potential not set");
     for (int s = 0; s < p->B; ++s)
         if (!p->sys[s].set) return fail(MSC_ERR_ARG, "system " + std::to_string(s) + " not set");
@@ -952,28 +1023,23 @@ msc_status finalize(msc_plan *p)
     p->sys_tile0_h[p->B] = (int)p->tile_row0_h.size();
     p->ntiles = (int)p->tile_row0_h.size();
     // per-row data and neighbour table
-    std::vector<double> pkd(p->R), fn(p->R);
+    // per-row data; position tables (row of each torus position per system)
+    const int ntor = p->nkx * p->nky;
+    std::vector<double> pkd(p->R);
     std::vector<double2> rc(p->R), rb(p->R), bspec(p->B), aspec(p->B);
-    std::vector<int> spec_row(p->B), nbr((size_t)p->R * std::max(p->K, 1), -1);
-    std::vector<int> lookup((size_t)p->nkx * p->nky);
+    std::vector<int> spec_row(p->B), row_pos(p->R), pos_map((size_t)p->B * ntor, -1);
     for (int s = 0; s < p->B; ++s) {
         const SystemHost &sh = p->sys[s];
         const int r0 = p->sys_row0_h[s];
-        std::fill(lookup.begin(), lookup.end(), -1);
-        for (int j = 0; j < sh.C; ++j) lookup[(size_t)sh.ix[j] * p->nky + sh.iy[j]] = r0 + j;
+        int *map = pos_map.data() + (size_t)s * ntor;
         for (int j = 0; j < sh.C; ++j) {
             const int row = r0 + j;
+            const int q = sh.ix[j] * p->nky + sh.iy[j];
+            row_pos[row] = q;
+            map[q] = row;
             pkd[row] = sh.pkd[j];
             rc[row] = sh.c[j];
             rb[row] = sh.b[j];
-            double f = 0.0;
-            for (int k = 0; k < n; ++k) f += p->en_host[k] * p->en_host[k] / (sh.pkd[j] + p->lam_host[k]);
-            fn[row] = f;
-            for (int t = 0; t < p->K; ++t) {
-                const int sx = ((sh.ix[j] - p->taps[t].first) % p->nkx + p->nkx) % p->nkx;
-                const int sy = ((sh.iy[j] - p->taps[t].second) % p->nky + p->nky) % p->nky;
-                nbr[(size_t)row * p->K + t] = lookup[(size_t)sx * p->nky + sy];
-            }
         }
         spec_row[s] = r0 + sh.spec;
         bspec[s] = sh.b[sh.spec];
@@ -986,15 +1052,33 @@ msc_status finalize(msc_plan *p)
     for (int s = 0; s < p->B; ++s) p->rhs_default_h[spec_row[s]] = bspec[s];
     p->row_c_h = rc;
 
+    tm.mark("host row tables");
     MSC_CUDA(upload(p->row_pkd, pkd));
-    MSC_CUDA(upload(p->row_fn, fn));
     MSC_CUDA(upload(p->row_c, rc));
     MSC_CUDA(upload(p->row_b, rb));
     MSC_CUDA(upload(p->row_rhs, p->rhs_default_h));
     MSC_CUDA(upload(p->sys_row0, p->sys_row0_h));
     MSC_CUDA(upload(p->sys_aspec, aspec));
     MSC_CUDA(upload(p->sys_spec_row, spec_row));
-    MSC_CUDA(upload(p->nbr, nbr));
+    MSC_CUDA(upload(p->row_pos, row_pos));
+    MSC_CUDA(upload(p->pos_map, pos_map));
+    MSC_CUDA(upload(p->row_sys, p->row_sys_h));
+    {
+        std::vector<int2> taps(std::max(p->K, 1), make_int2(0, 0));
+        for (int t = 0; t < p->K; ++t) taps[t] = make_int2(p->taps[t].first, p->taps[t].second);
+        MSC_CUDA(upload(p->taps_d, taps));
+    }
+    MSC_CUDA(p->row_fn.alloc(p->R));
+    MSC_CUDA(p->nbr.alloc((size_t)p->R * std::max(p->K, 1)));
+    if (p->K == 0) MSC_CUDA(cudaMemset(p->nbr.p, 0xff, p->nbr.count * sizeof(int)));
+    if (p->mixed) MSC_CUDA(p->row_fn32.alloc(p->R));
+    msc::k_row_tables<<<std::min((p->R + 255) / 256, 4096), 256>>>(
+        p->R, n, p->K, p->nkx, p->nky, p->row_pos.p, p->row_sys.p, p->pos_map.p, p->taps_d.p,
+        p->row_pkd.p, p->en.p, p->lam.p, p->row_fn.p, p->mixed ? p->row_fn32.p : nullptr,
+        p->K > 0 ? p->nbr.p : nullptr);
+    MSC_CUDA(cudaGetLastError());
+    MSC_CUDA(cudaDeviceSynchronize());
+    tm.mark("row tables (device)");
     {
         // Halo-tiled coupling: signed tap reach, tap window, position->row
         // tables and the list of 8 x kHaloBX position patches that hold
@@ -1021,16 +1105,13 @@ msc_status finalize(msc_plan *p)
             std::vector<int> win((size_t)(2 * hx + 1) * wy, -1);
             for (int t = 0; t < p->K; ++t)
                 win[(size_t)(sgn[t].first + hx) * wy + (sgn[t].second + hyt)] = t;
-            const int npos = p->nkx * p->nky;
-            std::vector<int> pr((size_t)p->B * npos, -1), wl;
+            std::vector<int> wl;
             const int nbx = (p->nkx + kHaloBX - 1) / kHaloBX, nby = (p->nky + 7) / 8;
             for (int s2 = 0; s2 < p->B; ++s2) {
                 const SystemHost &sh = p->sys[s2];
                 std::vector<char> occ((size_t)nbx * nby, 0);
-                for (int j = 0; j < sh.C; ++j) {
-                    pr[(size_t)s2 * npos + sh.ix[j] * p->nky + sh.iy[j]] = p->sys_row0_h[s2] + j;
+                for (int j = 0; j < sh.C; ++j)
                     occ[(size_t)(sh.ix[j] / kHaloBX) * nby + sh.iy[j] / 8] = 1;
-                }
                 for (int bx = 0; bx < nbx; ++bx)
                     for (int by = 0; by < nby; ++by)
                         if (occ[(size_t)bx * nby + by]) {
@@ -1041,29 +1122,27 @@ msc_status finalize(msc_plan *p)
             }
             p->nwork = (int)(wl.size() / 3);
             MSC_CUDA(upload(p->tap_window, win));
-            MSC_CUDA(upload(p->pos_row, pr));
             MSC_CUDA(upload(p->work, wl));
         }
     }
+    tm.mark("halo tables");
     MSC_CUDA(upload(p->tile_row0, p->tile_row0_h));
     MSC_CUDA(upload(p->tile_nrow, p->tile_nrow_h));
     MSC_CUDA(upload(p->tile_sys, p->tile_sys_h));
     MSC_CUDA(upload(p->sys_tile0, p->sys_tile0_h));
-    MSC_CUDA(upload(p->row_sys, p->row_sys_h));
     MSC_CUDA(upload(p->bnorm, bn));
     if (p->mixed) {
-        std::vector<float> pkd32(p->R), fn32(p->R);
+        std::vector<float> pkd32(p->R);
         std::vector<float2> c32(p->R);
         for (int r = 0; r < p->R; ++r) {
             pkd32[r] = (float)pkd[r];
-            fn32[r] = (float)fn[r];
             c32[r] = make_float2((float)rc[r].x, (float)rc[r].y);
         }
         MSC_CUDA(upload(p->row_pkd32, pkd32));
-        MSC_CUDA(upload(p->row_fn32, fn32));
         MSC_CUDA(upload(p->row_c32, c32));
     }
 
+    tm.mark("tile uploads");
     const size_t vs = (size_t)p->R * n;
     const int m = p->m;
     p->pstride = m + 2;
@@ -1111,14 +1190,17 @@ msc_status finalize(msc_plan *p)
     MSC_CUDA(cudaMemset(p->h1.p, 0, p->h1.count * sizeof(double2)));
     MSC_CUDA(cudaMemset(p->y.p, 0, p->y.count * sizeof(double2)));
 
+    tm.mark("solver allocations");
     {
         msc_status tst = setup_tensor_core(p);
         if (tst != MSC_OK) return tst;
     }
+    tm.mark("tensor-core setup");
     {
         msc_status tst = autotune(p);
         if (tst != MSC_OK) return tst;
     }
+    tm.mark("autotune");
     MSC_CUDA(cudaMallocHost(&p->kcyc_host, p->B * sizeof(int)));
     for (int s = 0; s < p->B; ++s) p->kcyc_host[s] = 0;
     p->tev.resize((size_t)msc_plan::kKinds * (m + 1) * 2);
@@ -1127,6 +1209,7 @@ msc_status finalize(msc_plan *p)
     if (st != MSC_OK) return st;
     st = capture(p, record_cycle_iterations, &p->g_iter, &p->launches_iter);
     if (st != MSC_OK) return st;
+    tm.mark("graph capture");
     p->finalized = true;
     return MSC_OK;
 }
@@ -1214,8 +1297,20 @@ msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc)
 msc_status msc_plan_destroy(msc_plan *plan)
 {
     if (!plan) return MSC_OK;
+    SetupTimer tm;
     cudaStreamSynchronize(plan->stream);
+    cudaDeviceSynchronize();     // nothing may still use the buffers going back to the pool
     delete plan;
+    tm.mark("plan destroy");
+    return MSC_OK;
+}
+
+msc_status msc_release_cached_memory(void)
+{
+    cudaMemPool_t pool;
+    MSC_CUDA(plan_pool(&pool));
+    MSC_CUDA(cudaDeviceSynchronize());
+    MSC_CUDA(cudaMemPoolTrimTo(pool, 0));
     return MSC_OK;
 }
 
@@ -1632,20 +1727,6 @@ msc_status msc_potential_gradient(msc_plan *p, const double *psi, const double *
     msc_status st = finalize(p);
     if (st != MSC_OK) return st;
     const int nkx = p->nkx, nky = p->nky, n = p->n, ntor = nkx * nky;
-    if (!p->pos_map.p) {
-        std::vector<int> pos(p->R), map((size_t)p->B * ntor, -1);
-        for (int s = 0; s < p->B; ++s) {
-            const SystemHost &sh = p->sys[s];
-            const int r0 = p->sys_row0_h[s];
-            for (int j = 0; j < sh.C; ++j) {
-                const int q = sh.ix[j] * nky + sh.iy[j];
-                pos[r0 + j] = q;
-                map[(size_t)s * ntor + q] = r0 + j;
-            }
-        }
-        MSC_CUDA(upload(p->row_pos, pos));
-        MSC_CUDA(upload(p->pos_map, map));
-    }
     int wx = nkx, hx = 0, wy = nky, hy = 0;
     if (half_x >= 0 && 2 * half_x + 1 < nkx) {
         wx = 2 * half_x + 1;

@@ -296,6 +296,12 @@ class ScatteringPlan:
         return int(self._lib.msc_plan_uses_tensor_cores(self._plan))
 
 
+def release_cached_memory() -> None:
+    """Give the library's unused plan memory on the current device back to the driver."""
+    lib = nat.load()
+    nat.check("msc_release_cached_memory", lib.msc_release_cached_memory())
+
+
 def _device_rows(t, dtype, rows: int) -> torch.Tensor:
     t = torch.as_tensor(t).to(device=torch.device("cuda", torch.cuda.current_device()),
                               dtype=dtype).contiguous()
