@@ -781,6 +781,13 @@ constexpr int kProjGroup = 8;   // basis vectors per accumulation pass
 
 constexpr int kProjSlots = 2 * kProjGroup + 1;   // re/im per vector + |w|^2
 
+// Elements per thread per step of the projection loops: P1 streams Q from
+// DRAM over large row chunks and wants many loads in flight; P2's second
+// projection re-reads, from L1/L2, the small row tile its update pass just
+// touched, and is best left at one element per step.
+template <typename R> struct ProjUnroll { static constexpr int p1 = 4, p2 = 1; };
+template <> struct ProjUnroll<double> { static constexpr int p1 = 2, p2 = 1; };
+
 // Block sums of the accumulator slots in use: slots i < 2 gn, and slot
 // kProjSlots - 1 (the norm) when with_norm.  Results in red[slot].
 __device__ __forceinline__ void block_sum(double (&v)[kProjSlots], int gn, bool with_norm,
@@ -819,7 +826,7 @@ __device__ __forceinline__ void elem_range(const ArnoldiArgs &a, int tile, int s
 
 // Partial dot products of this block: slots [0, nvec) = Q_i^H w, slot nvec =
 // |w|^2 when with_norm.  Written to out[*].
-template <typename R>
+template <typename R, int U>
 __device__ void block_project(const ArnoldiArgs &a, const typename CT<R>::t *Q, int nvec,
                               const typename CT<R>::t *W, size_t e0, int ne, int with_norm,
                               double2 *out)
@@ -835,18 +842,35 @@ __device__ void block_project(const ArnoldiArgs &a, const typename CT<R>::t *Q, 
         double acc[kProjSlots];
 #pragma unroll
         for (int i = 0; i < kProjSlots; ++i) acc[i] = 0.0;
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            const C2 w = W[e0 + e];
+        // U elements per thread per step, every load of the step issued before
+        // the arithmetic: the kernel is bound by loads in flight, not by math.
+        for (int base = threadIdx.x; base < ne; base += blockDim.x * U) {
+            C2 w[U];
+            C2 q[kProjGroup][U];
 #pragma unroll
-            for (int i = 0; i < kProjGroup; ++i) {
-                if (i < gn) {
-                    const C2 q = Q[(size_t)(g0 + i) * a.qstride + e0 + e];
-                    acc[2 * i] = fma((double)q.x, (double)w.x, fma((double)q.y, (double)w.y, acc[2 * i]));
-                    acc[2 * i + 1] = fma((double)q.x, (double)w.y, fma(-(double)q.y, (double)w.x, acc[2 * i + 1]));
-                }
+            for (int u = 0; u < U; ++u) {
+                const int e = base + u * blockDim.x;
+                w[u] = (e < ne) ? W[e0 + e] : mk2<R>(0, 0);
             }
-            if (norm_here)
-                acc[kProjSlots - 1] = fma((double)w.x, (double)w.x, fma((double)w.y, (double)w.y, acc[kProjSlots - 1]));
+#pragma unroll
+            for (int i = 0; i < kProjGroup; ++i)
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int e = base + u * blockDim.x;
+                    q[i][u] = (i < gn && e < ne) ? Q[(size_t)(g0 + i) * a.qstride + e0 + e]
+                                                 : mk2<R>(0, 0);
+                }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double wx = (double)w[u].x, wy = (double)w[u].y;
+#pragma unroll
+                for (int i = 0; i < kProjGroup; ++i) {
+                    const double qx = (double)q[i][u].x, qy = (double)q[i][u].y;
+                    acc[2 * i] = fma(qx, wx, fma(qy, wy, acc[2 * i]));
+                    acc[2 * i + 1] = fma(qx, wy, fma(-qy, wx, acc[2 * i + 1]));
+                }
+                if (norm_here) acc[kProjSlots - 1] = fma(wx, wx, fma(wy, wy, acc[kProjSlots - 1]));
+            }
         }
         block_sum(acc, gn, norm_here, red_ws, red);
         if (threadIdx.x < gn) out[g0 + threadIdx.x] = make_double2(red[2 * threadIdx.x], red[2 * threadIdx.x + 1]);
@@ -888,7 +912,7 @@ __device__ __forceinline__ bool last_block_reduce(const ArnoldiArgs &a, int s, i
 
 // P1: h1 = Q^H w
 template <typename R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
 k_arnoldi_p1(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
              const typename CT<R>::t *__restrict__ W, double2 *__restrict__ h1, int hstride)
 {
@@ -898,7 +922,8 @@ k_arnoldi_p1(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
     size_t e0;
     int ne;
     elem_range<R>(a, tile, sub, e0, ne);
-    block_project<R>(a, Q, nvec, W, e0, ne, 0, a.partial + (size_t)blockIdx.x * a.pstride);
+    block_project<R, ProjUnroll<R>::p1>(a, Q, nvec, W, e0, ne, 0,
+                                        a.partial + (size_t)blockIdx.x * a.pstride);
     last_block_reduce(a, s, nvec, h1 + (size_t)s * hstride);
 }
 
@@ -942,7 +967,8 @@ k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
     }
     __syncthreads();
     }   // cgs2
-    block_project<R>(a, Q, nvec, W, e0, ne, 1, a.partial + (size_t)blockIdx.x * a.pstride);
+    block_project<R, ProjUnroll<R>::p2>(a, Q, nvec, W, e0, ne, 1,
+                                        a.partial + (size_t)blockIdx.x * a.pstride);
     if (last_block_reduce(a, s, nvec + 1, st.h2 + (size_t)s * hs)) {
         if (threadIdx.x == 0) arnoldi_givens(st, s, m, j, rtol, max_iter, inner_rtol, cgs2 != 0);
     }

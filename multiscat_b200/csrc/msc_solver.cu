@@ -174,7 +174,11 @@ struct msc_plan {
     DevBuf<int> tc_error;
     DevBuf<int> active, kcyc, iters, cycles, unfinished, status, counter;
     int *counter_host = nullptr;   // pinned
-    int split = 1;                 // Arnoldi blocks per row tile
+    // Arnoldi blocks: runs of rows of one system ("chunks", first projection)
+    // and row tiles split `split` ways (update + second projection)
+    int nchunks = 0;
+    int split = 1;
+    DevBuf<int> chunk_row0, chunk_nrow, chunk_sys, sys_chunk0;
     // halo-tiled coupling
     bool use_halo = false;             // halo tables built (taps reach <= 8)
     int halo32 = 0, halo64 = 0;    // autotuned coupling kind per precision (0 nbr, 1/2 halo)
@@ -212,6 +216,7 @@ struct msc_plan {
         row_rhs.release(); sys_aspec.release(); row_pos.release(); pos_map.release();
         sys_row0.release(); nbr.release(); tile_row0.release();
         tile_nrow.release(); tile_sys.release(); sys_tile0.release(); sys_spec_row.release();
+        chunk_row0.release(); chunk_nrow.release(); chunk_sys.release(); sys_chunk0.release();
         row_sys.release(); X.release(); W.release(); U.release(); TMP.release(); Q.release();
         partial.release(); H.release(); cs.release(); sn.release(); g.release(); h1.release();
         h2.release(); y.release(); scale.release(); bnorm.release(); resid.release();
@@ -226,6 +231,10 @@ struct msc_plan {
     msc::Tiles tiles() const
     {
         return msc::Tiles{tile_row0.p, tile_nrow.p, tile_sys.p, ntiles};
+    }
+    msc::Tiles chunks() const
+    {
+        return msc::Tiles{chunk_row0.p, chunk_nrow.p, chunk_sys.p, nchunks};
     }
     msc::GmresState state() const
     {
@@ -460,14 +469,16 @@ void launch_update(msc_plan *p, const int *gate, int nvec, const int *nvec_sys,
 
 int sys_blocks(int B) { return (B + 127) / 128; }
 
-msc::ArnoldiArgs arnoldi_args(msc_plan *p, const int *gate)
+// Block layout of an Arnoldi kernel: large row chunks (P1) or row tiles
+// split into about 600 blocks in all (P2).
+msc::ArnoldiArgs arnoldi_args(msc_plan *p, const int *gate, bool chunks)
 {
     msc::ArnoldiArgs a;
-    a.tiles = p->tiles();
-    a.sys_tile0 = p->sys_tile0.p;
+    a.tiles = chunks ? p->chunks() : p->tiles();
+    a.sys_tile0 = chunks ? p->sys_chunk0.p : p->sys_tile0.p;
     a.gate = gate;
     a.n = p->n;
-    a.split = p->split;
+    a.split = chunks ? 1 : p->split;
     a.qstride = (size_t)p->R * p->n;
     a.partial = p->partial.p;
     a.pstride = p->pstride;
@@ -526,19 +537,21 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
         if (tm) mark(p, 1, j, 0, st);
         launch_coupling_t<R>(p, p->active.p, U, Qj, R(1), W, st);
         if (tm) mark(p, 1, j, 1, st);
-        const msc::ArnoldiArgs aa = arnoldi_args(p, p->active.p);
-        const unsigned nblk = (unsigned)(p->ntiles * p->split);
+        const msc::ArnoldiArgs a1 = arnoldi_args(p, p->active.p, true);
+        const msc::ArnoldiArgs a2 = arnoldi_args(p, p->active.p, false);
+        const unsigned nblk1 = (unsigned)p->nchunks;
+        const unsigned nblk2 = (unsigned)(p->ntiles * p->split);
         // Two Gram-Schmidt passes; the mixed form may opt into one pass with
         // the Pythagorean norm (the FP64 true residual of the next refinement
         // step absorbs the loss of orthogonality, at the price of iterations).
         const int cgs2 = p->cgs1_inner ? 0 : 1;
         if (cgs2) {
             if (tm) mark(p, 2, j, 0, st);
-            msc::k_arnoldi_p1<R><<<nblk, 256, 0, st>>>(aa, Q, j + 1, W, p->h1.p, p->m + 2);
+            msc::k_arnoldi_p1<R><<<nblk1, 256, 0, st>>>(a1, Q, j + 1, W, p->h1.p, p->m + 2);
             if (tm) mark(p, 2, j, 1, st);
         }
         if (tm) mark(p, 3, j, 0, st);
-        msc::k_arnoldi_p2<R><<<nblk, 256, 0, st>>>(aa, Q, j + 1, W, p->state(), p->m, j,
+        msc::k_arnoldi_p2<R><<<nblk2, 256, 0, st>>>(a2, Q, j + 1, W, p->state(), p->m, j,
                                                    p->desc.rtol, p->desc.max_iterations, inner,
                                                    cgs2);
         if (tm) mark(p, 3, j, 1, st);
@@ -1159,13 +1172,38 @@ msc_status finalize(msc_plan *p)
         MSC_CUDA(p->Q.alloc(vs * (m + 1)));
     }
     {
-        // Enough Arnoldi blocks to fill the GPU (about 600 blocks of 256
-        // threads), without splitting a tile below 256 elements per block.
+        // Arnoldi chunks: about 4096 elements (16 per thread) per block, each
+        // block followed by one per-system reduction, but at least ~600
+        // blocks to fill the GPU; a chunk never spans two systems.
+        const int crow = std::max(1, std::min(std::max(1, 4096 / n), p->R / 600));
+        std::vector<int> c0, cn, cs, sc0(p->B + 1);
+        for (int s = 0; s < p->B; ++s) {
+            sc0[s] = (int)c0.size();
+            const int r0 = p->sys_row0_h[s], C = p->sys[s].C;
+            const int nch = (C + crow - 1) / crow;
+            for (int c = 0; c < nch; ++c) {
+                const int a = r0 + (int)((long long)C * c / nch);
+                const int b = r0 + (int)((long long)C * (c + 1) / nch);
+                c0.push_back(a);
+                cn.push_back(b - a);
+                cs.push_back(s);
+            }
+        }
+        sc0[p->B] = (int)c0.size();
+        p->nchunks = (int)c0.size();
+        MSC_CUDA(upload(p->chunk_row0, c0));
+        MSC_CUDA(upload(p->chunk_nrow, cn));
+        MSC_CUDA(upload(p->chunk_sys, cs));
+        MSC_CUDA(upload(p->sys_chunk0, sc0));
+    }
+    {
+        // P2: enough blocks to fill the GPU (about 600 blocks of 256 threads)
+        // without splitting a tile below 256 elements per block.
         const int tile_elems = msc::kTileRows * n;
         const int max_split = std::max(1, tile_elems / 256);
         p->split = std::max(1, std::min(max_split, (600 + p->ntiles - 1) / p->ntiles));
     }
-    MSC_CUDA(p->partial.alloc((size_t)p->ntiles * p->split * p->pstride));
+    MSC_CUDA(p->partial.alloc((size_t)std::max(p->ntiles * p->split, p->nchunks) * p->pstride));
     MSC_CUDA(p->sys_counter.alloc(p->B));
     MSC_CUDA(cudaMemset(p->sys_counter.p, 0, p->B * sizeof(int)));
     MSC_CUDA(p->H.alloc((size_t)p->B * (m + 1) * m));
@@ -1276,7 +1314,10 @@ msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc)
     p->m = desc->restart;
     p->mixed = desc->precision == MSC_PRECISION_MIXED;
     if (p->mixed) {
-        if (desc->inner_restart > 0) p->m = desc->inner_restart;
+        // The inner FP32 solve only has to gain inner_rtol (1e-5) per
+        // refinement step, which takes ~15-20 iterations here; longer inner
+        // cycles only add launches of systems that already stopped.
+        p->m = desc->inner_restart > 0 ? desc->inner_restart : std::min(desc->restart, 20);
         p->inner_rtol = desc->inner_rtol > 0.0 ? desc->inner_rtol : 1e-5;
         p->cgs1_inner = (desc->flags & 4) != 0;
         p->max_cycles = desc->max_refinements > 0 ? desc->max_refinements : 30;
