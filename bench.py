@@ -398,7 +398,8 @@ def cfg4_measurement(args, torch, stream) -> dict:
         inten[prec] = r.intensities
         out[prec] = {"solves_per_s": len(systems) / (ms / 1e3), "ms": ms,
                      "iterations_max": int(r.iterations.max()),
-                     "all_converged": bool((r.status == 0).all())}
+                     "all_converged": bool((r.status == 0).all()),
+                     "autotune": p.tuning_report()}
         p.close()
     out["max_abs_dI_mixed_vs_fp64"] = float((inten["mixed"] - inten["fp64"]).abs().max())
     out["mixed_over_fp64"] = out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]

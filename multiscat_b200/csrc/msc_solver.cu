@@ -666,7 +666,7 @@ msc_status set_kernel_attributes(int n, int K)
                                   (int)std::min<size_t>(halo_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448))); \
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_halo<HY, kHaloBX, halo_zc<R>(), 4, R>,        \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
-                                  (int)std::min<size_t>(halo_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448)));
+                                  (int)std::min<size_t>(halo_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448)));;
     MSC_HALO_ATTR(1, float)
     MSC_HALO_ATTR(2, float)
     MSC_HALO_ATTR(4, float)

@@ -330,3 +330,40 @@ def test_cfg4_batch_mixed_matches_fp64():
         inten = r64.system_intensities(s).cpu().numpy()
         assert abs(inten.sum() - 1.0) <= 1e-8
     mixed.close()
+
+
+# ---------------------------------------------------------------------------
+# Every coupling kernel the autotuner can pick (forced through MSC_TUNE):
+# FP64 operators against the neighbour-table kernel, and mixed solves of a
+# small uneven batch against the FP64 solve.
+# ---------------------------------------------------------------------------
+COUPLING_KINDS = {0: "neighbour", 1: "halo_y8", 2: "halo_y4"}
+
+
+@pytest.mark.parametrize("kind", sorted(COUPLING_KINDS))
+def test_every_coupling_kernel_agrees(kind, monkeypatch):
+    case, systems = cfg2_batch(n_solves=5, seed=4)
+    monkeypatch.setenv("MSC_TUNE", f"c64={kind},c32={kind},bi=128")
+    plan = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed")
+    res = plan.solve()
+    assert plan.tuning_report()["chosen"].startswith(f"coupling64={COUPLING_KINDS[kind]},"
+                                                     f"coupling32={COUPLING_KINDS[kind]}")
+    monkeypatch.setenv("MSC_TUNE", "c64=0,c32=0,bi=128")
+    ref = ScatteringPlan(case.v, case.t, systems, rtol=1e-10).solve()
+    assert (res.status == 0).all()
+    d = (res.intensities - ref.intensities).abs().max().item()
+    assert d <= MIXED_TOL, d
+    plan.close()
+    # FP64 operator of one full-grid system with this kind vs the neighbour
+    # table (a plan reads MSC_TUNE when its first call sets it up)
+    c0 = cfg0_case(nz=48)
+    x = torch.randn(c0.pkd.size, 48, dtype=torch.complex128, device="cuda")
+    monkeypatch.setenv("MSC_TUNE", f"c64={kind},c32={kind},bi=0")
+    pk = ScatteringPlan(c0.v, c0.t, [c0.system()])
+    yk = pk.apply_coupling(x)
+    monkeypatch.setenv("MSC_TUNE", "c64=0,c32=0,bi=0")
+    p0 = ScatteringPlan(c0.v, c0.t, [c0.system()])
+    y0 = p0.apply_coupling(x)
+    assert float((yk - y0).abs().max()) <= 1e-13 * float(y0.abs().max())
+    pk.close()
+    p0.close()
