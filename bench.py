@@ -127,14 +127,25 @@ def build_workload(name: str):
     raise ValueError(name)
 
 
-def kernel_work(name: str, n: int, rows: int, taps: int, mixed: bool) -> tuple[float, float]:
-    """Algorithmic (flops, bytes) of ONE launch over all `rows` channel rows.
+# FP32 FMA nominal peak of a B200 at its 1965 MHz boost clock (148 SMs x 128
+# lanes x 2 flop); the channel coupling runs on CUDA cores, not tensor cores.
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+# DRAM bytes of one full-batch cfg2 launch measured by ncu (profiles/), used
+# as the `traffic` of the roofline line for that workload.
+NCU_TRAFFIC_FULL_LAUNCH = {
+    ("cfg2", "coupling"): 439.8e6 + 138.9e6,
+    ("cfg2", "block_inverse"): 148.2e6 + 100.1e6,
+}
+
+
+def kernel_work(name: str, n: int, rows: float, taps: int, mixed: bool) -> tuple[float, float]:
+    """Algorithmic (flops, bytes) for `rows` channel rows processed.
 
     block inverse: two real GEMMs (n x n)(n x 2 rows) = 8 n^2 rows flop (x3 for
     the BF16x3 split on tensor cores); bytes: x in, u out.  coupling: 8 taps
     flop per complex output; bytes: source, addend and result vectors.
     Arnoldi kernels are byte-bound; their bytes depend on the step j and are
-    not attributed per launch here.
+    not attributed here.
     """
     es = 8 if mixed else 16
     nv = float(n) * rows
@@ -143,6 +154,17 @@ def kernel_work(name: str, n: int, rows: int, taps: int, mixed: bool) -> tuple[f
     if name == "coupling":
         return 8.0 * taps * nv, 3 * es * nv
     return 0.0, 0.0
+
+
+def rows_processed(res, name: str) -> float:
+    """Channel rows a kernel kind processed in one solve: each Krylov step of a
+    system runs the coupling over its rows; the block inverse also runs once
+    per restart / refinement cycle (the solution update)."""
+    rows = np.diff(res.row_offsets).astype(float)
+    steps = float(np.dot(rows, res.iterations))
+    if name == "block_inverse":
+        return steps + float(np.dot(rows, res.cycles))
+    return steps
 
 
 def timed_steps(plan, steps: int, stream, torch) -> float:
@@ -172,11 +194,8 @@ def run_b200(args) -> None:
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        from multiscat_b200.replicas import max_over_ranks as mor
+        return mor(x, device="cuda")
 
     case, systems = build_workload(args.workload)
     nsys = len(systems)
@@ -213,34 +232,52 @@ def run_b200(args) -> None:
     for k, v in kt.items():
         if not v["launches"]:
             continue
-        avg_s = v["ms"] / v["launches"] / 1e3
-        flops, nbytes = kernel_work(k, n, rows, taps, mixed)
+        t_s = v["ms"] / 1e3
+        flops, nbytes = kernel_work(k, n, rows_processed(res, k), taps, mixed)
         kernels[k] = {"what": KERNEL_NAMES[k], "launches": v["launches"],
-                      "avg_us": 1e6 * avg_s, "share_of_timed_kernels": v["ms"] / total_ms}
+                      "avg_us": 1e6 * t_s / v["launches"],
+                      "share_of_timed_kernels": v["ms"] / total_ms}
         if flops:
-            kernels[k]["achieved_tflops_full_batch_equivalent"] = flops / avg_s / 1e12
-            kernels[k]["achieved_gbs_full_batch_equivalent"] = nbytes / avg_s / 1e9
+            kernels[k]["achieved_tflops"] = flops / t_s / 1e12
+            kernels[k]["achieved_gbs"] = nbytes / t_s / 1e9
     dom = max(kt.items(), key=lambda kv: kv[1]["ms"])[0] if kt else None
     roof = None
     if dom and kt[dom]["launches"]:
-        avg_s = kt[dom]["ms"] / kt[dom]["launches"] / 1e3
-        flops, nbytes = kernel_work(dom, n, rows, taps, mixed)
+        nl = kt[dom]["launches"]
+        t_s = kt[dom]["ms"] / 1e3
+        rows_done = rows_processed(res, dom)
+        flops, nbytes = kernel_work(dom, n, rows_done, taps, mixed)
+        traffic = NCU_TRAFFIC_FULL_LAUNCH.get((args.workload, dom))
+        if traffic is not None and mixed:
+            traffic = traffic * (rows_done / nl) / rows      # at this run's average rows per launch
+        else:
+            traffic = None
         if dom == "block_inverse" and mixed and "tc_" in tuning.get("chosen", ""):
-            achieved = flops / avg_s / 1e12
+            achieved = flops / t_s / 1e12
             roof = {"kernel": f"{dom}: {KERNEL_NAMES[dom]} (tcgen05 BF16x3)", "bound": "tensor",
                     "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                    "frac": achieved / peaks["bf16_tflops"], "traffic": None}
+                    "frac": achieved / peaks["bf16_tflops"], "traffic": traffic}
         else:
-            achieved = nbytes / avg_s / 1e9
+            achieved = nbytes / t_s / 1e9
             roof = {"kernel": f"{dom}: {KERNEL_NAMES[dom]}", "bound": "hbm",
                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": achieved / peaks["hbm_gbs"], "traffic": None}
+                    "frac": achieved / peaks["hbm_gbs"], "traffic": traffic}
             if flops:
-                roof["achieved_tflops"] = flops / avg_s / 1e12
+                roof["achieved_tflops"] = flops / t_s / 1e12
+                if dom == "coupling" and mixed:
+                    roof["fp32_fma_nominal_tflops"] = FP32_NOMINAL_TFLOPS
+                    roof["frac_of_fp32_fma_nominal"] = roof["achieved_tflops"] / FP32_NOMINAL_TFLOPS
+                    roof["note"] = ("the coupling is arithmetic on CUDA cores (FP32 FMA); its HBM "
+                                    "fraction is low by design, the FP32 fraction is the one "
+                                    "that bounds it")
         roof.update({"peak_source": f"{peak_kind} (MEASURED_PEAKS.json)",
-                     "avg_launch_us": 1e6 * avg_s, "launches_timed": kt[dom]["launches"],
-                     "per_launch_work": ("all rows of the batch; launches of systems already "
-                                         "converged skip their rows, so this is a lower bound"),
+                     "avg_launch_us": 1e6 * t_s / nl, "launches_timed": nl,
+                     "per_launch_work": (f"{rows_done / nl:.0f} channel rows per launch on "
+                                         f"average ({rows} in the batch; converged systems "
+                                         "skip their rows), x algorithmic work per row"),
+                     "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of a "
+                                        "full-batch launch (profiles/), scaled to the average "
+                                        "rows per launch") if traffic else None,
                      "share": kt[dom]["ms"] / total_ms})
 
     extra = {}
