@@ -20,11 +20,15 @@
 // threads themselves (FP32 -> BF16 hi/lo, re/im de-interleaved).
 //
 // Execution.  Persistent CTAs (one per SM, 256 threads = 8 warps).  Per tile:
-// stage B, one thread issues the MMAs and commits to an mbarrier, all warps
-// read the accumulator with tcgen05.ld (warp w owns TMEM lanes
-// 32 (w % 4)..32 (w % 4) + 31 and the column half w / 4),
-// form the Sherman-Morrison scalars and yt (pkd + lam in FP64), stage yt as
-// the next B operand, second GEMM, store u.  Every mbarrier wait is bounded;
+// stage x as B with 16-byte stores; one thread issues the MMAs and commits to
+// an mbarrier; all warps read the accumulator with tcgen05.ld (warp w owns
+// TMEM lanes 32 (w % 4)..32 (w % 4) + 31 and the column half w / 4), reduce
+// the Sherman-Morrison sums over k with a reduce-scatter butterfly, form
+// yt (pkd + lam in FP64) and stage it as the MN-major B operand of the second
+// GEMM with 16-byte stores, store u.  beta is formed from the accumulator
+// before the division by pkd + lam (adding the correction after the second
+// GEMM instead, u = u0 + beta (H0 + pkd)^-1 e_n, cancels two large terms in
+// FP32 near resonances of H0 + pkd and stalls the refinement).  Every mbarrier wait is bounded;
 // on time-out the kernel records an error code, stops issuing work and still
 // releases its TMEM.
 #pragma once
@@ -156,16 +160,53 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo_bytes
     return d;
 }
 
-// Instruction descriptor: BF16 x BF16 -> FP32, M = 128, given N and A major-ness.
-__host__ __device__ constexpr uint32_t make_idesc(int n, int a_mn_major)
+// Instruction descriptor: BF16 x BF16 -> FP32, M = 128, given N and the
+// major-ness of A and B (0 K-major, 1 MN-major).
+__host__ __device__ constexpr uint32_t make_idesc(int n, int a_mn_major, int b_mn_major)
 {
     return (1u << 4)                         // D format F32
            | (1u << 7)                       // A format BF16
            | (1u << 10)                      // B format BF16
-           | ((uint32_t)a_mn_major << 15)    // A major: 0 K-major, 1 MN-major
-           | (0u << 16)                      // B K-major
+           | ((uint32_t)a_mn_major << 15)    // A major
+           | ((uint32_t)b_mn_major << 16)    // B major
            | ((uint32_t)(n >> 3) << 17)      // N / 8
            | ((uint32_t)(128 >> 4) << 24);   // M / 16
+}
+
+// Reduce-scatter of 16 per-lane values over a warp: returns, in every lane,
+// the sum over all 32 lanes of value (lane >> 1) & 15 (lanes 2i and 2i + 1
+// hold the same column).  15 + 1 shuffles instead of 16 x 5; the order of
+// the additions is fixed, so the result is deterministic.
+__device__ __forceinline__ float warp_reduce_scatter16(float (&v)[16], int lane)
+{
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {          // lanes with bit 4 set keep columns 8..15
+        const bool up = lane & 16;
+        const float send = up ? v[i] : v[i + 8];
+        const float keep = up ? v[i + 8] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {          // bit 3: upper 4 of the 8
+        const bool up = lane & 8;
+        const float send = up ? v[i] : v[i + 4];
+        const float keep = up ? v[i + 4] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {          // bit 2
+        const bool up = lane & 4;
+        const float send = up ? v[i] : v[i + 2];
+        const float keep = up ? v[i + 2] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+    {                                      // bit 1
+        const bool up = lane & 2;
+        const float send = up ? v[0] : v[1];
+        const float keep = up ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
 }
 
 struct TcParams {
@@ -197,6 +238,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N must be a multiple of 16 in [16, 256]");
     // Supports n <= 256 (at most two M tiles of 128).
     constexpr int TR = N / 2;                 // channels per tile
+    constexpr int P = kThreads / TR;          // staging threads per channel
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t bar_e, bar_mma;
     __shared__ uint32_t tmem_base_s;
@@ -243,11 +285,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     bool e_waited = false;
     uint32_t mma_phase = 0;
     bool mma_pending = false;
-    const uint32_t idesc_mn = make_idesc(N, 1);   // GEMM 1: A = E^T via the MN-major view
-    const uint32_t idesc_k = make_idesc(N, 0);    // GEMM 2: A = E, K-major
+    const uint32_t idesc_mn = make_idesc(N, 1, 0);   // GEMM 1: A = E^T via the MN-major view, B K-major
+    const uint32_t idesc_k = make_idesc(N, 0, 1);    // GEMM 2: A = E K-major, B MN-major
     const uint32_t e_hi_a = smem_u32(e_hi), e_lo_a = smem_u32(e_lo);
     const uint32_t b_hi_a = smem_u32(b_hi), b_lo_a = smem_u32(b_lo);
     const int ksteps = kp >> 4;
+    const int sj = tid % TR, sp = tid / TR;               // staging: channel, z-block phase
 
     for (int tile = blockIdx.x; tile < prm.ntiles && ok; tile += gridDim.x) {
         const int row0 = tile * TR;
@@ -261,32 +304,38 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         for (int j = tid; j < TR; j += kThreads) pkd_s[j] = (j < nrow) ? prm.row_pkd[row0 + j] : 0.0;
         if (!__syncthreads_or(tid == 0 ? any : 0)) continue;
 
-        // ---- stage x as the B operand of GEMM 1 (rows = 2 TR re/im columns, K = z).
-        // Loads are batched (kBatch per thread in flight) because one CTA per
-        // SM has only four warps to hide memory latency with.
-        constexpr int kBatch = 16;
-        for (int base = tid; base < TR * kp; base += kThreads * kBatch) {
-            float2 v[kBatch];
+        // ---- stage x as the B operand of GEMM 1 (K-major: rows = 2 TR re/im
+        // columns, K = z).  Thread (channel sj, z-blocks sp, sp + P, ...) loads
+        // 8 consecutive z (64 contiguous bytes) and writes four 16-byte units
+        // (re/im x hi/lo).
+        {
+            const bool jok = sj < nrow;
+            const float2 *xr = prm.x + (size_t)(row0 + sj) * n;
+            for (int zb = sp; zb < kb; zb += P) {
+                float2 v[8];
 #pragma unroll
-            for (int u = 0; u < kBatch; ++u) {
-                const int idx = base + u * kThreads;
-                const int j = idx / kp, z = idx - j * kp;
-                v[u] = make_float2(0.f, 0.f);
-                if (idx < TR * kp && j < nrow && z < n) v[u] = prm.x[(size_t)(row0 + j) * n + z];
-            }
+                for (int u = 0; u < 8; ++u) {
+                    const int z = zb * 8 + u;
+                    v[u] = (jok && z < n) ? xr[z] : make_float2(0.f, 0.f);
+                }
+                uint32_t rh[4], ih[4], rl[4], il[4];
 #pragma unroll
-            for (int u = 0; u < kBatch; ++u) {
-                const int idx = base + u * kThreads;
-                if (idx >= TR * kp) break;
-                const int j = idx / kp, z = idx - j * kp;
-                const __nv_bfloat16 hr = __float2bfloat16_rn(v[u].x), hi = __float2bfloat16_rn(v[u].y);
-                const __nv_bfloat16 lr = __float2bfloat16_rn(v[u].x - __bfloat162float(hr));
-                const __nv_bfloat16 li = __float2bfloat16_rn(v[u].y - __bfloat162float(hi));
-                const uint32_t o_re = kmaj_off(2 * j, z, N), o_im = kmaj_off(2 * j + 1, z, N);
-                *reinterpret_cast<__nv_bfloat16 *>(b_hi + o_re) = hr;
-                *reinterpret_cast<__nv_bfloat16 *>(b_hi + o_im) = hi;
-                *reinterpret_cast<__nv_bfloat16 *>(b_lo + o_re) = lr;
-                *reinterpret_cast<__nv_bfloat16 *>(b_lo + o_im) = li;
+                for (int u = 0; u < 8; u += 2) {
+                    const __nv_bfloat162 hr = __floats2bfloat162_rn(v[u].x, v[u + 1].x);
+                    const __nv_bfloat162 hi = __floats2bfloat162_rn(v[u].y, v[u + 1].y);
+                    const float2 fr = __bfloat1622float2(hr), fi = __bfloat1622float2(hi);
+                    const __nv_bfloat162 lr = __floats2bfloat162_rn(v[u].x - fr.x, v[u + 1].x - fr.y);
+                    const __nv_bfloat162 li = __floats2bfloat162_rn(v[u].y - fi.x, v[u + 1].y - fi.y);
+                    rh[u >> 1] = *reinterpret_cast<const uint32_t *>(&hr);
+                    ih[u >> 1] = *reinterpret_cast<const uint32_t *>(&hi);
+                    rl[u >> 1] = *reinterpret_cast<const uint32_t *>(&lr);
+                    il[u >> 1] = *reinterpret_cast<const uint32_t *>(&li);
+                }
+                const uint32_t o_re = kmaj_off(2 * sj, zb * 8, N), o_im = o_re + 16;
+                *reinterpret_cast<uint4 *>(b_hi + o_re) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+                *reinterpret_cast<uint4 *>(b_hi + o_im) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+                *reinterpret_cast<uint4 *>(b_lo + o_re) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+                *reinterpret_cast<uint4 *>(b_lo + o_im) = make_uint4(il[0], il[1], il[2], il[3]);
             }
         }
         fence_proxy_async();
@@ -328,6 +377,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         if (!__syncthreads_and(ok)) { ok = false; break; }
 
         // ---- epilogue 1a: Sherman-Morrison sums s_j = sum_k en_k xt_kj / (pkd_j + lam_k)
+        // from the accumulator itself (so beta is consistent with the xt that
+        // GEMM 2 consumes; pkd + lam in FP64).  Each 16-column chunk is
+        // reduced over the warp's 32 k-lanes by a reduce-scatter butterfly
+        // (16 shuffles), then over lane quarters and M tiles in a fixed order.
         for (int m = 0; m < mt_count && epi; ++m) {
             const int k = m * 128 + lq * 32 + lane;
             const bool valid = k < n;
@@ -339,19 +392,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
 #pragma unroll
                 for (int c = 0; c < 16; c += 2) {
                     const int j = (c0 + c) >> 1;
-                    float wr = 0.f, wi = 0.f;
-                    if (valid && j < nrow) {
-                        const float w = en_k / (float)(pkd_s[j] + lam_k);
-                        wr = w * v[c];
-                        wi = w * v[c + 1];
-                    }
-                    wr = warp_sum(wr);
-                    wi = warp_sum(wi);
-                    if (lane == 0) {
-                        sm_part[warp][m][c0 + c] = wr;
-                        sm_part[warp][m][c0 + c + 1] = wi;
-                    }
+                    float w = 0.f;
+                    if (valid && j < nrow) w = en_k * __frcp_rn((float)(pkd_s[j] + lam_k));
+                    v[c] *= w;
+                    v[c + 1] *= w;
                 }
+                const float sum = warp_reduce_scatter16(v, lane);
+                if ((lane & 1) == 0) sm_part[warp][m][c0 + ((lane >> 1) & 15)] = sum;
             }
         }
         __syncthreads();
@@ -373,8 +420,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         }
         __syncthreads();
 
-        // ---- epilogue 1b: yt = (xt + beta en) / (pkd + lam) as the B operand of GEMM 2
-        // (rows = 2 TR columns, K = k; rows k >= kp are never read, k in [n, kp) are zero)
+        // ---- epilogue 1b: yt = (xt + beta en) / (pkd + lam) as the B operand of
+        // GEMM 2 in the MN-major layout: one thread holds one k and 16
+        // consecutive columns, i.e. two 16-byte units per hi / lo part
+        // (rows k >= kp are never read; k in [n, kp) are zero).
         for (int m = 0; m < mt_count && epi; ++m) {
             const int k = m * 128 + lq * 32 + lane;
             const bool valid = k < n;
@@ -385,25 +434,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                 float v[16];
                 tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + c0), v);
                 if (!stage) continue;
+                uint32_t hw[8], lw[8];
 #pragma unroll
                 for (int c = 0; c < 16; c += 2) {
                     const int j = (c0 + c) >> 1;
                     float yr = 0.f, yi = 0.f;
                     if (valid && j < nrow) {
-                        const float inv = 1.0f / (float)(pkd_s[j] + lam_k);
+                        const float inv = __frcp_rn((float)(pkd_s[j] + lam_k));
                         const float2 b = beta_s[j];
                         yr = (v[c] + b.x * en_k) * inv;
                         yi = (v[c + 1] + b.y * en_k) * inv;
                     }
-                    const __nv_bfloat16 hr = __float2bfloat16_rn(yr), hi = __float2bfloat16_rn(yi);
-                    const __nv_bfloat16 lr = __float2bfloat16_rn(yr - __bfloat162float(hr));
-                    const __nv_bfloat16 li = __float2bfloat16_rn(yi - __bfloat162float(hi));
-                    const uint32_t o_re = kmaj_off(c0 + c, k, N), o_im = kmaj_off(c0 + c + 1, k, N);
-                    *reinterpret_cast<__nv_bfloat16 *>(b_hi + o_re) = hr;
-                    *reinterpret_cast<__nv_bfloat16 *>(b_hi + o_im) = hi;
-                    *reinterpret_cast<__nv_bfloat16 *>(b_lo + o_re) = lr;
-                    *reinterpret_cast<__nv_bfloat16 *>(b_lo + o_im) = li;
+                    const __nv_bfloat162 h = __floats2bfloat162_rn(yr, yi);
+                    const float2 fh = __bfloat1622float2(h);
+                    const __nv_bfloat162 l = __floats2bfloat162_rn(yr - fh.x, yi - fh.y);
+                    hw[c >> 1] = *reinterpret_cast<const uint32_t *>(&h);
+                    lw[c >> 1] = *reinterpret_cast<const uint32_t *>(&l);
                 }
+                // MN-major core matrix: (k, c) at ((k/8)(N/8) + c/8) 128 + (k%8) 16 + (c%8) 2
+                const uint32_t o = (uint32_t)(((k >> 3) * (N >> 3) + (c0 >> 3)) * 128 + (k & 7) * 16);
+                *reinterpret_cast<uint4 *>(b_hi + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                *reinterpret_cast<uint4 *>(b_hi + o + 128) = make_uint4(hw[4], hw[5], hw[6], hw[7]);
+                *reinterpret_cast<uint4 *>(b_lo + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                *reinterpret_cast<uint4 *>(b_lo + o + 128) = make_uint4(lw[4], lw[5], lw[6], lw[7]);
             }
         }
         tc_fence_before();
@@ -420,6 +473,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     const uint32_t a_off = (uint32_t)(m * 16) * sz + (uint32_t)(2 * s) * sk;
                     const uint64_t ah = make_desc(e_hi_a + a_off, sk, sz);
                     const uint64_t al = make_desc(e_lo_a + a_off, sk, sz);
+                    // B (MN-major): K-block (k) stride = 16 N (LBO), N-block stride = 128 (SBO)
                     const uint32_t b_off = (uint32_t)(2 * s) * b_lbo;
                     const uint64_t bh = make_desc(b_hi_a + b_off, b_lbo, 128);
                     const uint64_t bl = make_desc(b_lo_a + b_off, b_lbo, 128);
