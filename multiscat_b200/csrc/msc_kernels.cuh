@@ -781,12 +781,9 @@ constexpr int kProjGroup = 8;   // basis vectors per accumulation pass
 
 constexpr int kProjSlots = 2 * kProjGroup + 1;   // re/im per vector + |w|^2
 
-// Elements per thread per step of the projection loops: P1 streams Q from
-// DRAM over large row chunks and wants many loads in flight; P2's second
-// projection re-reads, from L1/L2, the small row tile its update pass just
-// touched, and is best left at one element per step.
-template <typename R> struct ProjUnroll { static constexpr int p1 = 4, p2 = 1; };
-template <> struct ProjUnroll<double> { static constexpr int p1 = 2, p2 = 1; };
+// Elements per thread per step of P2's second projection, which re-reads,
+// from L1/L2, the small row tile its update pass just touched.
+template <typename R> struct ProjUnroll { static constexpr int p2 = 1; };
 
 // Block sums of the accumulator slots in use: slots i < 2 gn, and slot
 // kProjSlots - 1 (the norm) when with_norm.  Results in red[slot].
@@ -910,20 +907,54 @@ __device__ __forceinline__ bool last_block_reduce(const ArnoldiArgs &a, int s, i
     return true;
 }
 
-// P1: h1 = Q^H w
+// P1: h1 = Q^H w.  One warp per basis vector (vectors warp, warp + 8, ...):
+// the warp streams its vector and the block's slice of w (re-read from L1
+// by the other warps) with U loads in flight per thread, two FP64
+// accumulators per thread, a warp sum, then the per-system last-block
+// reduction.  Few registers per thread, so the SM holds enough warps to
+// keep DRAM busy.
+template <typename R> struct P1Unroll { static constexpr int value = 8; };
+template <> struct P1Unroll<double> { static constexpr int value = 4; };
+
 template <typename R>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256)
 k_arnoldi_p1(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
              const typename CT<R>::t *__restrict__ W, double2 *__restrict__ h1, int hstride)
 {
+    using C2 = typename CT<R>::t;
+    constexpr int U = P1Unroll<R>::value;
     const int tile = blockIdx.x / a.split, sub = blockIdx.x - tile * a.split;
     const int s = a.tiles.sys[tile];
     if (a.gate && a.gate[s] == 0) return;
     size_t e0;
     int ne;
     elem_range<R>(a, tile, sub, e0, ne);
-    block_project<R, ProjUnroll<R>::p1>(a, Q, nvec, W, e0, ne, 0,
-                                        a.partial + (size_t)blockIdx.x * a.pstride);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    double2 *out = a.partial + (size_t)blockIdx.x * a.pstride;
+    const C2 *w = W + e0;
+    for (int i = warp; i < nvec; i += nw) {
+        const C2 *q = Q + (size_t)i * a.qstride + e0;
+        double sr = 0.0, si = 0.0;
+        for (int base = lane; base < ne; base += 32 * U) {
+            C2 qv[U], wv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = base + u * 32;
+                qv[u] = (e < ne) ? q[e] : mk2<R>(0, 0);
+                wv[u] = (e < ne) ? w[e] : mk2<R>(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double qx = (double)qv[u].x, qy = (double)qv[u].y;
+                const double wx = (double)wv[u].x, wy = (double)wv[u].y;
+                sr = fma(qx, wx, fma(qy, wy, sr));
+                si = fma(qx, wy, fma(-qy, wx, si));
+            }
+        }
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (lane == 0) out[i] = make_double2(sr, si);
+    }
     last_block_reduce(a, s, nvec, h1 + (size_t)s * hstride);
 }
 
