@@ -777,40 +777,6 @@ struct ArnoldiArgs {
     int *counter;           // [B] arrival counters (left at 0)
 };
 
-constexpr int kProjGroup = 8;   // basis vectors per accumulation pass
-
-constexpr int kProjSlots = 2 * kProjGroup + 1;   // re/im per vector + |w|^2
-
-// Elements per thread per step of P2's second projection, which re-reads,
-// from L1/L2, the small row tile its update pass just touched.
-template <typename R> struct ProjUnroll { static constexpr int p2 = 1; };
-
-// Block sums of the accumulator slots in use: slots i < 2 gn, and slot
-// kProjSlots - 1 (the norm) when with_norm.  Results in red[slot].
-__device__ __forceinline__ void block_sum(double (&v)[kProjSlots], int gn, bool with_norm,
-                                          double *red_ws, double *red)
-{
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int i = 0; i < kProjSlots; ++i) {
-        const bool used = (i < 2 * gn) || (with_norm && i == kProjSlots - 1);
-        if (used) {
-            const double t = warp_sum(v[i]);
-            if (lane == 0) red_ws[warp * kProjSlots + i] = t;
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x < kProjSlots) {
-        const int i = threadIdx.x;
-        const bool used = (i < 2 * gn) || (with_norm && i == kProjSlots - 1);
-        double t = 0.0;
-        if (used)
-            for (int w = 0; w < nw; ++w) t += red_ws[w * kProjSlots + i];
-        red[i] = t;
-    }
-    __syncthreads();
-}
-
 template <typename R>
 __device__ __forceinline__ void elem_range(const ArnoldiArgs &a, int tile, int sub, size_t &e0, int &ne)
 {
@@ -819,60 +785,6 @@ __device__ __forceinline__ void elem_range(const ArnoldiArgs &a, int tile, int s
     const int lo = min(tot, sub * per);
     e0 = (size_t)a.tiles.row0[tile] * a.n + lo;
     ne = min(tot, lo + per) - lo;
-}
-
-// Partial dot products of this block: slots [0, nvec) = Q_i^H w, slot nvec =
-// |w|^2 when with_norm.  Written to out[*].
-template <typename R, int U>
-__device__ void block_project(const ArnoldiArgs &a, const typename CT<R>::t *Q, int nvec,
-                              const typename CT<R>::t *W, size_t e0, int ne, int with_norm,
-                              double2 *out)
-{
-    using C2 = typename CT<R>::t;
-    __shared__ double red_ws[8 * kProjSlots];
-    __shared__ double red[kProjSlots];
-    const int ngroups = (nvec > 0) ? (nvec + kProjGroup - 1) / kProjGroup : (with_norm ? 1 : 0);
-    for (int gi = 0; gi < ngroups; ++gi) {
-        const int g0 = gi * kProjGroup;
-        const int gn = min(kProjGroup, nvec - g0);
-        const bool norm_here = with_norm && (gi == ngroups - 1);
-        double acc[kProjSlots];
-#pragma unroll
-        for (int i = 0; i < kProjSlots; ++i) acc[i] = 0.0;
-        // U elements per thread per step, every load of the step issued before
-        // the arithmetic: the kernel is bound by loads in flight, not by math.
-        for (int base = threadIdx.x; base < ne; base += blockDim.x * U) {
-            C2 w[U];
-            C2 q[kProjGroup][U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int e = base + u * blockDim.x;
-                w[u] = (e < ne) ? W[e0 + e] : mk2<R>(0, 0);
-            }
-#pragma unroll
-            for (int i = 0; i < kProjGroup; ++i)
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int e = base + u * blockDim.x;
-                    q[i][u] = (i < gn && e < ne) ? Q[(size_t)(g0 + i) * a.qstride + e0 + e]
-                                                 : mk2<R>(0, 0);
-                }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const double wx = (double)w[u].x, wy = (double)w[u].y;
-#pragma unroll
-                for (int i = 0; i < kProjGroup; ++i) {
-                    const double qx = (double)q[i][u].x, qy = (double)q[i][u].y;
-                    acc[2 * i] = fma(qx, wx, fma(qy, wy, acc[2 * i]));
-                    acc[2 * i + 1] = fma(qx, wy, fma(-qy, wx, acc[2 * i + 1]));
-                }
-                if (norm_here) acc[kProjSlots - 1] = fma(wx, wx, fma(wy, wy, acc[kProjSlots - 1]));
-            }
-        }
-        block_sum(acc, gn, norm_here, red_ws, red);
-        if (threadIdx.x < gn) out[g0 + threadIdx.x] = make_double2(red[2 * threadIdx.x], red[2 * threadIdx.x + 1]);
-        if (norm_here && threadIdx.x == 0) out[nvec] = make_double2(red[kProjSlots - 1], 0.0);
-    }
 }
 
 // Last-arriving block of system s sums the system's partials into dst[0..nslot).
@@ -996,10 +908,44 @@ k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
         }
         W[e0 + e] = w;
     }
-    __syncthreads();
+    __syncthreads();            // the block's updated w is visible to all its warps
     }   // cgs2
-    block_project<R, ProjUnroll<R>::p2>(a, Q, nvec, W, e0, ne, 1,
-                                        a.partial + (size_t)blockIdx.x * a.pstride);
+    // Second projection and |w|^2: one warp per basis vector (the last task is
+    // the norm), reading w and Q back from L1/L2.
+    {
+        constexpr int U = 4;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        double2 *out = a.partial + (size_t)blockIdx.x * a.pstride;
+        const C2 *w = W + e0;
+        for (int task = warp; task <= nvec; task += nw) {
+            const C2 *q = Q + (size_t)min(task, nvec - 1) * a.qstride + e0;
+            const bool norm = task == nvec;
+            double sr = 0.0, si = 0.0;
+            for (int base = lane; base < ne; base += 32 * U) {
+                C2 qv[U], wv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int e = base + u * 32;
+                    wv[u] = (e < ne) ? w[e] : mk2<R>(0, 0);
+                    qv[u] = (e < ne && !norm) ? q[e] : mk2<R>(0, 0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const double wx = (double)wv[u].x, wy = (double)wv[u].y;
+                    if (norm) {
+                        sr = fma(wx, wx, fma(wy, wy, sr));
+                    } else {
+                        const double qx = (double)qv[u].x, qy = (double)qv[u].y;
+                        sr = fma(qx, wx, fma(qy, wy, sr));
+                        si = fma(qx, wy, fma(-qy, wx, si));
+                    }
+                }
+            }
+            sr = warp_sum(sr);
+            si = warp_sum(si);
+            if (lane == 0) out[task] = make_double2(sr, norm ? 0.0 : si);
+        }
+    }
     if (last_block_reduce(a, s, nvec + 1, st.h2 + (size_t)s * hs)) {
         if (threadIdx.x == 0) arnoldi_givens(st, s, m, j, rtol, max_iter, inner_rtol, cgs2 != 0);
     }
