@@ -201,7 +201,8 @@ def run_b200(args) -> None:
     nsys = len(systems)
     stream = torch.cuda.current_stream()
     plan = ScatteringPlan(case.v, case.t, systems, rtol=args.rtol, restart=args.restart,
-                          precision=args.precision, inner_restart=args.inner_restart)
+                          precision=args.precision, inner_restart=args.inner_restart,
+                          preconditioner_order=args.precond_order)
     for _ in range(args.warmup):
         res = plan.solve()
     torch.cuda.synchronize()
@@ -587,6 +588,8 @@ def main() -> None:
     ap.add_argument("--restart", type=int, default=30)
     ap.add_argument("--inner-restart", type=int, default=0,
                     help="mixed form: inner FP32 restart (0 = the library default)")
+    ap.add_argument("--precond-order", type=int, default=0,
+                    help="von Neumann order of the preconditioner (0 = block-diagonal)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true",
                     help="only the main timed steps (no secondary rates, no e2e)")

@@ -71,6 +71,10 @@ typedef struct {
                                (Pythagorean norm) in the inner solve instead
                                of two; fewer bytes per iteration, but on
                                ill-conditioned batches more iterations        */
+    int32_t precond_order;  /* von Neumann order k of the preconditioner
+                               M = sum_{i<=k} (-D^-1 V)^i D^-1 (0 = block-diagonal
+                               D^-1; 0..8), the reference's
+                               _scipy_von_neumann.py:40-58                    */
 } msc_plan_desc;
 
 typedef struct msc_plan msc_plan;

@@ -19,6 +19,7 @@ from .api import (
     UnitSystem,
     get_scattering_matrices,
     get_scattering_matrix,
+    get_scattering_matrix_von_neumann,
     momentum_from_angles,
     natural_arrays,
 )
@@ -34,7 +35,8 @@ from .solver import (
 
 __all__ = [
     "OptimizationConfig", "ScatteringCondition", "ScatteringMetadata", "UnitSystem",
-    "get_scattering_matrices", "get_scattering_matrix", "momentum_from_angles", "natural_arrays",
+    "get_scattering_matrices", "get_scattering_matrix", "get_scattering_matrix_von_neumann",
+    "momentum_from_angles", "natural_arrays",
     "ScatteringPlan", "SolveResult", "SystemSpec", "channel_subset_system", "full_grid_system",
     "release_cached_memory", "run_multiscat_fortran",
 ]

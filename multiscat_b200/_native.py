@@ -52,6 +52,7 @@ class PlanDesc(ctypes.Structure):
         ("inner_rtol", ctypes.c_double),
         ("max_refinements", ctypes.c_int32),
         ("flags", ctypes.c_int32),
+        ("precond_order", ctypes.c_int32),
     ]
 
 

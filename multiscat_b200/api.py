@@ -169,12 +169,27 @@ def get_scattering_matrix(condition: ScatteringCondition, config: OptimizationCo
     """|S_G0|^2 on the (nkx, nky) channel grid, complex128 (``_multiscat.py:131-175``)."""
     if backend != "b200":
         raise ValueError(f"Unknown backend '{backend}'. Expected 'b200'.")
+    return _single_solve(condition, config, order=0)
+
+
+def get_scattering_matrix_von_neumann(condition: ScatteringCondition, config: OptimizationConfig,
+                                      *, order: int = 1) -> np.ndarray:
+    """Same result with the von Neumann preconditioner of the given order,
+    sum_{k<=order} (-D^-1 V_scatter)^k D^-1 (``_multiscat.py:179-224``,
+    ``_scipy_von_neumann.py:40-58``); order 0 is the block-diagonal D^-1."""
+    if order < 0:
+        raise ValueError(f"Invalid von Neumann order {order}. Expected a non-negative integer.")
+    return _single_solve(condition, config, order=order)
+
+
+def _single_solve(condition: ScatteringCondition, config: OptimizationConfig, *,
+                  order: int) -> np.ndarray:
     arr = natural_arrays(condition)
     system = _system_for(arr, config)
     plan = ScatteringPlan(arr.potential_values, arr.kinetic, [system],
                           rtol=config.residual_tolerance, restart=config.restart,
                           max_iterations=config.max_iterations,
-                          precision=config.precision_mode)
+                          precision=config.precision_mode, preconditioner_order=order)
     try:
         result = plan.solve(raise_on_error=False)
     finally:

@@ -628,7 +628,14 @@ __global__ void k_cycle_start(GmresState st, int nsys, int m, const double2 *__r
     st.active[s] = 0;
     st.kcyc[s] = 0;
     if (!st.unfinished[s]) return;
-    const double beta = sqrt(fmax(nrm[(size_t)s * nstride].x, 0.0));
+    const double nrm2 = nrm[(size_t)s * nstride].x;
+    if (!isfinite(nrm2)) {              // (fmax would turn a NaN norm into 0)
+        st.resid[s] = nrm2;
+        st.unfinished[s] = 0;
+        st.status[s] = 4;
+        return;
+    }
+    const double beta = sqrt(fmax(nrm2, 0.0));
     if (beta == 0.0) {                  // exact (also: zero right-hand side)
         st.resid[s] = 0.0;
         st.unfinished[s] = 0;
@@ -1125,6 +1132,27 @@ __global__ void k_row_tables(int nrows, int n, int ntaps, int nkx, int nky,
             sy += (sy < 0) ? nky : 0;
             nbr[(size_t)row * ntaps + t] = map[sx * nky + sy];
         }
+    }
+}
+
+// dst = src (add = 0) or dst += src (add = 1) on the rows of the gated tiles.
+template <typename R>
+__global__ void __launch_bounds__(256)
+k_copy_add(Tiles tiles, const int *__restrict__ gate, int n, const typename CT<R>::t *__restrict__ src,
+           typename CT<R>::t *__restrict__ dst, int add)
+{
+    const int tile = blockIdx.x;
+    if (gate && gate[tiles.sys[tile]] == 0) return;
+    const size_t e0 = (size_t)tiles.row0[tile] * n;
+    const int ne = tiles.nrow[tile] * n;
+    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < ne; e += gridDim.y * blockDim.x) {
+        typename CT<R>::t v = src[e0 + e];
+        if (add) {
+            const typename CT<R>::t d = dst[e0 + e];
+            v.x += d.x;
+            v.y += d.y;
+        }
+        dst[e0 + e] = v;
     }
 }
 

@@ -109,6 +109,16 @@ struct DevBuf {
             count = 0;
             return e;
         }
+        // Debugging aid: MSC_POISON_ALLOC=1 fills new buffers with 0xFF bytes
+        // (NaN in FP32 and FP64) so that a read of an unwritten element shows.
+        static const bool poison = [] {
+            const char *v = std::getenv("MSC_POISON_ALLOC");
+            return v && v[0] == '1';
+        }();
+        if (poison) {
+            e = cudaMemsetAsync(p, 0xff, c * sizeof(T), 0);
+            if (e != cudaSuccess) return e;
+        }
         return cudaStreamSynchronize(0);
     }
     void release()
@@ -164,7 +174,8 @@ struct msc_plan {
     double inner_rtol = 0.0;
     int max_cycles = 0;
     DevBuf<float> E32, ET32, lam32, en32, row_pkd32, row_fn32;
-    DevBuf<float2> Vt32, row_c32, Q32, W32, U32;
+    DevBuf<float2> Vt32, row_c32, Q32, W32, U32, T32;
+    DevBuf<double2> T64;            // von Neumann preconditioner term (order > 0)
     DevBuf<double2> R64;
     // tcgen05 block inverse (mixed form)
     bool use_tc = false;
@@ -225,6 +236,7 @@ struct msc_plan {
         sys_counter.release(); work.release(); tap_window.release(); taps_d.release();
         E32.release(); ET32.release(); lam32.release(); en32.release(); row_pkd32.release();
         row_fn32.release(); Vt32.release(); row_c32.release(); Q32.release(); W32.release();
+        T32.release(); T64.release();
         U32.release(); R64.release(); e_img.release(); tc_error.release();
     }
 
@@ -522,6 +534,33 @@ void record_cycle_start(msc_plan *p, cudaStream_t st)
 }
 
 // m Arnoldi steps (CGS2) in precision R and the solution update x += M (Q y).
+// out = M x with the von Neumann preconditioner of order k,
+// M = sum_{i<=k} (-D^-1 V)^i D^-1: term_0 = D^-1 x, term_i = -D^-1 V term_{i-1}.
+// Order 0 is one block inverse.  `scratch` and `term` are work vectors of the
+// plan (the input x is not overwritten unless it is `scratch`, which is read
+// only by the first block inverse).
+template <typename R>
+void apply_precond_t(msc_plan *p, const int *gate, const C2<R> *x, C2<R> *out, C2<R> *scratch,
+                     C2<R> *term, cudaStream_t st)
+{
+    const int k = p->desc.precond_order;
+    if (k <= 0) {
+        launch_block_inverse_t<R>(p, gate, x, out, 0, st);
+        return;
+    }
+    launch_block_inverse_t<R>(p, gate, x, term, 0, st);
+    msc::k_copy_add<R><<<elementwise_grid(p), 256, 0, st>>>(p->tiles(), gate, p->n, term, out, 0);
+    for (int i = 0; i < k; ++i) {
+        launch_coupling_t<R>(p, gate, term, nullptr, R(-1), scratch, st);
+        launch_block_inverse_t<R>(p, gate, scratch, term, 0, st);
+        msc::k_copy_add<R><<<elementwise_grid(p), 256, 0, st>>>(p->tiles(), gate, p->n, term, out, 1);
+    }
+}
+
+template <typename R> C2<R> *precond_term(msc_plan *p);
+template <> C2<float> *precond_term<float>(msc_plan *p) { return p->T32.p; }
+template <> C2<double> *precond_term<double>(msc_plan *p) { return p->T64.p; }
+
 template <typename R>
 void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t st)
 {
@@ -532,10 +571,14 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
         C2<R> *Qj = Q + (size_t)j * vs;
         C2<R> *Qn = Q + (size_t)(j + 1) * vs;
         if (tm) mark(p, 0, j, 0, st);
-        launch_block_inverse_t<R>(p, p->active.p, Qj, U, 0, st);
+        apply_precond_t<R>(p, p->active.p, Qj, U, W, precond_term<R>(p), st);
         if (tm) mark(p, 0, j, 1, st);
         if (tm) mark(p, 1, j, 0, st);
-        launch_coupling_t<R>(p, p->active.p, U, Qj, R(1), W, st);
+        // w = A M q_j.  (D + V) M_k = I + (-1)^k (V D^-1)^{k+1} telescopes, so
+        // w = q_j + V term_k with term_k = (-D^-1 V)^k D^-1 q_j the last term
+        // of the series (for k = 0, term_0 = U = D^-1 q_j).
+        const C2<R> *last = p->desc.precond_order > 0 ? precond_term<R>(p) : U;
+        launch_coupling_t<R>(p, p->active.p, last, Qj, R(1), W, st);
         if (tm) mark(p, 1, j, 1, st);
         const msc::ArnoldiArgs a1 = arnoldi_args(p, p->active.p, true);
         const msc::ArnoldiArgs a2 = arnoldi_args(p, p->active.p, false);
@@ -563,7 +606,13 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
     msc::k_trisolve<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m);
     launch_update_t<R>(p, p->kcyc.p, Q, 0, p->kcyc.p, p->y.p, p->m, nullptr, nullptr, U, 1, st);
     if (tm) mark(p, 0, p->m, 0, st);
-    if (p->mixed) {
+    if (p->desc.precond_order > 0) {
+        // W = M U (U is free after the first block inverse and serves as scratch)
+        apply_precond_t<R>(p, p->kcyc.p, U, W, U, precond_term<R>(p), st);
+        if (!p->mixed)
+            msc::k_copy_add<R><<<elementwise_grid(p), 256, 0, st>>>(
+                p->tiles(), p->kcyc.p, p->n, W, reinterpret_cast<C2<R> *>(p->X.p), 1);
+    } else if (p->mixed) {
         launch_block_inverse_t<R>(p, p->kcyc.p, U, W, 0, st);
     } else {
         launch_block_inverse_t<R>(p, p->kcyc.p, U, reinterpret_cast<C2<R> *>(p->X.p), 1, st);
@@ -1166,9 +1215,11 @@ msc_status finalize(msc_plan *p)
         MSC_CUDA(p->Q32.alloc(vs * (m + 1)));
         MSC_CUDA(p->W32.alloc(vs));
         MSC_CUDA(p->U32.alloc(vs));
+        if (p->desc.precond_order > 0) MSC_CUDA(p->T32.alloc(vs));
     } else {
         MSC_CUDA(p->W.alloc(vs));
         MSC_CUDA(p->U.alloc(vs));
+        if (p->desc.precond_order > 0) MSC_CUDA(p->T64.alloc(vs));
         MSC_CUDA(p->Q.alloc(vs * (m + 1)));
     }
     {
@@ -1304,6 +1355,8 @@ msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc)
         (desc->inner_restart < 0 || desc->inner_restart > msc::kMaxRestart || desc->inner_rtol < 0.0 ||
          desc->max_refinements < 0))
         return fail(MSC_ERR_ARG, "bad mixed-precision options");
+    if (desc->precond_order < 0 || desc->precond_order > 8)
+        return fail(MSC_ERR_ARG, "precond_order must be in 0..8");
     msc_plan *p = new (std::nothrow) msc_plan();
     if (!p) return fail(MSC_ERR_CUDA, "host allocation failed");
     p->desc = *desc;

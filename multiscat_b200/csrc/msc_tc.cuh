@@ -391,11 +391,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                 tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + c0), v);
 #pragma unroll
                 for (int c = 0; c < 16; c += 2) {
+                    // select, not multiply: accumulator rows k >= kp of the last
+                    // M tile come from bytes past E in shared memory and may hold
+                    // NaN, which a zero weight would not remove
                     const int j = (c0 + c) >> 1;
-                    float w = 0.f;
-                    if (valid && j < nrow) w = en_k * __frcp_rn((float)(pkd_s[j] + lam_k));
-                    v[c] *= w;
-                    v[c + 1] *= w;
+                    if (valid && j < nrow) {
+                        const float w = en_k * __frcp_rn((float)(pkd_s[j] + lam_k));
+                        v[c] *= w;
+                        v[c + 1] *= w;
+                    } else {
+                        v[c] = 0.f;
+                        v[c + 1] = 0.f;
+                    }
                 }
                 const float sum = warp_reduce_scatter16(v, lane);
                 if ((lane & 1) == 0) sm_part[warp][m][c0 + ((lane >> 1) & 15)] = sum;

@@ -98,7 +98,7 @@ class ScatteringPlan:
                  rtol: float = 1e-10, restart: int = 30, max_iterations: int = 2000,
                  precision: str = "fp64", inner_rtol: float = 0.0, inner_restart: int = 0,
                  max_refinements: int = 0, tensor_cores: bool | None = None,
-                 inner_gram_schmidt_passes: int = 2):
+                 inner_gram_schmidt_passes: int = 2, preconditioner_order: int = 0):
         self._lib = nat.load()
         v = np.ascontiguousarray(np.asarray(potential_values), dtype=np.complex128)
         nkx, nky, nz = v.shape
@@ -124,6 +124,8 @@ class ScatteringPlan:
             raise ValueError("inner_gram_schmidt_passes must be 1 or 2")
         if inner_gram_schmidt_passes == 1:
             desc.flags |= 4
+        # von Neumann order k: M = sum_{i<=k} (-D^-1 V)^i D^-1 (0 = block-diagonal D^-1)
+        desc.precond_order = int(preconditioner_order)
         self._plan = ctypes.c_void_p()
         nat.check("msc_plan_create", self._lib.msc_plan_create(ctypes.byref(self._plan),
                                                               ctypes.byref(desc)))

@@ -367,3 +367,77 @@ def test_every_coupling_kernel_agrees(kind, monkeypatch):
     assert float((yk - y0).abs().max()) <= 1e-13 * float(y0.abs().max())
     pk.close()
     p0.close()
+
+
+# ---------------------------------------------------------------------------
+# von Neumann preconditioner of order k (the reference's
+# _scipy_von_neumann.py; its tests ask orders 0-2 to agree with the scipy
+# solve at 1e-5, tests/test_fixed_example.py:387-408).  Here: the API at
+# orders 0-2 against the He-LiF golden file, and orders 1-2 of the plan
+# against order 0 on a batch, in both precisions.
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_von_neumann_api_reproduces_reference_golden(order):
+    from multiscat_b200 import get_scattering_matrix_von_neumann
+    s = get_scattering_matrix_von_neumann(_wolken_condition(0.0),
+                                          OptimizationConfig(precision=1e-5, max_iterations=1000),
+                                          order=order)
+    inten = np.real_if_close(s)
+    assert math.isclose(float(np.sum(inten).real), 1.0, abs_tol=1e-6)
+    np.testing.assert_allclose(inten.real, _read_wolken_golden(), rtol=0.0, atol=1e-5)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_von_neumann_orders_agree_on_a_batch(precision):
+    case, systems = cfg2_batch(n_solves=6, seed=7)
+    res, iters = {}, {}
+    for order in (0, 1, 2):
+        plan = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision=precision,
+                              preconditioner_order=order)
+        r = plan.solve()
+        assert (r.status == 0).all()
+        res[order] = r.intensities
+        iters[order] = int(r.iterations.sum())
+        plan.close()
+    tol = 1e-8 if precision == "fp64" else MIXED_TOL
+    for order in (1, 2):
+        assert float((res[order] - res[0]).abs().max()) <= tol
+    assert iters[1] < iters[0] and iters[2] < iters[1], iters
+
+
+def test_von_neumann_order_is_validated(cfg0):
+    with pytest.raises(Exception):
+        ScatteringPlan(cfg0.v, cfg0.t, [cfg0.system()], preconditioner_order=9)
+
+
+POISON_SCRIPT = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+from multiscat_b200 import ScatteringPlan
+from multiscat_b200.workloads import cfg2_batch
+case, systems = cfg2_batch(n_solves=6, seed=7)
+ref = ScatteringPlan(case.v, case.t, systems, rtol=1e-10).solve().intensities
+worst = 0.0
+for tc in (True, False):
+    for order in (0, 1):
+        r = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed",
+                           tensor_cores=tc, preconditioner_order=order).solve()
+        assert (r.status == 0).all(), (tc, order, r.status)
+        worst = max(worst, float((r.intensities - ref).abs().max()))
+print(worst)
+"""
+
+
+def test_no_kernel_reads_unwritten_memory():
+    """Every plan buffer starts as NaN bytes (MSC_POISON_ALLOC=1, read once per
+    process, hence the subprocess): mixed solves on tensor cores and SIMT, with
+    and without the von Neumann preconditioner, still match FP64."""
+    import os
+    import subprocess
+    import sys
+    root = str(pathlib.Path(__file__).resolve().parents[1])
+    env = dict(os.environ, MSC_POISON_ALLOC="1")
+    out = subprocess.run([sys.executable, "-c", POISON_SCRIPT, root], env=env,
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert float(out.stdout.strip().splitlines()[-1]) <= MIXED_TOL
