@@ -132,6 +132,14 @@ msc_status msc_plan_set_system(msc_plan *plan, int32_t s, int32_t n_channels,
 msc_status msc_solve(msc_plan *plan, double *psi_out, double *intensities_out,
                      msc_result *results, void *stream);
 
+/* Warm start: psi0 complex [total_rows][n_z] (plan row order) becomes the
+ * initial guess of every following msc_solve (the reference's x0,
+ * _gmres.py:106-108), e.g. the solution of a neighbouring beam in a sweep.
+ * on_device != 0: device pointer read in order on `stream`; psi0 = NULL
+ * returns to the zero guess.  The stop rule is unchanged (relative to ||u||). */
+msc_status msc_plan_set_initial_guess(msc_plan *plan, const double *psi0, int32_t on_device,
+                                      void *stream);
+
 /* Total channel rows of the plan (sum of C_s) once all systems are set. */
 int64_t msc_plan_total_rows(const msc_plan *plan);
 

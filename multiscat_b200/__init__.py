@@ -19,7 +19,9 @@ from .api import (
     UnitSystem,
     get_scattering_matrices,
     get_scattering_matrix,
+    get_scattering_matrix_from_state,
     get_scattering_matrix_von_neumann,
+    get_scattering_state,
     momentum_from_angles,
     natural_arrays,
 )
@@ -36,6 +38,7 @@ from .solver import (
 __all__ = [
     "OptimizationConfig", "ScatteringCondition", "ScatteringMetadata", "UnitSystem",
     "get_scattering_matrices", "get_scattering_matrix", "get_scattering_matrix_von_neumann",
+    "get_scattering_state", "get_scattering_matrix_from_state",
     "momentum_from_angles", "natural_arrays",
     "ScatteringPlan", "SolveResult", "SystemSpec", "channel_subset_system", "full_grid_system",
     "release_cached_memory", "run_multiscat_fortran",

@@ -22,7 +22,7 @@ EXPORTED = (
     "msc_plan_kernel_timing", "msc_apply_operator_noalloc", "msc_debug_apply_block_inverse_f32",
     "msc_plan_uses_tensor_cores", "msc_plan_tuning_report", "msc_plan_set_adjoint",
     "msc_plan_is_adjoint", "msc_plan_set_boundary_rhs", "msc_plan_set_adjoint_rhs",
-    "msc_potential_gradient", "msc_release_cached_memory",
+    "msc_potential_gradient", "msc_release_cached_memory", "msc_plan_set_initial_guess",
 )
 
 MSC_OK = 0
@@ -146,6 +146,8 @@ def load() -> ctypes.CDLL:
     lib.msc_plan_set_adjoint_rhs.argtypes = [_vp, _vp, _vp, _vp, _vp]
     lib.msc_potential_gradient.restype = ctypes.c_int
     lib.msc_potential_gradient.argtypes = [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp]
+    lib.msc_plan_set_initial_guess.restype = ctypes.c_int
+    lib.msc_plan_set_initial_guess.argtypes = [_vp, _vp, ctypes.c_int32, _vp]
     lib.msc_release_cached_memory.restype = ctypes.c_int
     lib.msc_release_cached_memory.argtypes = []
     lib.msc_last_error.restype = ctypes.c_char_p

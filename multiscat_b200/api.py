@@ -201,6 +201,52 @@ def _single_solve(condition: ScatteringCondition, config: OptimizationConfig, *,
     return _to_grid(result, 0, system, condition.metadata.shape[:2])
 
 
+def get_scattering_state(condition: ScatteringCondition, config: OptimizationConfig, *,
+                         initial_state: np.ndarray | None = None) -> np.ndarray:
+    """The full interior state psi_G(z_k), complex128 (nkx, nky, nz)
+    (``_multiscat.py:227-246``); channels outside an ``n_channels`` set are 0.
+
+    ``initial_state`` (same shape) warm-starts the solve, e.g. with the state of
+    a neighbouring energy or angle (the reference's ``x0``, ``_gmres.py:106-108``).
+    Convention: this returns psi itself.  The reference's state is L psi, its
+    Gauss-Seidel lower block applied to psi (``_gmres.py:127``), because its
+    solver works in that variable; the intensities that both states lead to
+    are the same."""
+    arr = natural_arrays(condition)
+    system = _system_for(arr, config)
+    nkx, nky, nz = arr.potential_values.shape
+    plan = ScatteringPlan(arr.potential_values, arr.kinetic, [system],
+                          rtol=config.residual_tolerance, restart=config.restart,
+                          max_iterations=config.max_iterations, precision=config.precision_mode)
+    try:
+        if initial_state is not None:
+            guess = np.asarray(initial_state, np.complex128).reshape(nkx, nky, nz)
+            plan.set_initial_guess(guess[system.channel_ix, system.channel_iy])
+        result = plan.solve(raise_on_error=False)
+    finally:
+        plan.close()
+    if result.status[0] != 0:
+        raise RuntimeError(f"B200 GMRES did not converge (status={result.status[0]})")
+    out = np.zeros((nkx, nky, nz), np.complex128)
+    out[system.channel_ix, system.channel_iy] = result.system_psi(0).cpu().numpy()
+    return out
+
+
+def get_scattering_matrix_from_state(state: np.ndarray,
+                                     condition: ScatteringCondition) -> np.ndarray:
+    """|S_G0|^2 on the channel grid from a state of ``get_scattering_state``
+    (``_multiscat.py:63-99``; S_G = 2i b_G psi_G(z_n) + delta_G0 a_0,
+    ``_multiscat.py:40-60``)."""
+    arr = natural_arrays(condition)
+    nkx, nky, nz = arr.potential_values.shape
+    psi_n = np.asarray(state, np.complex128).reshape(nkx, nky, nz)[:, :, -1]
+    b = np.asarray(arr.wave_b, np.complex128).reshape(nkx, nky)
+    a = np.asarray(arr.wave_a, np.complex128).reshape(nkx, nky)
+    s = 2.0j * b * psi_n
+    s[0, 0] += a[0, 0]
+    return (np.abs(s) ** 2).astype(np.complex128)
+
+
 def get_scattering_matrices(conditions: Sequence[ScatteringCondition],
                             config: OptimizationConfig) -> list[np.ndarray]:
     """Batched sweep: many beams over ONE potential and grid, one GPU solve."""

@@ -176,6 +176,8 @@ struct msc_plan {
     DevBuf<float> E32, ET32, lam32, en32, row_pkd32, row_fn32;
     DevBuf<float2> Vt32, row_c32, Q32, W32, U32, T32;
     DevBuf<double2> T64;            // von Neumann preconditioner term (order > 0)
+    DevBuf<double2> X0;             // initial guess of the next solve (warm start)
+    bool has_x0 = false;
     DevBuf<double2> R64;
     // tcgen05 block inverse (mixed form)
     bool use_tc = false;
@@ -236,7 +238,7 @@ struct msc_plan {
         sys_counter.release(); work.release(); tap_window.release(); taps_d.release();
         E32.release(); ET32.release(); lam32.release(); en32.release(); row_pkd32.release();
         row_fn32.release(); Vt32.release(); row_c32.release(); Q32.release(); W32.release();
-        T32.release(); T64.release();
+        T32.release(); T64.release(); X0.release();
         U32.release(); R64.release(); e_img.release(); tc_error.release();
     }
 
@@ -1552,9 +1554,12 @@ msc_status msc_solve(msc_plan *p, double *psi_out, double *intensities_out, msc_
     MSC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     MSC_CUDA(cudaEventRecord(ev, user));
     MSC_CUDA(cudaStreamWaitEvent(ps, ev, 0));
-    // reset state
+    // reset state (x = the warm-start guess when one is set, else 0)
     const size_t vs = (size_t)p->R * p->n;
-    MSC_CUDA(cudaMemsetAsync(p->X.p, 0, vs * sizeof(double2), ps));
+    if (p->has_x0)
+        MSC_CUDA(cudaMemcpyAsync(p->X.p, p->X0.p, vs * sizeof(double2), cudaMemcpyDeviceToDevice, ps));
+    else
+        MSC_CUDA(cudaMemsetAsync(p->X.p, 0, vs * sizeof(double2), ps));
     MSC_CUDA(cudaMemsetAsync(p->iters.p, 0, p->B * sizeof(int), ps));
     MSC_CUDA(cudaMemsetAsync(p->cycles.p, 0, p->B * sizeof(int), ps));
     MSC_CUDA(cudaMemsetAsync(p->status.p, 0, p->B * sizeof(int), ps));
@@ -1747,6 +1752,25 @@ int msc_plan_uses_tensor_cores(const msc_plan *p) { return (p && p->use_tc) ? p-
 // Adjoint solves and the potential gradient (no counterpart in the reference;
 // the operator they transpose is the one of multiscat_gmres.f90:452-687).
 // ---------------------------------------------------------------------------
+msc_status msc_plan_set_initial_guess(msc_plan *p, const double *psi0, int32_t on_device, void *stream)
+{
+    if (!p) return fail(MSC_ERR_ARG, "null plan");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    if (!psi0) {
+        p->has_x0 = false;
+        return MSC_OK;
+    }
+    const size_t vs = (size_t)p->R * p->n;
+    if (!p->X0.p) MSC_CUDA(p->X0.alloc(vs));
+    cudaStream_t us = reinterpret_cast<cudaStream_t>(stream);
+    MSC_CUDA(cudaMemcpyAsync(p->X0.p, psi0, vs * sizeof(double2),
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, us));
+    if (!on_device) MSC_CUDA(cudaStreamSynchronize(us));
+    p->has_x0 = true;
+    return MSC_OK;
+}
+
 msc_status msc_plan_set_adjoint(msc_plan *p, int32_t adjoint)
 {
     if (!p) return fail(MSC_ERR_ARG, "null plan");

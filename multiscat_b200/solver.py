@@ -159,6 +159,22 @@ class ScatteringPlan:
         except Exception:
             pass
 
+    def set_initial_guess(self, psi0: torch.Tensor | None) -> None:
+        """Warm start for the following solves: psi0 complex128 [total_rows, nz]
+        (plan row order), or None for the zero guess."""
+        stream = torch.cuda.current_stream().cuda_stream
+        if psi0 is None:
+            st = self._lib.msc_plan_set_initial_guess(self._plan, None, 0, ctypes.c_void_p(stream))
+        else:
+            dev = torch.device("cuda", torch.cuda.current_device())
+            psi0 = torch.as_tensor(psi0).to(device=dev, dtype=torch.complex128).contiguous()
+            if psi0.shape != (self.total_rows, self.nz):
+                raise ValueError(f"expected [{self.total_rows}, {self.nz}], got {tuple(psi0.shape)}")
+            self._x0_keepalive = psi0
+            st = self._lib.msc_plan_set_initial_guess(self._plan, ctypes.c_void_p(psi0.data_ptr()), 1,
+                                                      ctypes.c_void_p(stream))
+        nat.check("msc_plan_set_initial_guess", st)
+
     def solve(self, *, raise_on_error: bool = True) -> SolveResult:
         dev = torch.device("cuda", torch.cuda.current_device())
         psi = torch.empty((self.total_rows, self.nz), dtype=torch.complex128, device=dev)

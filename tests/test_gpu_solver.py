@@ -441,3 +441,44 @@ def test_no_kernel_reads_unwritten_memory():
                          capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     assert float(out.stdout.strip().splitlines()[-1]) <= MIXED_TOL
+
+
+# ---------------------------------------------------------------------------
+# Full-state API and warm start (the reference's get_scattering_state /
+# get_scattering_matrix_from_state, _multiscat.py:63-99, 227-246, and x0).
+# ---------------------------------------------------------------------------
+def test_state_api_round_trip_matches_scattering_matrix():
+    from multiscat_b200 import get_scattering_matrix_from_state, get_scattering_state
+    cond = _wolken_condition(0.0)
+    cfg = OptimizationConfig(precision=1e-7, max_iterations=1000)
+    state = get_scattering_state(cond, cfg)
+    assert state.shape == (10, 10, 550) and state.dtype == np.complex128
+    s_state = get_scattering_matrix_from_state(state, cond)
+    s_direct = get_scattering_matrix(cond, cfg)
+    np.testing.assert_allclose(s_state.real, s_direct.real, rtol=0.0, atol=1e-12)
+    np.testing.assert_allclose(s_state.real, _read_wolken_golden(), rtol=0.0, atol=1e-5)
+    # warm start from the converged state: already below the tolerance
+    again = get_scattering_state(cond, cfg, initial_state=state)
+    np.testing.assert_allclose(again, state, rtol=0.0, atol=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_warm_start_from_a_neighbouring_beam(precision):
+    """Beams 0 and 1 of a seeded batch differ; warm-starting beam 0's plan from
+    its own solution needs no iterations, and the answer does not depend on
+    the guess."""
+    case, systems = cfg2_batch(n_solves=2, seed=11)
+    plan = ScatteringPlan(case.v, case.t, [systems[0]], rtol=1e-10, precision=precision)
+    cold = plan.solve()
+    plan.set_initial_guess(cold.psi)
+    warm = plan.solve()
+    assert warm.iterations[0] == 0 and warm.status[0] == 0
+    assert float((warm.intensities - cold.intensities).abs().max()) <= 1e-12
+    # a poor guess (a random state) still converges to the same answer
+    plan.set_initial_guess(torch.randn_like(cold.psi))
+    noisy = plan.solve()
+    tol = 1e-8 if precision == "fp64" else MIXED_TOL
+    assert float((noisy.intensities - cold.intensities).abs().max()) <= tol
+    plan.set_initial_guess(None)
+    assert plan.solve().iterations[0] == cold.iterations[0]
+    plan.close()
