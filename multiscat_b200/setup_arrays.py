@@ -208,3 +208,54 @@ def hexagonal_xi(a1, a2, h):
         return (h / 3.0) * (torch.cos(b1[0] * x + b1[1] * y) + torch.cos(b2[0] * x + b2[1] * y) +
                             torch.cos(b3[0] * x + b3[1] * y))
     return fn
+
+
+def interpolate_potential(values, z_grid, nodes, nkx: int, nky: int, *, device=None) -> torch.Tensor:
+    """Potential samples on an evenly spaced (x, y, z) grid -> V_G(z_k) on the
+    channel grid at the Lobatto nodes (``interpolate.py:38-116``).
+
+    values   [nx, ny, nz_grid] real or complex samples V(x_i, y_j, z_l) over
+             one unit cell (fractional coordinates i/nx, j/ny);
+    z_grid   [nz_grid] increasing sample heights; nodes [n] target heights.
+
+    The parallel directions go to momentum space (fft2 / (nx ny), the
+    solver's convention) and the modes are placed in FFT order on the
+    nkx x nky grid (modes beyond the sample grid's Nyquist range are zero;
+    modes beyond the channel grid are dropped).  Along z each V_G is linearly
+    interpolated with the end values held outside the sampled range
+    (``np.interp`` behaviour).  The result holds plain values V_G(z_k), the
+    solver's ``potential_values`` (the reference multiplies by the Lobatto
+    weights only because it stores an operator in a weighted basis).
+    """
+    dev = device if device is not None else (values.device if torch.is_tensor(values) else "cpu")
+    v = torch.as_tensor(values, device=dev)
+    v = v.to(torch.complex128) if not torch.is_complex(v) else v.to(torch.complex128)
+    nx, ny, ng = v.shape
+    zg = torch.as_tensor(np.asarray(z_grid, float) if not torch.is_tensor(z_grid) else z_grid,
+                         dtype=torch.float64, device=dev)
+    zn = torch.as_tensor(np.asarray(nodes, float) if not torch.is_tensor(nodes) else nodes,
+                         dtype=torch.float64, device=dev)
+    if zg.numel() != ng or ng < 2 or bool((zg[1:] <= zg[:-1]).any()):
+        raise ValueError("z_grid must be increasing and match the last axis of values")
+    coef = torch.fft.fft2(v, dim=(0, 1)) / (nx * ny)                    # [nx, ny, ng]
+
+    def mode_map(nk: int, ns: int):
+        # FFT-order index on the channel grid -> index on the sample grid (or -1);
+        # both grids use numpy's FFT mode order (0, 1, ..., -1)
+        m = fft_modes(nk)
+        ok = (m <= (ns - 1) // 2) & (m >= -(ns // 2))
+        return np.where(ok, np.mod(m, ns), -1)
+
+    mx, my = mode_map(nkx, nx), mode_map(nky, ny)
+    out_modes = torch.zeros((nkx, nky, ng), dtype=torch.complex128, device=dev)
+    ix = torch.as_tensor(np.nonzero(mx >= 0)[0], device=dev)
+    iy = torch.as_tensor(np.nonzero(my >= 0)[0], device=dev)
+    sx = torch.as_tensor(mx[mx >= 0], device=dev)
+    sy = torch.as_tensor(my[my >= 0], device=dev)
+    out_modes[ix[:, None], iy[None, :]] = coef[sx[:, None], sy[None, :]]
+    # linear interpolation along z, clamped at the ends
+    zc = zn.clamp(zg[0], zg[-1])
+    hi = torch.searchsorted(zg, zc).clamp(1, ng - 1)
+    lo = hi - 1
+    t = ((zc - zg[lo]) / (zg[hi] - zg[lo])).to(torch.complex128)
+    return out_modes[:, :, lo] * (1 - t) + out_modes[:, :, hi] * t

@@ -482,3 +482,26 @@ def test_warm_start_from_a_neighbouring_beam(precision):
     plan.set_initial_guess(None)
     assert plan.solve().iterations[0] == cold.iterations[0]
     plan.close()
+
+
+def test_interpolated_potential_on_device_gives_the_same_intensities():
+    """A sampled potential interpolated on the GPU (interpolate_potential, the
+    reference's interpolate.py) scatters like the analytic components."""
+    case = cfg0_case()
+    a = 2.54
+    zg = torch.linspace(-1.5, 10.0, 4000, dtype=torch.float64, device="cuda")
+    f = torch.arange(64, dtype=torch.float64, device="cuda") / 64
+    fx, fy = torch.meshgrid(f, f, indexing="ij")
+    xiv = sa.square_xi(a, 0.1)(fx * a, fy * a)
+    factor = sa.natural_units_factor(sa.HE4_MASS)
+    samples = factor * 7.63 * (torch.exp(-2.2 * (zg[None, None, :] - xiv[:, :, None]))
+                               - 2.0 * torch.exp(-1.1 * zg)[None, None, :])
+    v = sa.interpolate_potential(samples, zg, case.nodes, 11, 11)
+    assert v.is_cuda
+    keep = torch.zeros(11, 11, dtype=torch.bool)
+    idx = [i for i, m in enumerate(sa.fft_modes(11)) if abs(m) <= 4]
+    keep[np.ix_(idx, idx)] = True
+    v = v * keep.to(v.device)[:, :, None]        # the |m|,|n| <= 4 modes of the workload
+    r_int = ScatteringPlan(v.cpu().numpy(), case.t, [case.system()], rtol=1e-12).solve()
+    r_dir = ScatteringPlan(case.v, case.t, [case.system()], rtol=1e-12).solve()
+    assert float((r_int.intensities - r_dir.intensities).abs().max()) <= 1e-4
