@@ -540,20 +540,37 @@ k_update(Tiles tiles, const int *__restrict__ gate, int n, const typename CT<R>:
     const size_t e0 = (size_t)tiles.row0[tile] * n;
     const int ne = tiles.nrow[tile] * n;
     const R sc = scale ? (R)scale[sys] : R(1);
-    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < ne; e += gridDim.y * blockDim.x) {
-        C2 acc = (W && !sum_only) ? W[e0 + e] : mk2<R>(0, 0);
-        for (int i = 0; i < nv; ++i) {
-            const C2 q = Q[(size_t)i * qstride + e0 + e];
-            const C2 c = cf[i];
-            if (sum_only) {
-                acc.x = fma(q.x, c.x, acc.x); acc.x = fma(-q.y, c.y, acc.x);
-                acc.y = fma(q.x, c.y, acc.y); acc.y = fma(q.y, c.x, acc.y);
-            } else {
-                acc.x = fma(-q.x, c.x, acc.x); acc.x = fma(q.y, c.y, acc.x);
-                acc.y = fma(-q.x, c.y, acc.y); acc.y = fma(-q.y, c.x, acc.y);
-            }
+    const R sg = sum_only ? R(1) : R(-1);     // dst = sc (W - Q c)  or  sc (Q c)
+    // Two consecutive elements per step: one 16-byte load per basis vector for
+    // FP32 when the row chunk starts on an even element (n even).
+    const bool pairs = std::is_same<R, float>::value && (e0 % 2 == 0);
+    const int step = pairs ? 2 : 1;
+    for (int e = (blockIdx.y * blockDim.x + threadIdx.x) * step; e < ne;
+         e += gridDim.y * blockDim.x * step) {
+        const bool two = pairs && e + 1 < ne;
+        C2 a0 = mk2<R>(0, 0), a1 = mk2<R>(0, 0);
+        if (W && !sum_only) {
+            a0 = W[e0 + e];
+            if (two) a1 = W[e0 + e + 1];
         }
-        dst[e0 + e] = mk2<R>(acc.x * sc, acc.y * sc);
+        for (int i = 0; i < nv; ++i) {
+            const C2 *qp = Q + (size_t)i * qstride + e0 + e;
+            C2 q0, q1 = mk2<R>(0, 0);
+            if (two) {
+                const float4 v = *reinterpret_cast<const float4 *>(qp);
+                q0 = mk2<R>((R)v.x, (R)v.y);
+                q1 = mk2<R>((R)v.z, (R)v.w);
+            } else {
+                q0 = *qp;
+            }
+            const C2 c = cf[i];
+            a0.x = fma(sg * q0.x, c.x, a0.x); a0.x = fma(-sg * q0.y, c.y, a0.x);
+            a0.y = fma(sg * q0.x, c.y, a0.y); a0.y = fma(sg * q0.y, c.x, a0.y);
+            a1.x = fma(sg * q1.x, c.x, a1.x); a1.x = fma(-sg * q1.y, c.y, a1.x);
+            a1.y = fma(sg * q1.x, c.y, a1.y); a1.y = fma(sg * q1.y, c.x, a1.y);
+        }
+        dst[e0 + e] = mk2<R>(a0.x * sc, a0.y * sc);
+        if (two) dst[e0 + e + 1] = mk2<R>(a1.x * sc, a1.y * sc);
     }
 }
 

@@ -468,9 +468,10 @@ void launch_update_t(msc_plan *p, const int *gate, const C2<R> *Q, int nvec, con
                      const double2 *coef, int cstride, const C2<R> *W, const double *scale,
                      C2<R> *dst, int sum_only, cudaStream_t st)
 {
-    msc::k_update<R><<<elementwise_grid(p), 256, 0, st>>>(p->tiles(), gate, p->n, Q,
-                                                           (size_t)p->R * p->n, nvec, nvec_sys,
-                                                           coef, cstride, W, scale, dst, sum_only);
+    // one block per row chunk of one system (~4096 elements)
+    msc::k_update<R><<<dim3(p->nchunks, 1), 256, 0, st>>>(p->chunks(), gate, p->n, Q,
+                                                          (size_t)p->R * p->n, nvec, nvec_sys,
+                                                          coef, cstride, W, scale, dst, sum_only);
 }
 
 void launch_update(msc_plan *p, const int *gate, int nvec, const int *nvec_sys,
