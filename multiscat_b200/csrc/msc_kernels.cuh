@@ -922,15 +922,31 @@ k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
         cf[i] = mk2<R>((R)c.x, (R)c.y);
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        C2 w = W[e0 + e];
+    // w <- w - Q h1, two consecutive elements per step (one 16-byte load per
+    // basis vector for FP32 when the range starts on an even element)
+    const bool pairs = std::is_same<R, float>::value && (e0 % 2 == 0);
+    const int step = pairs ? 2 : 1;
+    for (int e = threadIdx.x * step; e < ne; e += blockDim.x * step) {
+        const bool two = pairs && e + 1 < ne;
+        C2 w0 = W[e0 + e], w1 = two ? W[e0 + e + 1] : mk2<R>(0, 0);
         for (int i = 0; i < nvec; ++i) {
-            const C2 q = Q[(size_t)i * a.qstride + e0 + e];
+            const C2 *qp = Q + (size_t)i * a.qstride + e0 + e;
+            C2 q0, q1 = mk2<R>(0, 0);
+            if (two) {
+                const float4 v = *reinterpret_cast<const float4 *>(qp);
+                q0 = mk2<R>((R)v.x, (R)v.y);
+                q1 = mk2<R>((R)v.z, (R)v.w);
+            } else {
+                q0 = *qp;
+            }
             const C2 c = cf[i];
-            w.x = fma(-q.x, c.x, fma(q.y, c.y, w.x));
-            w.y = fma(-q.x, c.y, fma(-q.y, c.x, w.y));
+            w0.x = fma(-q0.x, c.x, fma(q0.y, c.y, w0.x));
+            w0.y = fma(-q0.x, c.y, fma(-q0.y, c.x, w0.y));
+            w1.x = fma(-q1.x, c.x, fma(q1.y, c.y, w1.x));
+            w1.y = fma(-q1.x, c.y, fma(-q1.y, c.x, w1.y));
         }
-        W[e0 + e] = w;
+        W[e0 + e] = w0;
+        if (two) W[e0 + e + 1] = w1;
     }
     __syncthreads();            // the block's updated w is visible to all its warps
     }   // cgs2
