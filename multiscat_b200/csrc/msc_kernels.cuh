@@ -385,22 +385,47 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
     __syncthreads();
     constexpr int kU = 8;
     const int total = npos * ZC;
-    for (int base = threadIdx.x; base < total; base += NT * kU) {
-        C2 v[kU];
+    if (std::is_same<R, float>::value && (n % 2) == 0) {
+        // FP32, n even: two consecutive z per 16-byte load (z0 and ZC are even)
+        const int total2 = total / 2;
+        float4 *halo4 = reinterpret_cast<float4 *>(halo);
+        for (int base = threadIdx.x; base < total2; base += NT * kU) {
+            float4 v[kU];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int idx = base + u * NT;
-            v[u] = mk2<R>(0, 0);
-            if (idx < total) {
-                const int row = rows[idx / ZC];
-                const int z = z0 + (idx % ZC);
-                if (row >= 0 && z < n) v[u] = src[(size_t)row * n + z];
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (idx < total2) {
+                    const int row = rows[(2 * idx) / ZC];
+                    const int z = z0 + ((2 * idx) % ZC);
+                    if (row >= 0 && z < n)    // z < n implies z + 1 < n (both even)
+                        v[u] = *reinterpret_cast<const float4 *>(src + (size_t)row * n + z);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                if (idx < total2) halo4[idx] = v[u];
             }
         }
+    } else {
+        for (int base = threadIdx.x; base < total; base += NT * kU) {
+            C2 v[kU];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int idx = base + u * NT;
-            if (idx < total) halo[idx] = v[u];
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                v[u] = mk2<R>(0, 0);
+                if (idx < total) {
+                    const int row = rows[idx / ZC];
+                    const int z = z0 + (idx % ZC);
+                    if (row >= 0 && z < n) v[u] = src[(size_t)row * n + z];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                if (idx < total) halo[idx] = v[u];
+            }
         }
     }
     __syncthreads();
