@@ -94,6 +94,14 @@ __device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint3
         : "memory");
 }
 
+__device__ __forceinline__ void cp_async_16(void *smem_dst, const void *gsrc)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void fence_proxy_async()
 {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -292,50 +300,104 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     const int ksteps = kp >> 4;
     const int sj = tid % TR, sp = tid / TR;               // staging: channel, z-block phase
 
-    for (int tile = blockIdx.x; tile < prm.ntiles && ok; tile += gridDim.x) {
+    // Staging units: thread (channel sj, z-blocks sp, sp + P, ...) handles 8
+    // consecutive z (64 contiguous bytes of x) and writes four 16-byte units
+    // (re/im x hi/lo) of the K-major B operand of GEMM 1.
+    auto write_unit = [&](int zb, const float2 (&v)[8]) {
+        uint32_t rh[4], ih[4], rl[4], il[4];
+#pragma unroll
+        for (int u = 0; u < 8; u += 2) {
+            const __nv_bfloat162 hr = __floats2bfloat162_rn(v[u].x, v[u + 1].x);
+            const __nv_bfloat162 hi = __floats2bfloat162_rn(v[u].y, v[u + 1].y);
+            const float2 fr = __bfloat1622float2(hr), fi = __bfloat1622float2(hi);
+            const __nv_bfloat162 lr = __floats2bfloat162_rn(v[u].x - fr.x, v[u + 1].x - fr.y);
+            const __nv_bfloat162 li = __floats2bfloat162_rn(v[u].y - fi.x, v[u + 1].y - fi.y);
+            rh[u >> 1] = *reinterpret_cast<const uint32_t *>(&hr);
+            ih[u >> 1] = *reinterpret_cast<const uint32_t *>(&hi);
+            rl[u >> 1] = *reinterpret_cast<const uint32_t *>(&lr);
+            il[u >> 1] = *reinterpret_cast<const uint32_t *>(&li);
+        }
+        const uint32_t o_re = kmaj_off(2 * sj, zb * 8, N), o_im = o_re + 16;
+        *reinterpret_cast<uint4 *>(b_hi + o_re) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+        *reinterpret_cast<uint4 *>(b_hi + o_im) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+        *reinterpret_cast<uint4 *>(b_lo + o_re) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+        *reinterpret_cast<uint4 *>(b_lo + o_im) = make_uint4(il[0], il[1], il[2], il[3]);
+    };
+    // Prefetch: once the second GEMM has consumed the B buffer, the next
+    // tile's raw x rows ([TR][n] complex FP32 = 8 TR n bytes, within the B
+    // buffer's 4 N kp = 8 TR kp bytes) are copied into it with cp.async while
+    // the current tile is stored; the next staging converts them from shared
+    // memory.  Needs 16-byte aligned rows (n even) and at most kMaxPf units
+    // per thread held in registers (raw and converted data share the buffer).
+    constexpr int kMaxPf = 5;
+    const int upt = (kb + P - 1) / P;
+    const bool use_pf = (n % 2 == 0) && upt <= kMaxPf;
+    float2 *raw = reinterpret_cast<float2 *>(b_hi);
+    auto prefetch = [&](int t) {
+        const int r0 = t * TR, nr = min(TR, prm.rows - r0), half = n >> 1;
+        for (int idx = tid; idx < nr * half; idx += kThreads) {
+            const int j = idx / half, q = idx - j * half;
+            cp_async_16(raw + (size_t)j * n + 2 * q, prm.x + (size_t)(r0 + j) * n + 2 * q);
+        }
+        cp_async_commit_group();
+    };
+    // first active tile of this CTA at or after t (stride gridDim.x); thread 0
+    auto find_active = [&](int t) {
+        for (; t < prm.ntiles; t += gridDim.x) {
+            if (!prm.gate) return t;
+            const int r0 = t * TR, nr = min(TR, prm.rows - r0);
+            const int s0 = prm.row_sys[r0], s1 = prm.row_sys[r0 + nr - 1];
+            for (int q = s0; q <= s1; ++q)
+                if (prm.gate[q]) return t;
+        }
+        return prm.ntiles;
+    };
+    __shared__ int next_s;
+    if (tid == 0) next_s = find_active(blockIdx.x);
+    __syncthreads();
+    int tile = next_s;
+    if (use_pf && tile < prm.ntiles) prefetch(tile);
+
+    while (tile < prm.ntiles && ok) {
         const int row0 = tile * TR;
         const int nrow = min(TR, prm.rows - row0);
-        int any = 1;
-        if (tid == 0 && prm.gate) {
-            any = 0;
-            const int s0 = prm.row_sys[row0], s1 = prm.row_sys[row0 + nrow - 1];
-            for (int s = s0; s <= s1 && !any; ++s) any = prm.gate[s] != 0;
-        }
         for (int j = tid; j < TR; j += kThreads) pkd_s[j] = (j < nrow) ? prm.row_pkd[row0 + j] : 0.0;
-        if (!__syncthreads_or(tid == 0 ? any : 0)) continue;
 
         // ---- stage x as the B operand of GEMM 1 (K-major: rows = 2 TR re/im
-        // columns, K = z).  Thread (channel sj, z-blocks sp, sp + P, ...) loads
-        // 8 consecutive z (64 contiguous bytes) and writes four 16-byte units
-        // (re/im x hi/lo).
+        // columns, K = z)
         {
             const bool jok = sj < nrow;
-            const float2 *xr = prm.x + (size_t)(row0 + sj) * n;
-            for (int zb = sp; zb < kb; zb += P) {
-                float2 v[8];
+            if (use_pf) {
+                cp_async_wait_all();
+                __syncthreads();                       // the raw tile is complete
+                float2 v[kMaxPf][8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int z = zb * 8 + u;
-                    v[u] = (jok && z < n) ? xr[z] : make_float2(0.f, 0.f);
-                }
-                uint32_t rh[4], ih[4], rl[4], il[4];
+                for (int u = 0; u < kMaxPf; ++u) {
+                    const int zb = sp + u * P;
 #pragma unroll
-                for (int u = 0; u < 8; u += 2) {
-                    const __nv_bfloat162 hr = __floats2bfloat162_rn(v[u].x, v[u + 1].x);
-                    const __nv_bfloat162 hi = __floats2bfloat162_rn(v[u].y, v[u + 1].y);
-                    const float2 fr = __bfloat1622float2(hr), fi = __bfloat1622float2(hi);
-                    const __nv_bfloat162 lr = __floats2bfloat162_rn(v[u].x - fr.x, v[u + 1].x - fr.y);
-                    const __nv_bfloat162 li = __floats2bfloat162_rn(v[u].y - fi.x, v[u + 1].y - fi.y);
-                    rh[u >> 1] = *reinterpret_cast<const uint32_t *>(&hr);
-                    ih[u >> 1] = *reinterpret_cast<const uint32_t *>(&hi);
-                    rl[u >> 1] = *reinterpret_cast<const uint32_t *>(&lr);
-                    il[u >> 1] = *reinterpret_cast<const uint32_t *>(&li);
+                    for (int e = 0; e < 8; ++e) {
+                        const int z = zb * 8 + e;
+                        v[u][e] = (u < upt && zb < kb && jok && z < n) ? raw[(size_t)sj * n + z]
+                                                                        : make_float2(0.f, 0.f);
+                    }
                 }
-                const uint32_t o_re = kmaj_off(2 * sj, zb * 8, N), o_im = o_re + 16;
-                *reinterpret_cast<uint4 *>(b_hi + o_re) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-                *reinterpret_cast<uint4 *>(b_hi + o_im) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-                *reinterpret_cast<uint4 *>(b_lo + o_re) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-                *reinterpret_cast<uint4 *>(b_lo + o_im) = make_uint4(il[0], il[1], il[2], il[3]);
+                __syncthreads();                       // raw reads done before B is overwritten
+#pragma unroll
+                for (int u = 0; u < kMaxPf; ++u) {
+                    const int zb = sp + u * P;
+                    if (u < upt && zb < kb) write_unit(zb, v[u]);
+                }
+            } else {
+                const float2 *xr = prm.x + (size_t)(row0 + sj) * n;
+                for (int zb = sp; zb < kb; zb += P) {
+                    float2 v[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int z = zb * 8 + u;
+                        v[u] = (jok && z < n) ? xr[z] : make_float2(0.f, 0.f);
+                    }
+                    write_unit(zb, v);
+                }
             }
         }
         fence_proxy_async();
@@ -500,6 +562,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         }
         tc_fence_after();
         if (!__syncthreads_and(ok)) { ok = false; break; }
+        // the B buffer is free: find the next active tile and start its copy
+        if (tid == 0) next_s = find_active(tile + gridDim.x);
+        __syncthreads();
+        const int next = next_s;
+        if (use_pf && next < prm.ntiles) prefetch(next);
 
         // ---- epilogue 2: u rows to global (z contiguous across lanes)
         for (int m = 0; m < mt_count && epi; ++m) {
@@ -518,9 +585,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         }
         tc_fence_before();
         __syncthreads();
+        tile = next;
     }
 
     if (!ok && tid == 0 && prm.error) atomicExch(prm.error, 1);
+    cp_async_wait_all();   // no copy may land after the kernel leaves
     // Drain on a time-out: give the copy or MMAs still in flight a bounded
     // chance to finish before the accumulator columns are released.
     if (tid == 0 && !e_ok) (void)mbar_wait(&bar_e, 0);   // copy issued but not yet seen complete
