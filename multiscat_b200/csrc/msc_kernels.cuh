@@ -599,6 +599,26 @@ k_update(Tiles tiles, const int *__restrict__ gate, int n, const typename CT<R>:
     }
 }
 
+// Residual of the zero guess: out = b (b_spec e_n on the specular row, the
+// boundary source of an adjoint solve otherwise).  Replaces the T GEMM and
+// the FP64 coupling of the first refinement step when x = 0.
+__global__ void __launch_bounds__(256)
+k_rhs_residual(Tiles tiles, const int *__restrict__ gate, int n,
+               const double2 *__restrict__ row_rhs, double2 *__restrict__ out)
+{
+    const int tile = blockIdx.x;
+    const int sys = tiles.sys[tile];
+    if (gate && gate[sys] == 0) return;
+    const int row0 = tiles.row0[tile];
+    const size_t e0 = (size_t)row0 * n;
+    const int ne = tiles.nrow[tile] * n;
+    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < ne; e += gridDim.y * blockDim.x) {
+        const int r = e / n;
+        const int z = e - r * n;
+        out[e0 + e] = (z == n - 1) ? row_rhs[row0 + r] : make_double2(0.0, 0.0);
+    }
+}
+
 // Mixed form: dst32 = src64 * scale[s]  (the normalised FP64 residual as the
 // first FP32 Krylov vector).
 __global__ void __launch_bounds__(256)
@@ -778,14 +798,6 @@ __device__ void arnoldi_givens(GmresState &st, int s, int m, int j, double rtol,
     if (st.iters[s] >= max_iter) stop = true;
     if (beta <= 1e-300) stop = true;
     if (stop) st.active[s] = 0;
-}
-
-__global__ void k_arnoldi_step(GmresState st, int nsys, int m, int j, double rtol, int max_iter,
-                               double inner_rtol)
-{
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nsys) return;
-    arnoldi_givens(st, s, m, j, rtol, max_iter, inner_rtol);
 }
 
 // y = R^-1 g over the kcyc columns of this cycle.

@@ -203,7 +203,7 @@ struct msc_plan {
     DevBuf<int2> taps_d;                      // [K] tap offsets (dx, dy)
     DevBuf<int> sys_counter;       // per-system arrival counters of the fused Arnoldi kernels
     cudaStream_t stream = nullptr;
-    cudaGraphExec_t g_start = nullptr, g_iter = nullptr;
+    cudaGraphExec_t g_start = nullptr, g_start0 = nullptr, g_iter = nullptr;
     int pstride = 0;
     // measurement
     bool timing = false;
@@ -214,11 +214,12 @@ struct msc_plan {
     int *kcyc_host = nullptr;            // pinned [B]
     int64_t launches_last = 0;
     int cycles_last = 0;
-    int64_t launches_start = 0, launches_iter = 0;   // kernel nodes per graph
+    int64_t launches_start = 0, launches_start0 = 0, launches_iter = 0;   // kernel nodes per graph
 
     ~msc_plan()
     {
         if (g_start) cudaGraphExecDestroy(g_start);
+        if (g_start0) cudaGraphExecDestroy(g_start0);
         if (g_iter) cudaGraphExecDestroy(g_iter);
         if (counter_host) cudaFreeHost(counter_host);
         if (kcyc_host) cudaFreeHost(kcyc_host);
@@ -516,12 +517,17 @@ void mark(msc_plan *p, int kind, int slot, int which, cudaStream_t st)
 // FP64 form: r lands in Q0 and is scaled in place.  Mixed form: r lands in
 // R64 and its normalised FP32 copy becomes the first inner Krylov vector, so
 // every cycle is one step of iterative refinement with an FP64 residual.
-void record_cycle_start(msc_plan *p, cudaStream_t st)
+void record_cycle_start_t(msc_plan *p, bool x_zero, cudaStream_t st)
 {
     double2 *r64 = p->mixed ? p->R64.p : p->Q.p;
     cudaMemsetAsync(p->counter.p, 0, sizeof(int), st);
-    launch_residual_diag(p, p->unfinished.p, p->X.p, p->TMP.p, 1, st);
-    launch_coupling(p, p->unfinished.p, p->X.p, p->TMP.p, -1.0, r64, st);
+    if (x_zero) {
+        msc::k_rhs_residual<<<elementwise_grid(p), 256, 0, st>>>(p->tiles(), p->unfinished.p, p->n,
+                                                                 p->row_rhs.p, r64);
+    } else {
+        launch_residual_diag(p, p->unfinished.p, p->X.p, p->TMP.p, 1, st);
+        launch_coupling(p, p->unfinished.p, p->X.p, p->TMP.p, -1.0, r64, st);
+    }
     launch_dots_t<double>(p, p->unfinished.p, p->Q.p, 0, r64, 1, st);
     launch_reduce(p, p->unfinished.p, 1, p->h2.p, st);
     msc::k_cycle_start<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m, p->h2.p,
@@ -535,6 +541,12 @@ void record_cycle_start(msc_plan *p, cudaStream_t st)
     }
     cudaMemcpyAsync(p->counter_host, p->counter.p, sizeof(int), cudaMemcpyDeviceToHost, st);
 }
+
+void record_cycle_start(msc_plan *p, cudaStream_t st) { record_cycle_start_t(p, false, st); }
+
+// First cycle of a solve from x = 0 (no warm start): r = b without the
+// residual's T GEMM and FP64 coupling.
+void record_cycle_start_zero(msc_plan *p, cudaStream_t st) { record_cycle_start_t(p, true, st); }
 
 // m Arnoldi steps (CGS2) in precision R and the solution update x += M (Q y).
 // out = M x with the von Neumann preconditioner of order k,
@@ -1299,6 +1311,8 @@ msc_status finalize(msc_plan *p)
     for (cudaEvent_t &e : p->tev) MSC_CUDA(cudaEventCreate(&e));
     msc_status st = capture(p, record_cycle_start, &p->g_start, &p->launches_start);
     if (st != MSC_OK) return st;
+    st = capture(p, record_cycle_start_zero, &p->g_start0, &p->launches_start0);
+    if (st != MSC_OK) return st;
     st = capture(p, record_cycle_iterations, &p->g_iter, &p->launches_iter);
     if (st != MSC_OK) return st;
     tm.mark("graph capture");
@@ -1576,8 +1590,9 @@ msc_status msc_solve(msc_plan *p, double *psi_out, double *intensities_out, msc_
     int64_t launches = 0;
     bool pending = false;
     for (; cycle < max_cycles; ++cycle) {
-        MSC_CUDA(cudaGraphLaunch(p->g_start, ps));
-        launches += p->launches_start;
+        const bool x_zero = cycle == 0 && !p->has_x0;
+        MSC_CUDA(cudaGraphLaunch(x_zero ? p->g_start0 : p->g_start, ps));
+        launches += x_zero ? p->launches_start0 : p->launches_start;
         MSC_CUDA(cudaStreamSynchronize(ps));
         if (pending && p->timing) accumulate_timing(p);
         pending = false;

@@ -89,3 +89,28 @@ def test_corrugated_morse_is_differentiable():
     v.real.sum().backward()
     assert h.grad is not None and torch.isfinite(h.grad)
     assert d.grad is not None and torch.isfinite(d.grad)
+
+
+def test_scattering_matrix_from_state_is_the_boundary_formula():
+    """get_scattering_matrix_from_state (_multiscat.py:63-99) against the oracle's
+    S_G = 2i b_G psi_G(z_n) + delta_G0 a_0 on a random state of a 10x10x40 grid."""
+    from multiscat_b200.api import (ScatteringCondition, ScatteringMetadata,
+                                    get_scattering_matrix_from_state, natural_arrays)
+    nkx, nky, nz = 10, 10, 40
+    nodes, _ = inputs.lobatto_rule(0.0, 8.0, nz)
+    md = ScatteringMetadata(vectors=(np.array([2.84e-10, 0.0]), np.array([0.0, 2.84e-10])),
+                            shape=(nkx, nky, nz), z_delta=8e-10)
+    cond = ScatteringCondition.from_angles(
+        mass=sa.ALPHA_PARTICLE_MASS, theta=math.radians(30.0), phi=math.radians(15.0),
+        energy=20e-3 * sa.ELECTRON_VOLT,
+        potential_values=inputs.wolken_potential(nodes, nkx, nky) * sa.MEV, metadata=md)
+    rng = np.random.default_rng(11)
+    state = rng.normal(size=(nkx, nky, nz)) + 1j * rng.normal(size=(nkx, nky, nz))
+    got = get_scattering_matrix_from_state(state, cond)
+    assert got.dtype == np.complex128 and got.shape == (nkx, nky)
+    arr = natural_arrays(cond)
+    wa, wb, _ = inputs.waves(arr.pkd.ravel(), arr.weights, 0.0, 8.0)
+    want = inputs.intensities(state.reshape(nkx * nky, nz), np.asarray(wa).ravel(),
+                              np.asarray(wb).ravel()).reshape(nkx, nky)
+    np.testing.assert_allclose(got.real, want, rtol=1e-12, atol=0)
+    assert float(np.abs(got.imag).max()) == 0.0
