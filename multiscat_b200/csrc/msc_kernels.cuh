@@ -315,9 +315,9 @@ k_coupling(Tiles tiles, const int *__restrict__ gate, int n, int K,
 // positions -- the reach of the coupling taps -- for its z range in shared
 // memory (absent channels, i.e. positions outside a truncated channel set,
 // read as zero; positions wrap around the torus exactly as the reference's
-// modulo(G_j - G_i, n) does).  Each thread keeps one column of 8 + 2 HY halo
-// values in registers and produces 8 outputs along y for one (x, z):
-// for every tap (sdx, sdy) in the window it issues 8 complex FMAs from
+// modulo(G_j - G_i, n) does).  Each thread keeps one column of YS + 2 HY halo
+// values in registers and produces YS outputs along y for one (x, z):
+// for every tap (sdx, sdy) in the window it issues YS complex FMAs from
 // registers, so a halo value loaded once serves up to 2 HY + 1 taps.
 //   out[r] = in0[r] + sgn * sum_t V_t(z) src[pos(r) - delta_t](z)
 // ---------------------------------------------------------------------------
@@ -349,7 +349,11 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
     C2 *halo = reinterpret_cast<C2 *>(smem_raw);                              // [HXW][HYW][ZC]
     C2 *vw = halo + (size_t)HXW * HYW * ZC;                                   // [window cell][ZC]
     int *rows = reinterpret_cast<int *>(vw + (size_t)nwin * ZC);              // [HXW][HYW]
-    __shared__ int colany[BX];
+    // segany[seg][x]: does y segment seg (YS positions) of patch column x hold
+    // a channel?  Threads of empty segments skip the tap loop (truncated
+    // channel sets leave many near the edge of the channel disk).
+    constexpr int NSEG = BY / YS;
+    __shared__ int segany[NSEG * BX];
 
     const int w = blockIdx.x;
     const int s = ct.work[3 * w];
@@ -374,13 +378,14 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
         if (gy < 0) gy += nky;
         rows[pidx] = pr[gx * nky + gy];
     }
-    if (threadIdx.x < BX) {
-        const int gx = x0 + threadIdx.x;
+    if (threadIdx.x < NSEG * BX) {
+        const int cx = threadIdx.x % BX, seg = threadIdx.x / BX;
+        const int gx = x0 + cx;
         int any = 0;
         if (gx < nkx)
-            for (int y = 0; y < BY && !any; ++y)
+            for (int y = seg * YS; y < (seg + 1) * YS && !any; ++y)
                 any = (y0 + y < nky) && pr[gx * nky + y0 + y] >= 0;
-        colany[threadIdx.x] = any;
+        segany[threadIdx.x] = any;
     }
     __syncthreads();
     constexpr int kU = 8;
@@ -434,7 +439,7 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
     const int tx = (threadIdx.x / ZC) % BX;
     const int ysub = threadIdx.x / (ZC * BX);      // which YS-slice of the 8 y outputs
     const int z = z0 + zl;
-    if (x0 + tx >= nkx || z >= n || !colany[tx]) return;
+    if (x0 + tx >= nkx || z >= n || !segany[ysub * BX + tx]) return;
     R ar[YS], ai[YS];
 #pragma unroll
     for (int y = 0; y < YS; ++y) {
