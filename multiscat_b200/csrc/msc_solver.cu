@@ -182,7 +182,9 @@ struct msc_plan {
     // tcgen05 block inverse (mixed form)
     bool use_tc = false;
     int tc_n = 0, tc_tile_rows = 0, tc_ntiles = 0, tc_grid = 0;
-    size_t tc_smem = 0;
+    int tc_groups = 1;          // warp groups with their own tile loop (1 or 2)
+    int tc2_max = 0;            // widest N the two-group kernel may take (0: none)
+    size_t tc_smem = 0, tc2_smem = 0;
     DevBuf<__nv_bfloat16> e_img;
     DevBuf<int> tc_error;
     DevBuf<int> active, kcyc, iters, cycles, unfinished, status, counter;
@@ -346,12 +348,25 @@ void launch_block_inverse_tc(msc_plan *p, const int *gate, const float2 *x, floa
     prm.x = x;
     prm.out = out;
     prm.error = p->tc_error.p;
+    using msc::tc::k_block_inverse_tc;
+    constexpr int T = msc::tc::kThreads;
+    if (p->tc_groups == 2) {
+        const size_t sm = p->tc2_smem;
+        switch (p->tc_n) {
+        case 16: k_block_inverse_tc<16, 2><<<p->tc_grid, T, sm, st>>>(prm); break;
+        case 32: k_block_inverse_tc<32, 2><<<p->tc_grid, T, sm, st>>>(prm); break;
+        case 64: k_block_inverse_tc<64, 2><<<p->tc_grid, T, sm, st>>>(prm); break;
+        default: k_block_inverse_tc<128, 2><<<p->tc_grid, T, sm, st>>>(prm); break;
+        }
+        return;
+    }
+    const size_t sm = p->tc_smem;
     switch (p->tc_n) {
-    case 16: msc::tc::k_block_inverse_tc<16><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
-    case 32: msc::tc::k_block_inverse_tc<32><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
-    case 64: msc::tc::k_block_inverse_tc<64><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
-    case 128: msc::tc::k_block_inverse_tc<128><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
-    default: msc::tc::k_block_inverse_tc<256><<<p->tc_grid, msc::tc::kThreads, p->tc_smem, st>>>(prm); break;
+    case 16: k_block_inverse_tc<16, 1><<<p->tc_grid, T, sm, st>>>(prm); break;
+    case 32: k_block_inverse_tc<32, 1><<<p->tc_grid, T, sm, st>>>(prm); break;
+    case 64: k_block_inverse_tc<64, 1><<<p->tc_grid, T, sm, st>>>(prm); break;
+    case 128: k_block_inverse_tc<128, 1><<<p->tc_grid, T, sm, st>>>(prm); break;
+    default: k_block_inverse_tc<256, 1><<<p->tc_grid, T, sm, st>>>(prm); break;
     }
 }
 
@@ -749,43 +764,90 @@ msc_status set_kernel_attributes(int n, int K)
     return MSC_OK;
 }
 
-// Shared memory the tensor-core kernel needs for tile width N (bytes of the
-// dynamic part), including the bytes its padded M tiles may read past E.
-size_t tc_smem_bytes(int n, int N)
+// Shared memory the tensor-core kernel needs for tile width N and G warp
+// groups (bytes of the dynamic part: E_hi, E_lo and one B buffer per group),
+// including the bytes its padded M tiles may read past E.
+size_t tc_smem_bytes(int n, int N, int G = 1)
 {
     const size_t kp = (size_t)(n + 15) / 16 * 16;
     const size_t kb = kp / 8, mt = (size_t)(n + 127) / 128;
     const size_t part = kp * kp * 2, sz = kb * 128;
     const size_t read1 = (16 * mt - 1) * 128 + (kb - 1) * sz + 128;
     const size_t read2 = (16 * mt - 1) * sz + (kb - 1) * 128 + 128;
-    const size_t need = std::max(2 * part + 4 * (size_t)N * kp, part + std::max(read1, read2));
+    const size_t need = std::max(2 * part + (size_t)G * 4 * N * kp, part + std::max(read1, read2));
     return (need + 1023) / 1024 * 1024 + 1024;
 }
 
-template <int N>
+// TMEM columns one CTA allocates: a power of two >= 32 per group.
+int tc_tmem_cols(int n, int N, int G)
+{
+    const int mt = (n + 127) / 128;
+    int ncols = 32;
+    while (ncols < 2 * mt * N) ncols <<= 1;
+    return G * ncols;
+}
+
+template <int N, int G>
 cudaError_t tc_set_smem(size_t bytes)
 {
-    return cudaFuncSetAttribute(msc::tc::k_block_inverse_tc<N>,
+    return cudaFuncSetAttribute(msc::tc::k_block_inverse_tc<N, G>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-template <int N>
+template <int N, int G>
 size_t tc_static_smem()
 {
     cudaFuncAttributes a{};
-    if (cudaFuncGetAttributes(&a, msc::tc::k_block_inverse_tc<N>) != cudaSuccess) return 1u << 30;
+    if (cudaFuncGetAttributes(&a, msc::tc::k_block_inverse_tc<N, G>) != cudaSuccess) return 1u << 30;
     return a.sharedSizeBytes;
 }
 
-size_t tc_static_for(int N)
+size_t tc_static_for(int N, int G = 1)
 {
-    switch (N) {
-    case 16: return tc_static_smem<16>();
-    case 32: return tc_static_smem<32>();
-    case 64: return tc_static_smem<64>();
-    case 128: return tc_static_smem<128>();
-    default: return tc_static_smem<256>();
+    if (G == 2) {
+        switch (N) {
+        case 16: return tc_static_smem<16, 2>();
+        case 32: return tc_static_smem<32, 2>();
+        case 64: return tc_static_smem<64, 2>();
+        default: return tc_static_smem<128, 2>();
+        }
     }
+    switch (N) {
+    case 16: return tc_static_smem<16, 1>();
+    case 32: return tc_static_smem<32, 1>();
+    case 64: return tc_static_smem<64, 1>();
+    case 128: return tc_static_smem<128, 1>();
+    default: return tc_static_smem<256, 1>();
+    }
+}
+
+cudaError_t tc_set_smem_for(int N, int G, size_t bytes)
+{
+    if (G == 2) {
+        switch (N) {
+        case 16: return tc_set_smem<16, 2>(bytes);
+        case 32: return tc_set_smem<32, 2>(bytes);
+        case 64: return tc_set_smem<64, 2>(bytes);
+        default: return tc_set_smem<128, 2>(bytes);
+        }
+    }
+    switch (N) {
+    case 16: return tc_set_smem<16, 1>(bytes);
+    case 32: return tc_set_smem<32, 1>(bytes);
+    case 64: return tc_set_smem<64, 1>(bytes);
+    case 128: return tc_set_smem<128, 1>(bytes);
+    default: return tc_set_smem<256, 1>(bytes);
+    }
+}
+
+// Shared-memory request of a kernel variant: what it needs, padded so that
+// no more CTAs fit on one SM than its 512 TMEM columns can serve.
+size_t tc_request_bytes(int n, int N, int G)
+{
+    const size_t max_ctas = 512 / (size_t)tc_tmem_cols(n, N, G);
+    const size_t sm_bytes = 233472;   // 228 KB of shared memory per SM
+    const size_t floor_bytes = sm_bytes / (max_ctas + 1) + 1024;
+    return std::max(tc_smem_bytes(n, N, G), floor_bytes);
 }
 
 // Decide whether the mixed form uses the tcgen05 block inverse and with what
@@ -801,10 +863,10 @@ msc_status setup_tensor_core(msc_plan *p)
     MSC_CUDA(cudaDeviceGetAttribute(&cc_minor, cudaDevAttrComputeCapabilityMinor, dev));
     MSC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (cc_major != 10 || cc_minor != 0) return MSC_OK;   // tcgen05 path is built for sm_100a
-    const int n = p->n, mt = (n + 127) / 128;
+    const int n = p->n;
     int chosen = 0;
     for (int N = 16; N <= 256; N *= 2) {
-        if (2 * mt * N > 512) break;
+        if (tc_tmem_cols(n, N, 1) > 512) break;
         if (tc_smem_bytes(n, N) + tc_static_for(N) > (size_t)optin) break;
         const int tiles = (p->R + N / 2 - 1) / (N / 2);
         chosen = N;
@@ -812,33 +874,31 @@ msc_status setup_tensor_core(msc_plan *p)
     }
     if (chosen == 0) return MSC_OK;
     p->tc_n = chosen;
+    p->tc_groups = 1;
     p->tc_tile_rows = chosen / 2;
     p->tc_ntiles = (p->R + p->tc_tile_rows - 1) / p->tc_tile_rows;
     p->tc_grid = std::min(p->tc_ntiles, sms);
-    p->tc_smem = tc_smem_bytes(n, chosen);
-    {
-        // TMEM: CTAs resident on one SM must fit in its 512 columns, so pad
-        // the shared-memory request until no more than 512 / ncols CTAs fit.
-        int ncols = 32;
-        while (ncols < 2 * mt * chosen) ncols <<= 1;
-        const size_t max_ctas = 512 / (size_t)ncols;
-        const size_t sm_bytes = 233472;   // 228 KB of shared memory per SM
-        const size_t floor_bytes = sm_bytes / (max_ctas + 1) + 1024;
-        p->tc_smem = std::max(p->tc_smem, floor_bytes);
-        if (p->tc_smem + tc_static_for(chosen) > (size_t)optin) return MSC_OK;
-    }
     // every width up to `chosen` may be picked by the autotuner; all launch
     // with the same (largest) shared-memory request
+    p->tc_smem = tc_request_bytes(n, chosen, 1);
+    if (p->tc_smem + tc_static_for(chosen) > (size_t)optin) return MSC_OK;
     for (int N = 16; N <= chosen; N *= 2) {
-        cudaError_t e = cudaSuccess;
-        switch (N) {
-        case 16: e = tc_set_smem<16>(p->tc_smem); break;
-        case 32: e = tc_set_smem<32>(p->tc_smem); break;
-        case 64: e = tc_set_smem<64>(p->tc_smem); break;
-        case 128: e = tc_set_smem<128>(p->tc_smem); break;
-        default: e = tc_set_smem<256>(p->tc_smem); break;
-        }
+        cudaError_t e = tc_set_smem_for(N, 1, p->tc_smem);
         if (e != cudaSuccess) return fail(MSC_ERR_CUDA, std::string("tc smem attribute: ") + cudaGetErrorString(e));
+    }
+    // two-group variants: widths whose two TMEM regions and two B buffers fit
+    p->tc2_max = 0;
+    for (int N = 16; N <= std::min(chosen, 128); N *= 2) {
+        if (tc_tmem_cols(n, N, 2) > 512) break;
+        if (tc_request_bytes(n, N, 2) + tc_static_for(N, 2) > (size_t)optin) break;
+        p->tc2_max = N;
+    }
+    if (p->tc2_max > 0) {
+        p->tc2_smem = tc_request_bytes(n, p->tc2_max, 2);
+        for (int N = 16; N <= p->tc2_max; N *= 2) {
+            cudaError_t e = tc_set_smem_for(N, 2, p->tc2_smem);
+            if (e != cudaSuccess) return fail(MSC_ERR_CUDA, std::string("tc smem attribute: ") + cudaGetErrorString(e));
+        }
     }
     // E image: [hi|lo][z/8][k/8][z%8][k%8], zero padded to kp x kp
     const int kp = (n + 15) / 16 * 16, kb = kp / 8;
@@ -891,36 +951,39 @@ struct TuneKey {
     }
 };
 struct TuneChoice {
-    int halo64, halo32, use_tc, tc_n;
+    int halo64, halo32, use_tc, tc_n, tc_groups;
 };
 std::mutex g_tune_mutex;
 std::map<TuneKey, TuneChoice> g_tune_cache;
 
 msc_status autotune_measure(msc_plan *p);
 
-void apply_tc_width(msc_plan *p, int N)
+void apply_tc_width(msc_plan *p, int N, int G = 1)
 {
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (G == 2 && N > p->tc2_max) G = 1;
     p->tc_n = N;
+    p->tc_groups = G;
     p->tc_tile_rows = N / 2;
     p->tc_ntiles = (p->R + N / 2 - 1) / (N / 2);
-    p->tc_grid = std::min(p->tc_ntiles, sms);
+    p->tc_grid = std::min((p->tc_ntiles + G - 1) / G, sms);
 }
 
 // Autotuner front end: reuse the choices of an earlier plan of the same
 // shape (same sizes, batch, tap reach and options), else measure.
-// MSC_TUNE="c64=K,c32=K,bi=N" fixes the choices (K: 0 neighbour table,
-// 1 halo 8 y/thread, 2 halo 4 y/thread; N: tcgen05 tile width, 0 = SIMT).
+// MSC_TUNE="c64=K,c32=K,bi=N[,bg=G]" fixes the choices (K: 0 neighbour
+// table, 1 halo 8 y/thread, 2 halo 4 y/thread; N: tcgen05 tile width,
+// 0 = SIMT; G: 1 or 2 warp groups in the tcgen05 kernel, default 1).
 // Profiling runs use it so that a profiler's overhead cannot change what the
 // autotuner picks.
 bool tune_from_env(msc_plan *p)
 {
     const char *env = std::getenv("MSC_TUNE");
     if (!env || !*env) return false;
-    int c64 = p->halo64, c32 = p->halo32, bi = p->use_tc ? p->tc_n : 0;
-    std::sscanf(env, "c64=%d,c32=%d,bi=%d", &c64, &c32, &bi);
+    int c64 = p->halo64, c32 = p->halo32, bi = p->use_tc ? p->tc_n : 0, bg = 1;
+    std::sscanf(env, "c64=%d,c32=%d,bi=%d,bg=%d", &c64, &c32, &bi, &bg);
     p->halo64 = p->use_halo ? std::max(0, std::min(2, c64)) : 0;
     p->halo32 = p->use_halo ? std::max(0, std::min(2, c32)) : 0;
     if (p->use_tc) {
@@ -929,7 +992,7 @@ bool tune_from_env(msc_plan *p)
         } else {
             int N = 16;
             while (N < bi && N < p->tc_n) N *= 2;
-            apply_tc_width(p, N);
+            apply_tc_width(p, N, bg == 2 ? 2 : 1);
         }
     }
     p->tune_log.push_back({"from_MSC_TUNE", 1.f});
@@ -949,7 +1012,7 @@ msc_status autotune(msc_plan *p)
             p->halo32 = it->second.halo32;
             if (p->use_tc) {
                 p->use_tc = it->second.use_tc != 0;
-                if (p->use_tc) apply_tc_width(p, it->second.tc_n);
+                if (p->use_tc) apply_tc_width(p, it->second.tc_n, it->second.tc_groups);
             }
             p->tune_log.push_back({"cached", 1.f});
             return MSC_OK;
@@ -958,7 +1021,7 @@ msc_status autotune(msc_plan *p)
     msc_status st = autotune_measure(p);
     if (st != MSC_OK) return st;
     std::lock_guard<std::mutex> lock(g_tune_mutex);
-    g_tune_cache[key] = TuneChoice{p->halo64, p->halo32, p->use_tc ? 1 : 0, p->tc_n};
+    g_tune_cache[key] = TuneChoice{p->halo64, p->halo32, p->use_tc ? 1 : 0, p->tc_n, p->tc_groups};
     return MSC_OK;
 }
 
@@ -1005,11 +1068,8 @@ msc_status autotune_measure(msc_plan *p)
             p->halo32 = best_k;
         }
         if (p->use_tc) {
-            int sms = 0, dev = 0;
-            MSC_CUDA(cudaGetDevice(&dev));
-            MSC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
             const int best_n0 = p->tc_n;
-            int best_n = 0;
+            int best_n = 0, best_g = 1;
             float best_t = 0.f;
             p->use_tc = false;
             const float t_simt = time_launch(p, [&](cudaStream_t st) {
@@ -1017,30 +1077,28 @@ msc_status autotune_measure(msc_plan *p)
             });
             p->tune_log.push_back({"block_inverse32_simt_us", t_simt});
             p->use_tc = true;
-            for (int N = 16; N <= best_n0; N *= 2) {
-                p->tc_n = N;
-                p->tc_tile_rows = N / 2;
-                p->tc_ntiles = (p->R + N / 2 - 1) / (N / 2);
-                p->tc_grid = std::min(p->tc_ntiles, sms);
-                const float t = time_launch(p, [&](cudaStream_t st) {
-                    launch_block_inverse_t<float>(p, nullptr, a, b, 0, st);
-                });
-                p->tune_log.push_back({"block_inverse32_tc_N" + std::to_string(N) + "_us", t});
-                if (best_n == 0 || t < best_t) {
-                    best_n = N;
-                    best_t = t;
+            for (int G = 1; G <= 2; ++G)
+                for (int N = 16; N <= (G == 1 ? best_n0 : p->tc2_max); N *= 2) {
+                    apply_tc_width(p, N, G);
+                    const float t = time_launch(p, [&](cudaStream_t st) {
+                        launch_block_inverse_t<float>(p, nullptr, a, b, 0, st);
+                    });
+                    p->tune_log.push_back({std::string("block_inverse32_tc") + (G == 2 ? "2" : "") +
+                                               "_N" + std::to_string(N) + "_us",
+                                           t});
+                    if (best_n == 0 || t < best_t) {
+                        best_n = N;
+                        best_g = G;
+                        best_t = t;
+                    }
                 }
-            }
             int tc_err = 0;
             MSC_CUDA(cudaMemcpy(&tc_err, p->tc_error.p, sizeof(int), cudaMemcpyDeviceToHost));
             if (tc_err) return fail(MSC_ERR_CUDA, "tensor-core block inverse timed out during tuning");
             if (t_simt < best_t && !(p->desc.flags & 2)) {
                 p->use_tc = false;
             } else {
-                p->tc_n = best_n;
-                p->tc_tile_rows = best_n / 2;
-                p->tc_ntiles = (p->R + best_n / 2 - 1) / (best_n / 2);
-                p->tc_grid = std::min(p->tc_ntiles, sms);
+                apply_tc_width(p, best_n, best_g);
             }
         }
     }
@@ -1737,7 +1795,7 @@ const char *msc_plan_tuning_report(msc_plan *p)
     const char *kn[3] = {"neighbour", "halo_y8", "halo_y4"};
     r += "\"chosen\": \"coupling64=" + std::string(p->use_halo ? kn[p->halo64] : kn[0]) +
          ",coupling32=" + std::string(p->use_halo ? kn[p->halo32] : kn[0]) +
-         ",block_inverse32=" + (p->use_tc ? "tc_N" + std::to_string(p->tc_n) : std::string("simt")) +
+         ",block_inverse32=" + (p->use_tc ? std::string(p->tc_groups == 2 ? "tc2_N" : "tc_N") + std::to_string(p->tc_n) : std::string("simt")) +
          "\"}";
     p->tune_report = r;
     return p->tune_report.c_str();

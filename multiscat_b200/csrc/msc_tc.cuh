@@ -107,6 +107,28 @@ __device__ __forceinline__ void fence_proxy_async()
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Named barrier `id` over `count` threads (a warp group's tile loop; barrier
+// 0 stays the CTA-wide __syncthreads).
+__device__ __forceinline__ void group_sync(int id, int count)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Named barrier that also returns the AND of `v` over the participating threads.
+__device__ __forceinline__ bool group_and(int id, int count, bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(count)
+        : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -240,48 +262,58 @@ __device__ __forceinline__ uint32_t kmaj_off(int c, int k, int rows)
     return (uint32_t)(((k >> 3) * (rows >> 3) + (c >> 3)) * 128 + (c & 7) * 16 + (k & 7) * 2);
 }
 
-template <int N>
+// G = 1: the CTA's 8 warps work on one tile at a time.  G = 2: two groups
+// of 4 warps (warps 0-3, 4-7), each with its own B buffer, TMEM columns,
+// mbarrier and named barrier, run independent tile loops over the shared E
+// image, so that one group's staging and epilogues overlap the other's MMAs.
+template <int N, int G>
 __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
 {
     static_assert(N % 16 == 0 && N >= 16 && N <= 256, "N must be a multiple of 16 in [16, 256]");
+    static_assert(G == 1 || (G == 2 && N <= 128), "two groups take N <= 128");
     // Supports n <= 256 (at most two M tiles of 128).
+    constexpr int GT = kThreads / G;          // threads per group
+    constexpr int NW = GT / 32;               // warps per group
     constexpr int TR = N / 2;                 // channels per tile
-    constexpr int P = kThreads / TR;          // staging threads per channel
+    constexpr int P = GT / TR;                // staging threads per channel
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bar_e, bar_mma;
+    __shared__ __align__(8) uint64_t bar_e, bar_mma[G];
     __shared__ uint32_t tmem_base_s;
-    __shared__ float sm_part[8][2][N];        // Sherman-Morrison partial sums [warp][M tile][col]
-    __shared__ float2 beta_s[TR];
-    __shared__ double pkd_s[TR];
+    __shared__ float sm_part[G][NW][2][N];    // Sherman-Morrison partial sums [group][warp][M tile][col]
+    __shared__ float2 beta_s[G][TR];
+    __shared__ double pkd_s[G][TR];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = (G == 1) ? 0 : warp / NW;               // group of this thread
+    const int gtid = tid - g * GT, wl = warp - g * NW;    // thread / warp index within the group
+    const int bar_id = 1 + g;                             // the group's named barrier
     const int lq = warp & 3;                              // TMEM lane quarter of this warp
-    constexpr int HALF = (N >= 32) ? N / 2 : N;           // columns per warp group
-    const int c_begin = (N >= 32) ? (warp >> 2) * HALF : 0;
-    const bool epi = (N >= 32) || warp < 4;               // N = 16: warps 4-7 sit out the epilogues
+    constexpr int HALF = (G == 1 && N >= 32) ? N / 2 : N; // columns per warp
+    const int c_begin = (G == 1 && N >= 32) ? (wl >> 2) * HALF : 0;
+    const bool epi = (G == 2) || (N >= 32) || wl < 4;     // G = 1, N = 16: warps 4-7 sit out the epilogues
     const int n = prm.n, kp = prm.kp, mt_count = prm.mt;
     const int kb = kp >> 3;                               // 8-blocks along z and k
     const uint32_t part_bytes = (uint32_t)kp * kp * 2u;   // one of E_hi / E_lo
     unsigned char *e_hi = smem;
     unsigned char *e_lo = smem + part_bytes;
-    unsigned char *b_hi = smem + 2 * part_bytes;
+    unsigned char *b_hi = smem + 2 * part_bytes + (size_t)g * 4 * N * kp;
     unsigned char *b_lo = b_hi + (size_t)N * kp * 2;
     const uint32_t sz = (uint32_t)kb * 128u;              // stride of a z 8-block in E
     const uint32_t sk = 128u;                             // stride of a k 8-block in E
     const uint32_t b_lbo = (uint32_t)N * 16u;             // B: stride between k 8-blocks
-    uint32_t ncols = 32;
+    uint32_t ncols = 32;                                  // TMEM columns of one group
     while (ncols < (uint32_t)(2 * mt_count * N)) ncols <<= 1;
 
-    if (warp == 0) tmem_alloc(&tmem_base_s, ncols);
+    if (warp == 0) tmem_alloc(&tmem_base_s, G * ncols);
     if (tid == 0) {
         mbar_init(&bar_e, 1);
-        mbar_init(&bar_mma, 1);
+        for (int q = 0; q < G; ++q) mbar_init(&bar_mma[q], 1);
         mbar_fence_init();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = tmem_base_s;
+    const uint32_t tmem = tmem_base_s + (uint32_t)g * ncols;
     bool ok = true;
 
     if (tid == 0) {
@@ -298,7 +330,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     const uint32_t e_hi_a = smem_u32(e_hi), e_lo_a = smem_u32(e_lo);
     const uint32_t b_hi_a = smem_u32(b_hi), b_lo_a = smem_u32(b_lo);
     const int ksteps = kp >> 4;
-    const int sj = tid % TR, sp = tid / TR;               // staging: channel, z-block phase
+    const int sj = gtid % TR, sp = gtid / TR;             // staging: channel, z-block phase
 
     // Staging units: thread (channel sj, z-blocks sp, sp + P, ...) handles 8
     // consecutive z (64 contiguous bytes of x) and writes four 16-byte units
@@ -335,15 +367,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     float2 *raw = reinterpret_cast<float2 *>(b_hi);
     auto prefetch = [&](int t) {
         const int r0 = t * TR, nr = min(TR, prm.rows - r0), half = n >> 1;
-        for (int idx = tid; idx < nr * half; idx += kThreads) {
+        for (int idx = gtid; idx < nr * half; idx += GT) {
             const int j = idx / half, q = idx - j * half;
             cp_async_16(raw + (size_t)j * n + 2 * q, prm.x + (size_t)(r0 + j) * n + 2 * q);
         }
         cp_async_commit_group();
     };
-    // first active tile of this CTA at or after t (stride gridDim.x); thread 0
+    // first active tile of this group at or after t (stride G gridDim.x); the
+    // group's thread 0
     auto find_active = [&](int t) {
-        for (; t < prm.ntiles; t += gridDim.x) {
+        for (; t < prm.ntiles; t += G * gridDim.x) {
             if (!prm.gate) return t;
             const int r0 = t * TR, nr = min(TR, prm.rows - r0);
             const int s0 = prm.row_sys[r0], s1 = prm.row_sys[r0 + nr - 1];
@@ -352,16 +385,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         }
         return prm.ntiles;
     };
-    __shared__ int next_s;
-    if (tid == 0) next_s = find_active(blockIdx.x);
+    __shared__ int next_s[G];
+    if (gtid == 0) next_s[g] = find_active(G * blockIdx.x + g);
     __syncthreads();
-    int tile = next_s;
+    int tile = next_s[g];
     if (use_pf && tile < prm.ntiles) prefetch(tile);
 
     while (tile < prm.ntiles && ok) {
         const int row0 = tile * TR;
         const int nrow = min(TR, prm.rows - row0);
-        for (int j = tid; j < TR; j += kThreads) pkd_s[j] = (j < nrow) ? prm.row_pkd[row0 + j] : 0.0;
+        for (int j = gtid; j < TR; j += GT) pkd_s[g][j] = (j < nrow) ? prm.row_pkd[row0 + j] : 0.0;
 
         // ---- stage x as the B operand of GEMM 1 (K-major: rows = 2 TR re/im
         // columns, K = z)
@@ -369,7 +402,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
             const bool jok = sj < nrow;
             if (use_pf) {
                 cp_async_wait_all();
-                __syncthreads();                       // the raw tile is complete
+                group_sync(bar_id, GT);                // the raw tile is complete
                 float2 v[kMaxPf][8];
 #pragma unroll
                 for (int u = 0; u < kMaxPf; ++u) {
@@ -381,7 +414,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                                                                         : make_float2(0.f, 0.f);
                     }
                 }
-                __syncthreads();                       // raw reads done before B is overwritten
+                group_sync(bar_id, GT);                // raw reads done before B is overwritten
 #pragma unroll
                 for (int u = 0; u < kMaxPf; ++u) {
                     const int zb = sp + u * P;
@@ -404,12 +437,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         if (!e_waited) {
             e_ok = mbar_wait(&bar_e, 0);
             e_waited = true;
-            if (!__syncthreads_and(e_ok)) { ok = false; break; }
+            if (!group_and(bar_id, GT, e_ok)) { ok = false; break; }
         }
-        __syncthreads();
+        group_sync(bar_id, GT);
 
         // ---- GEMM 1: D1[m] = E^T x   (M = k, K = z); accumulator columns [m N, m N + N)
-        if (tid == 0) {
+        if (gtid == 0) {
             tc_fence_after();
             for (int m = 0; m < mt_count; ++m) {
                 const uint32_t d = tmem + (uint32_t)(m * N);
@@ -426,17 +459,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     mma_bf16(d, al, bh, idesc_mn, 1u);
                 }
             }
-            mma_commit(&bar_mma);
+            mma_commit(&bar_mma[g]);
         }
         mma_pending = true;
-        if (mbar_wait(&bar_mma, mma_phase)) {
+        if (mbar_wait(&bar_mma[g], mma_phase)) {
             mma_phase ^= 1u;
             mma_pending = false;
         } else {
             ok = false;
         }
         tc_fence_after();
-        if (!__syncthreads_and(ok)) { ok = false; break; }
+        if (!group_and(bar_id, GT, ok)) { ok = false; break; }
 
         // ---- epilogue 1a: Sherman-Morrison sums s_j = sum_k en_k xt_kj / (pkd_j + lam_k)
         // from the accumulator itself (so beta is consistent with the xt that
@@ -458,7 +491,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     // NaN, which a zero weight would not remove
                     const int j = (c0 + c) >> 1;
                     if (valid && j < nrow) {
-                        const float w = en_k * __frcp_rn((float)(pkd_s[j] + lam_k));
+                        const float w = en_k * __frcp_rn((float)(pkd_s[g][j] + lam_k));
                         v[c] *= w;
                         v[c + 1] *= w;
                     } else {
@@ -467,27 +500,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     }
                 }
                 const float sum = warp_reduce_scatter16(v, lane);
-                if ((lane & 1) == 0) sm_part[warp][m][c0 + ((lane >> 1) & 15)] = sum;
+                if ((lane & 1) == 0) sm_part[g][wl][m][c0 + ((lane >> 1) & 15)] = sum;
             }
         }
-        __syncthreads();
-        for (int j = tid; j < TR; j += kThreads) {
+        group_sync(bar_id, GT);
+        for (int j = gtid; j < TR; j += GT) {
             double2 b = make_double2(0.0, 0.0);
             if (j < nrow) {
                 double sr = 0.0, si = 0.0;   // fixed summation order: deterministic
-                const int wg = (N >= 32) ? ((2 * j) / HALF) * 4 : 0;   // warps that own column 2j
+                // the 4 warps (one per lane quarter) that own column 2j
+                const int wg = (G == 1 && N >= 32) ? ((2 * j) / HALF) * 4 : 0;
                 for (int m = 0; m < mt_count; ++m)
                     for (int w = wg; w < wg + 4; ++w) {
-                        sr += sm_part[w][m][2 * j];
-                        si += sm_part[w][m][2 * j + 1];
+                        sr += sm_part[g][w][m][2 * j];
+                        si += sm_part[g][w][m][2 * j + 1];
                     }
                 const double2 c = prm.row_c[row0 + j];
                 const double fn = prm.row_fn[row0 + j];
                 b = cdiv(cmul(c, make_double2(sr, si)), make_double2(1.0 - c.x * fn, -c.y * fn));
             }
-            beta_s[j] = make_float2((float)b.x, (float)b.y);
+            beta_s[g][j] = make_float2((float)b.x, (float)b.y);
         }
-        __syncthreads();
+        group_sync(bar_id, GT);
 
         // ---- epilogue 1b: yt = (xt + beta en) / (pkd + lam) as the B operand of
         // GEMM 2 in the MN-major layout: one thread holds one k and 16
@@ -509,8 +543,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     const int j = (c0 + c) >> 1;
                     float yr = 0.f, yi = 0.f;
                     if (valid && j < nrow) {
-                        const float inv = __frcp_rn((float)(pkd_s[j] + lam_k));
-                        const float2 b = beta_s[j];
+                        const float inv = __frcp_rn((float)(pkd_s[g][j] + lam_k));
+                        const float2 b = beta_s[g][j];
                         yr = (v[c] + b.x * en_k) * inv;
                         yi = (v[c + 1] + b.y * en_k) * inv;
                     }
@@ -530,10 +564,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         }
         tc_fence_before();
         fence_proxy_async();
-        __syncthreads();
+        group_sync(bar_id, GT);
 
         // ---- GEMM 2: D2[m] = E yt   (M = z, K = k); accumulator columns after D1
-        if (tid == 0) {
+        if (gtid == 0) {
             tc_fence_after();
             for (int m = 0; m < mt_count; ++m) {
                 const uint32_t d = tmem + (uint32_t)((mt_count + m) * N);
@@ -551,21 +585,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     mma_bf16(d, al, bh, idesc_k, 1u);
                 }
             }
-            mma_commit(&bar_mma);
+            mma_commit(&bar_mma[g]);
         }
         mma_pending = true;
-        if (mbar_wait(&bar_mma, mma_phase)) {
+        if (mbar_wait(&bar_mma[g], mma_phase)) {
             mma_phase ^= 1u;
             mma_pending = false;
         } else {
             ok = false;
         }
         tc_fence_after();
-        if (!__syncthreads_and(ok)) { ok = false; break; }
+        if (!group_and(bar_id, GT, ok)) { ok = false; break; }
         // the B buffer is free: find the next active tile and start its copy
-        if (tid == 0) next_s = find_active(tile + gridDim.x);
-        __syncthreads();
-        const int next = next_s;
+        if (gtid == 0) next_s[g] = find_active(tile + G * gridDim.x);
+        group_sync(bar_id, GT);
+        const int next = next_s[g];
         if (use_pf && next < prm.ntiles) prefetch(next);
 
         // ---- epilogue 2: u rows to global (z contiguous across lanes)
@@ -584,20 +618,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
             }
         }
         tc_fence_before();
-        __syncthreads();
+        group_sync(bar_id, GT);
         tile = next;
     }
 
-    if (!ok && tid == 0 && prm.error) atomicExch(prm.error, 1);
+    if (!ok && gtid == 0 && prm.error) atomicExch(prm.error, 1);
     cp_async_wait_all();   // no copy may land after the kernel leaves
     // Drain on a time-out: give the copy or MMAs still in flight a bounded
     // chance to finish before the accumulator columns are released.
-    if (tid == 0 && !e_ok) (void)mbar_wait(&bar_e, 0);   // copy issued but not yet seen complete
-    if (tid == 0 && mma_pending) (void)mbar_wait(&bar_mma, mma_phase);
+    if (gtid == 0 && !e_ok) (void)mbar_wait(&bar_e, 0);   // copy issued but not yet seen complete
+    if (gtid == 0 && mma_pending) (void)mbar_wait(&bar_mma[g], mma_phase);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 0) tmem_dealloc(tmem, ncols);
+    if (warp == 0) tmem_dealloc(tmem_base_s, G * ncols);
 }
 
 }  // namespace tc

@@ -309,6 +309,38 @@ def test_tensor_core_block_inverse_matches_fp64(which):
     simt.close()
 
 
+@pytest.mark.parametrize("groups,width", [(1, 16), (1, 32), (1, 64), (1, 128),
+                                          (2, 16), (2, 32), (2, 64)])
+def test_tensor_core_width_and_warp_groups_match_simt(groups, width, monkeypatch):
+    """Every tcgen05 variant the autotuner can pick (tile width N; one tile
+    loop per CTA or two warp groups with their own), forced through MSC_TUNE,
+    on a 24-beam batch with enough rows for every width."""
+    case, systems = cfg2_batch(n_solves=24, seed=3)
+    rng = np.random.default_rng(19)
+    # a plan reads MSC_TUNE when its first call sets it up
+    monkeypatch.setenv("MSC_TUNE", f"c64=2,c32=2,bi={width},bg={groups}")
+    mixed = ScatteringPlan(case.v, case.t, systems, precision="mixed", tensor_cores=True)
+    shape = (mixed.total_rows, case.v.shape[2])
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    x32 = torch.as_tensor(x.astype(np.complex64), device="cuda")
+    y_tc = mixed.apply_block_inverse_f32(x32).cpu().numpy()
+    monkeypatch.setenv("MSC_TUNE", "c64=2,c32=2,bi=0")
+    simt = ScatteringPlan(case.v, case.t, systems, precision="mixed", tensor_cores=False)
+    y_simt = simt.apply_block_inverse_f32(x32).cpu().numpy()
+    assert mixed.tensor_core_tile == width
+    tag = ("tc2_N" if groups == 2 else "tc_N") + str(width)
+    assert f"block_inverse32={tag}" in mixed.tuning_report()["chosen"]
+    scale = np.abs(y_simt).max()
+    np.testing.assert_allclose(y_tc, y_simt, rtol=0, atol=TC_TOL * scale)
+    # a whole mixed solve on this variant against FP64
+    ref = ScatteringPlan(case.v, case.t, systems).solve().intensities
+    res = mixed.solve()
+    assert (res.status == 0).all()
+    assert float((res.intensities - ref).abs().max()) <= MIXED_TOL
+    mixed.close()
+    simt.close()
+
+
 # ---------------------------------------------------------------------------
 # cfg4 shape: 81 x 81 channels, 300 nodes, |m|,|n| <= 8 (288 taps, halo 8),
 # several azimuths batched.  No oracle here (the CPU restatement would need
@@ -424,6 +456,13 @@ for tc in (True, False):
                            tensor_cores=tc, preconditioner_order=order).solve()
         assert (r.status == 0).all(), (tc, order, r.status)
         worst = max(worst, float((r.intensities - ref).abs().max()))
+import os
+for bg in (1, 2):          # both tcgen05 kernel forms, forced
+    os.environ["MSC_TUNE"] = f"c64=2,c32=2,bi=16,bg={bg}"
+    r = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed",
+                       tensor_cores=True).solve()
+    assert (r.status == 0).all(), (bg, r.status)
+    worst = max(worst, float((r.intensities - ref).abs().max()))
 print(worst)
 """
 
