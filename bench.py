@@ -202,7 +202,7 @@ def run_b200(args) -> None:
     stream = torch.cuda.current_stream()
     plan = ScatteringPlan(case.v, case.t, systems, rtol=args.rtol, restart=args.restart,
                           precision=args.precision, inner_restart=args.inner_restart,
-                          preconditioner_order=args.precond_order)
+                          inner_rtol=args.inner_rtol, preconditioner_order=args.precond_order)
     for _ in range(args.warmup):
         res = plan.solve()
     torch.cuda.synchronize()
@@ -588,6 +588,8 @@ def main() -> None:
     ap.add_argument("--restart", type=int, default=30)
     ap.add_argument("--inner-restart", type=int, default=0,
                     help="mixed form: inner FP32 restart (0 = the library default)")
+    ap.add_argument("--inner-rtol", type=float, default=0.0,
+                    help="mixed form: inner FP32 reduction per refinement step (0 = the library default)")
     ap.add_argument("--precond-order", type=int, default=0,
                     help="von Neumann order of the preconditioner (0 = block-diagonal)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
