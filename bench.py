@@ -114,7 +114,7 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def build_workload(name: str):
+def build_workload(name: str, beams: int = 512):
     from multiscat_b200 import workloads as wl
     if name == "cfg1":
         case = wl.cfg1_case()
@@ -123,7 +123,7 @@ def build_workload(name: str):
         case = wl.cfg0_case()
         return case, [case.system()]
     if name == "cfg2":
-        return wl.cfg2_batch()
+        return wl.cfg2_batch(n_solves=beams)
     raise ValueError(name)
 
 
@@ -197,7 +197,7 @@ def run_b200(args) -> None:
         from multiscat_b200.replicas import max_over_ranks as mor
         return mor(x, device="cuda")
 
-    case, systems = build_workload(args.workload)
+    case, systems = build_workload(args.workload, args.beams)
     nsys = len(systems)
     stream = torch.cuda.current_stream()
     plan = ScatteringPlan(case.v, case.t, systems, rtol=args.rtol, restart=args.restart,
@@ -588,6 +588,9 @@ def main() -> None:
     ap.add_argument("--restart", type=int, default=30)
     ap.add_argument("--inner-restart", type=int, default=0,
                     help="mixed form: inner FP32 restart (0 = the library default)")
+    ap.add_argument("--beams", type=int, default=512,
+                    help="cfg2: beams in the batch (the headline workload is 512; smaller "
+                         "batches are for profiling captures)")
     ap.add_argument("--inner-rtol", type=float, default=0.0,
                     help="mixed form: inner FP32 reduction per refinement step (0 = the library default)")
     ap.add_argument("--precond-order", type=int, default=0,

@@ -885,12 +885,15 @@ __device__ __forceinline__ bool last_block_reduce(const ArnoldiArgs &a, int s, i
     return true;
 }
 
-// P1: h1 = Q^H w.  One warp per basis vector (vectors warp, warp + 8, ...):
-// the warp streams its vector and the block's slice of w (re-read from L1
-// by the other warps) with U loads in flight per thread, two FP64
-// accumulators per thread, a warp sum, then the per-system last-block
-// reduction.  Few registers per thread, so the SM holds enough warps to
-// keep DRAM busy.
+// P1: h1 = Q^H w.  Warps take (basis vector, sub-range) tasks: each vector's
+// slice of the block's row chunk is cut into S sub-ranges, S in {1, 2, 4, 8}
+// chosen so that the 8 warps get the most even share (9 vectors on 8 warps
+// would otherwise leave 7 warps idle while one reads a second vector).  A
+// warp streams its sub-range of the vector and of w (w re-read from L1 by
+// the other warps) with U loads in flight per thread, two FP64 accumulators
+// per thread, then a warp sum; the sub-range sums add up in a fixed order
+// (deterministic) before the per-system last-block reduction.  Few registers
+// per thread, so the SM holds enough warps to keep DRAM busy.
 template <typename R> struct P1Unroll { static constexpr int value = 8; };
 template <> struct P1Unroll<double> { static constexpr int value = 4; };
 
@@ -901,25 +904,41 @@ k_arnoldi_p1(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
 {
     using C2 = typename CT<R>::t;
     constexpr int U = P1Unroll<R>::value;
-    const int tile = blockIdx.x / a.split, sub = blockIdx.x - tile * a.split;
+    constexpr int kSub = 8;
+    __shared__ double2 red[kMaxRestart + 1][kSub];
+    const int tile = blockIdx.x / a.split, sub0 = blockIdx.x - tile * a.split;
     const int s = a.tiles.sys[tile];
     if (a.gate && a.gate[s] == 0) return;
     size_t e0;
     int ne;
-    elem_range<R>(a, tile, sub, e0, ne);
+    elem_range<R>(a, tile, sub0, e0, ne);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    double2 *out = a.partial + (size_t)blockIdx.x * a.pstride;
+    // S minimises the busiest warp's work, ceil(nvec S / nw) / S vector passes
+    int S = 1;
+    {
+        int best = (nvec + nw - 1) / nw * kSub;
+        for (int c = 2; c <= kSub; c *= 2) {
+            const int cost = (nvec * c + nw - 1) / nw * (kSub / c);
+            if (cost < best) {
+                best = cost;
+                S = c;
+            }
+        }
+    }
+    const int per = (ne + S - 1) / S;
     const C2 *w = W + e0;
-    for (int i = warp; i < nvec; i += nw) {
+    for (int t = warp; t < nvec * S; t += nw) {
+        const int i = t / S, sub = t - i * S;
+        const int lo = min(ne, sub * per), hi = min(ne, lo + per);
         const C2 *q = Q + (size_t)i * a.qstride + e0;
         double sr = 0.0, si = 0.0;
-        for (int base = lane; base < ne; base += 32 * U) {
+        for (int base = lo + lane; base < hi; base += 32 * U) {
             C2 qv[U], wv[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int e = base + u * 32;
-                qv[u] = (e < ne) ? q[e] : mk2<R>(0, 0);
-                wv[u] = (e < ne) ? w[e] : mk2<R>(0, 0);
+                qv[u] = (e < hi) ? q[e] : mk2<R>(0, 0);
+                wv[u] = (e < hi) ? w[e] : mk2<R>(0, 0);
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -931,7 +950,17 @@ k_arnoldi_p1(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
         }
         sr = warp_sum(sr);
         si = warp_sum(si);
-        if (lane == 0) out[i] = make_double2(sr, si);
+        if (lane == 0) red[i][sub] = make_double2(sr, si);
+    }
+    __syncthreads();
+    double2 *out = a.partial + (size_t)blockIdx.x * a.pstride;
+    for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
+        double2 acc = red[i][0];
+        for (int sub = 1; sub < S; ++sub) {
+            acc.x += red[i][sub].x;
+            acc.y += red[i][sub].y;
+        }
+        out[i] = acc;
     }
     last_block_reduce(a, s, nvec, h1 + (size_t)s * hstride);
 }
