@@ -572,8 +572,9 @@ k_update(Tiles tiles, const int *__restrict__ gate, int n, const typename CT<R>:
     const R sc = scale ? (R)scale[sys] : R(1);
     const R sg = sum_only ? R(1) : R(-1);     // dst = sc (W - Q c)  or  sc (Q c)
     // Two consecutive elements per step: one 16-byte load per basis vector for
-    // FP32 when the row chunk starts on an even element (n even).
-    const bool pairs = std::is_same<R, float>::value && (e0 % 2 == 0);
+    // FP32 when every vector's chunk starts on an even element (chunk start
+    // and vector stride even; otherwise an odd vector would be misaligned).
+    const bool pairs = std::is_same<R, float>::value && (e0 % 2 == 0) && (qstride % 2 == 0);
     const int step = pairs ? 2 : 1;
     for (int e = (blockIdx.y * blockDim.x + threadIdx.x) * step; e < ne;
          e += gridDim.y * blockDim.x * step) {
@@ -994,8 +995,9 @@ k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
     }
     __syncthreads();
     // w <- w - Q h1, two consecutive elements per step (one 16-byte load per
-    // basis vector for FP32 when the range starts on an even element)
-    const bool pairs = std::is_same<R, float>::value && (e0 % 2 == 0);
+    // basis vector for FP32 when the range start and the vector stride are
+    // even, so that every vector's range is 16-byte aligned)
+    const bool pairs = std::is_same<R, float>::value && (e0 % 2 == 0) && (a.qstride % 2 == 0);
     const int step = pairs ? 2 : 1;
     for (int e = threadIdx.x * step; e < ne; e += blockDim.x * step) {
         const bool two = pairs && e + 1 < ne;

@@ -309,6 +309,20 @@ def test_tensor_core_block_inverse_matches_fp64(which):
     simt.close()
 
 
+def test_mixed_odd_node_count_matches_fp64():
+    """nz = 41 with an odd row total (11 x 11 channels): the FP32 basis vectors
+    then start on odd elements (8-byte aligned only), so the paired 16-byte
+    load paths of the Arnoldi and update kernels must step aside."""
+    case = cfg0_case(nz=41)
+    systems = [case.system()]
+    assert len(systems[0].pkd) * 41 % 2 == 1
+    ref = ScatteringPlan(case.v, case.t, systems).solve().intensities
+    for tc in (True, False):
+        res = ScatteringPlan(case.v, case.t, systems, precision="mixed", tensor_cores=tc).solve()
+        assert (res.status == 0).all(), (tc, res.status)
+        assert float((res.intensities - ref).abs().max()) <= MIXED_TOL
+
+
 @pytest.mark.parametrize("groups,width", [(1, 16), (1, 32), (1, 64), (1, 128),
                                           (2, 16), (2, 32), (2, 64)])
 def test_tensor_core_width_and_warp_groups_match_simt(groups, width, monkeypatch):
