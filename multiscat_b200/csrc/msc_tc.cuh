@@ -31,6 +31,12 @@
 // FP32 near resonances of H0 + pkd and stalls the refinement).  Every mbarrier wait is bounded;
 // on time-out the kernel records an error code, stops issuing work and still
 // releases its TMEM.
+//
+// Warp groups.  With G = 2 the 8 warps form two groups of 4 (each group's
+// warps cover the four TMEM lane quarters and all N columns); each group has
+// its own B buffer, TMEM columns, mbarrier and named barrier and runs its own
+// tile loop (tiles 2 b + g, stride 2 gridDim), so one group's staging and
+// epilogues can overlap the other's MMAs.  G is autotuned with N.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -40,7 +46,7 @@
 namespace msc {
 namespace tc {
 
-constexpr int kThreads = 256;   // 8 warps: warp w reads TMEM lanes 32 (w % 4).., columns half w / 4
+constexpr int kThreads = 256;   // 8 warps: warp w reads TMEM lanes 32 (w % 4)..; G = 1: columns half w / 4
 constexpr long long kSpinLimit = 1ll << 26;   // polls before a wait is declared hung
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
