@@ -914,11 +914,13 @@ k_arnoldi_p1(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
     int ne;
     elem_range<R>(a, tile, sub0, e0, ne);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    // S minimises the busiest warp's work, ceil(nvec S / nw) / S vector passes
+    // S minimises the busiest warp's work, ceil(nvec S / nw) / S vector
+    // passes, among the splits that leave every sub-range at least one full
+    // unrolled warp pass (32 U elements; small chunks keep S = 1)
     int S = 1;
     {
         int best = (nvec + nw - 1) / nw * kSub;
-        for (int c = 2; c <= kSub; c *= 2) {
+        for (int c = 2; c <= kSub && ne >= c * 32 * U; c *= 2) {
             const int cost = (nvec * c + nw - 1) / nw * (kSub / c);
             if (cost < best) {
                 best = cost;
