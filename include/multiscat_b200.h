@@ -125,6 +125,19 @@ msc_status msc_plan_set_system(msc_plan *plan, int32_t s, int32_t n_channels,
                                const double *wave_c, int32_t specular,
                                const double *wave_a_spec);
 
+/* Set systems first .. first + count - 1 in one call (the batched form of
+ * msc_plan_set_system, for sweeps of many beams): the per-channel host arrays
+ * hold the systems one after another, system k's channels at
+ * [offsets[k], offsets[k + 1]) (offsets: count + 1 entries, offsets[0] = 0;
+ * wave_b / wave_c: complex, 2 doubles per channel); specular[k] indexes
+ * within system k; wave_a_spec: count complex values (may be NULL).  Same
+ * checks and error codes as msc_plan_set_system, applied system by system. */
+msc_status msc_plan_set_systems(msc_plan *plan, int32_t first, int32_t count,
+                                const int64_t *offsets, const int32_t *channel_ix,
+                                const int32_t *channel_iy, const double *pkd,
+                                const double *wave_b, const double *wave_c,
+                                const int32_t *specular, const double *wave_a_spec);
+
 /* Solve all systems.  psi_out (device, may be NULL): complex FP64 packed
  * rows [sum_s C_s][n_z] in system order.  intensities_out (device, may be
  * NULL): double [sum_s C_s] = |S_G0|^2.  results (host, may be NULL):

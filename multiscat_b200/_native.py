@@ -23,6 +23,7 @@ EXPORTED = (
     "msc_plan_uses_tensor_cores", "msc_plan_tuning_report", "msc_plan_set_adjoint",
     "msc_plan_is_adjoint", "msc_plan_set_boundary_rhs", "msc_plan_set_adjoint_rhs",
     "msc_potential_gradient", "msc_release_cached_memory", "msc_plan_set_initial_guess",
+    "msc_plan_set_systems",
 )
 
 MSC_OK = 0
@@ -108,6 +109,10 @@ def load() -> ctypes.CDLL:
     lib.msc_plan_set_system.restype = ctypes.c_int
     lib.msc_plan_set_system.argtypes = [_vp, ctypes.c_int32, ctypes.c_int32, _i32p, _i32p, _dp,
                                         _dp, _dp, ctypes.c_int32, _dp]
+    lib.msc_plan_set_systems.restype = ctypes.c_int
+    lib.msc_plan_set_systems.argtypes = [_vp, ctypes.c_int32, ctypes.c_int32,
+                                         ctypes.POINTER(ctypes.c_int64), _i32p, _i32p, _dp, _dp,
+                                         _dp, _i32p, _dp]
     lib.msc_solve.restype = ctypes.c_int
     lib.msc_solve.argtypes = [_vp, _vp, _vp, ctypes.POINTER(Result), _vp]
     lib.msc_plan_total_rows.restype = ctypes.c_int64

@@ -1607,6 +1607,26 @@ msc_status msc_plan_set_system(msc_plan *p, int32_t s, int32_t n_channels, const
     return MSC_OK;
 }
 
+msc_status msc_plan_set_systems(msc_plan *p, int32_t first, int32_t count, const int64_t *offsets,
+                                const int32_t *channel_ix, const int32_t *channel_iy, const double *pkd,
+                                const double *wave_b, const double *wave_c, const int32_t *specular,
+                                const double *wave_a_spec)
+{
+    if (!p || !offsets || !specular) return fail(MSC_ERR_ARG, "null argument");
+    if (count < 0 || first < 0 || (int64_t)first + count > p->B)
+        return fail(MSC_ERR_ARG, "system range out of range");
+    if (offsets[0] != 0) return fail(MSC_ERR_ARG, "offsets[0] must be 0");
+    for (int32_t k = 0; k < count; ++k) {
+        const int64_t lo = offsets[k], hi = offsets[k + 1];
+        if (hi < lo || hi - lo > (int64_t)p->nkx * p->nky) return fail(MSC_ERR_DIMS, "bad channel count");
+        msc_status st = msc_plan_set_system(p, first + k, (int32_t)(hi - lo), channel_ix + lo,
+                                            channel_iy + lo, pkd + lo, wave_b + 2 * lo, wave_c + 2 * lo,
+                                            specular[k], wave_a_spec ? wave_a_spec + 2 * k : nullptr);
+        if (st != MSC_OK) return st;
+    }
+    return MSC_OK;
+}
+
 int64_t msc_plan_total_rows(const msc_plan *p)
 {
     if (!p) return -1;

@@ -30,6 +30,33 @@ def _iptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
 
 
+def _stack_systems(systems: list) -> dict:
+    """The systems' channel arrays concatenated in system order, as the batched
+    msc_plan_set_systems takes them (offsets[k]..offsets[k + 1] is system k)."""
+    if not systems:
+        raise ValueError("a plan needs at least one system")
+    counts = np.fromiter((len(sp.channel_ix) for sp in systems), dtype=np.int64, count=len(systems))
+    offsets = np.zeros(len(systems) + 1, dtype=np.int64)
+    np.cumsum(counts, out=offsets[1:])
+
+    def cat(name, dtype):
+        return np.ascontiguousarray(np.concatenate([getattr(sp, name) for sp in systems], axis=None),
+                                    dtype=dtype)
+
+    return {
+        "offsets": offsets,
+        "ix": cat("channel_ix", np.int32),
+        "iy": cat("channel_iy", np.int32),
+        "pkd": cat("pkd", np.float64),
+        "wb": cat("wave_b", np.complex128),
+        "wc": cat("wave_c", np.complex128),
+        "specular": np.fromiter((int(sp.specular) for sp in systems), dtype=np.int32,
+                                count=len(systems)),
+        "a_spec": np.array([complex(sp.wave_a[sp.specular]) for sp in systems],
+                           dtype=np.complex128),
+    }
+
+
 def run_multiscat_fortran(gmres_preconditioner_flag: int, convergence_significant_figures: int,
                           potential_values, perpendicular_kinetic_difference, wave_a, wave_b,
                           wave_c, parallel_kinetic_energy) -> np.ndarray:
@@ -131,22 +158,16 @@ class ScatteringPlan:
                                                               ctypes.byref(desc)))
         nat.check("msc_plan_set_potential", self._lib.msc_plan_set_potential(
             self._plan, _dptr(v.view(np.float64)), _dptr(t)))
-        offsets = [0]
-        for s, sp in enumerate(systems):
-            ix = np.ascontiguousarray(sp.channel_ix, dtype=np.int32)
-            iy = np.ascontiguousarray(sp.channel_iy, dtype=np.int32)
-            pkd = np.ascontiguousarray(sp.pkd, dtype=np.float64)
-            wb = np.ascontiguousarray(sp.wave_b, dtype=np.complex128)
-            wc = np.ascontiguousarray(sp.wave_c, dtype=np.complex128)
-            asp = np.array([complex(sp.wave_a[sp.specular]).real,
-                            complex(sp.wave_a[sp.specular]).imag])
-            nat.check("msc_plan_set_system", self._lib.msc_plan_set_system(
-                self._plan, s, ix.size, _iptr(ix), _iptr(iy), _dptr(pkd),
-                _dptr(wb.view(np.float64)), _dptr(wc.view(np.float64)), int(sp.specular),
-                _dptr(asp)))
-            offsets.append(offsets[-1] + ix.size)
-        self.row_offsets = np.asarray(offsets)
-        self.total_rows = int(offsets[-1])
+        # every system in one call: per-channel arrays concatenated in system
+        # order (converting pointers system by system costs ~25 us per beam)
+        sa = _stack_systems(systems)
+        nat.check("msc_plan_set_systems", self._lib.msc_plan_set_systems(
+            self._plan, 0, len(systems), sa["offsets"].ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            _iptr(sa["ix"]), _iptr(sa["iy"]), _dptr(sa["pkd"]), _dptr(sa["wb"].view(np.float64)),
+            _dptr(sa["wc"].view(np.float64)), _iptr(sa["specular"]),
+            _dptr(sa["a_spec"].view(np.float64))))
+        self.row_offsets = sa["offsets"].copy()
+        self.total_rows = int(sa["offsets"][-1])
 
     def close(self) -> None:
         if getattr(self, "_plan", None) and self._plan.value:

@@ -114,3 +114,27 @@ def test_scattering_matrix_from_state_is_the_boundary_formula():
                               np.asarray(wb).ravel()).reshape(nkx, nky)
     np.testing.assert_allclose(got.real, want, rtol=1e-12, atol=0)
     assert float(np.abs(got.imag).max()) == 0.0
+
+
+def test_stacked_systems_match_the_per_system_arrays():
+    """The batched msc_plan_set_systems input: system k's channels at
+    offsets[k]..offsets[k + 1] of every concatenated array, C-ABI dtypes."""
+    from multiscat_b200.solver import _stack_systems
+    from multiscat_b200.workloads import cfg0_case, cfg2_batch
+    systems = cfg2_batch(n_solves=3, seed=5)[1] + [cfg0_case(nz=20).system()]
+    sa = _stack_systems(systems)
+    off = sa["offsets"]
+    assert off.dtype == np.int64 and off[0] == 0 and off.size == len(systems) + 1
+    assert sa["ix"].dtype == np.int32 and sa["iy"].dtype == np.int32
+    assert sa["specular"].dtype == np.int32 and sa["wb"].dtype == np.complex128
+    for k, sp in enumerate(systems):
+        sl = slice(off[k], off[k + 1])
+        np.testing.assert_array_equal(sa["ix"][sl], sp.channel_ix)
+        np.testing.assert_array_equal(sa["iy"][sl], sp.channel_iy)
+        np.testing.assert_array_equal(sa["pkd"][sl], sp.pkd)
+        np.testing.assert_array_equal(sa["wb"][sl], sp.wave_b)
+        np.testing.assert_array_equal(sa["wc"][sl], sp.wave_c)
+        assert sa["specular"][k] == sp.specular
+        assert sa["a_spec"][k] == sp.wave_a[sp.specular]
+    with pytest.raises(ValueError):
+        _stack_systems([])
