@@ -123,31 +123,78 @@ class NaturalArrays:
     weights: np.ndarray
 
 
-def natural_arrays(condition: ScatteringCondition) -> NaturalArrays:
-    """Convert to hbar = 1, m = 1/2, Angstrom (``_multiscat.py:102-128``) and build arrays."""
-    u = condition.units
-    to_ang = 1.0 / u.angstrom                                   # length unit -> Angstrom
-    energy_to_nat = 2.0 * condition.mass / u.hbar**2 * u.angstrom**2   # energy -> 1/A^2
+def _lattice_frame(condition: ScatteringCondition):
+    """Lattice vectors (a1 along x) and z domain of a condition, in Angstrom.
+
+    Incident k is read in the lattice frame: rotating both lattice vectors
+    leaves the result unchanged, as the reference's
+    tests/test_fixed_example.py:259-330 requires."""
+    to_ang = 1.0 / condition.units.angstrom                     # length unit -> Angstrom
     md = condition.metadata
-    nkx, nky, nz = md.shape
     a1 = np.asarray(md.vectors[0], float)[:2] * to_ang
     a2 = np.asarray(md.vectors[1], float)[:2] * to_ang
-    # Incident k is read in the lattice frame (a1 along x): rotating both
-    # lattice vectors leaves the result unchanged, as the reference's
-    # tests/test_fixed_example.py:259-330 requires.
     rot = math.atan2(a1[1], a1[0])
     cr, sr = math.cos(rot), math.sin(rot)
     unrot = np.array([[cr, sr], [-sr, cr]])
-    a1, a2 = unrot @ a1, unrot @ a2
-    z0 = md.z_start * to_ang
-    dz = md.z_delta * to_ang
-    k = tuple(float(c) * u.angstrom for c in condition.incident_k)
-    nodes, weights = sa.lobatto_rule(z0, z0 + dz, nz)
-    kinetic = sa.kinetic_matrix(nodes, weights)
+    return unrot @ a1, unrot @ a2, md.z_start * to_ang, md.z_delta * to_ang
+
+
+def _beam_arrays(condition: ScatteringCondition, a1, a2, weights, z0: float, dz: float):
+    """pkd and the boundary waves (a, b, c) of one beam on a built grid."""
+    nkx, nky, _ = condition.metadata.shape
+    k = tuple(float(c) * condition.units.angstrom for c in condition.incident_k)
     pkd = sa.perpendicular_kinetic_difference(k, a1, a2, nkx, nky)
     wa, wb, wc = sa.waves(pkd, weights, z0, dz)
+    return pkd, wa, wb, wc
+
+
+def natural_arrays(condition: ScatteringCondition) -> NaturalArrays:
+    """Convert to hbar = 1, m = 1/2, Angstrom (``_multiscat.py:102-128``) and build arrays."""
+    u = condition.units
+    energy_to_nat = 2.0 * condition.mass / u.hbar**2 * u.angstrom**2   # energy -> 1/A^2
+    nkx, nky, nz = condition.metadata.shape
+    a1, a2, z0, dz = _lattice_frame(condition)
+    nodes, weights = sa.lobatto_rule(z0, z0 + dz, nz)
+    kinetic = sa.kinetic_matrix(nodes, weights)
+    pkd, wa, wb, wc = _beam_arrays(condition, a1, a2, weights, z0, dz)
     v = np.asarray(condition.potential_values, np.complex128).reshape(nkx, nky, nz) * energy_to_nat
     return NaturalArrays(v, kinetic, pkd, wa, wb, wc, nodes, weights)
+
+
+def _shares_grid(c: ScatteringCondition, c0: ScatteringCondition) -> bool:
+    """Same potential, grid, units and mass (so the same natural-unit potential
+    and kinetic matrix serve both)."""
+    m, m0 = c.metadata, c0.metadata
+    if (tuple(m.shape) != tuple(m0.shape) or m.z_start != m0.z_start or m.z_delta != m0.z_delta
+            or c.units != c0.units or c.mass != c0.mass):
+        return False
+    if not all(np.array_equal(np.asarray(x, float), np.asarray(y, float))
+               for x, y in zip(m.vectors, m0.vectors)):
+        return False
+    return c.potential_values is c0.potential_values or np.array_equal(
+        np.asarray(c.potential_values), np.asarray(c0.potential_values))
+
+
+def _sweep_systems(conditions: Sequence[ScatteringCondition], config: OptimizationConfig):
+    """(natural arrays of the first condition, one system per condition).
+
+    The grid, the kinetic matrix and the potential are built once; each
+    further beam only needs its pkd and boundary waves (the per-condition
+    grid build took ~4 ms, 2 s for a 512-beam sweep)."""
+    if not conditions:
+        raise ValueError("no conditions")
+    c0 = conditions[0]
+    grid = natural_arrays(c0)
+    a1, a2, z0, dz = _lattice_frame(c0)
+    systems = [_system_for(grid, config)]
+    for i, c in enumerate(conditions[1:], start=1):
+        if not _shares_grid(c, c0):
+            raise ValueError(f"condition {i} does not share condition 0's potential, grid, "
+                             "units and mass (a batched sweep solves one potential)")
+        pkd, wa, wb, wc = _beam_arrays(c, a1, a2, grid.weights, z0, dz)
+        systems.append(_system_for(NaturalArrays(grid.potential_values, grid.kinetic, pkd, wa, wb,
+                                                 wc, grid.nodes, grid.weights), config))
+    return grid, systems
 
 
 def _system_for(arr: NaturalArrays, config: OptimizationConfig):
@@ -249,10 +296,10 @@ def get_scattering_matrix_from_state(state: np.ndarray,
 
 def get_scattering_matrices(conditions: Sequence[ScatteringCondition],
                             config: OptimizationConfig) -> list[np.ndarray]:
-    """Batched sweep: many beams over ONE potential and grid, one GPU solve."""
-    arrays = [natural_arrays(c) for c in conditions]
-    systems = [_system_for(a, config) for a in arrays]
-    plan = ScatteringPlan(arrays[0].potential_values, arrays[0].kinetic, systems,
+    """Batched sweep: many beams over ONE potential and grid, one GPU solve
+    (every condition must share condition 0's potential, grid, units and mass)."""
+    grid, systems = _sweep_systems(conditions, config)
+    plan = ScatteringPlan(grid.potential_values, grid.kinetic, systems,
                           rtol=config.residual_tolerance, restart=config.restart,
                           max_iterations=config.max_iterations,
                           precision=config.precision_mode)

@@ -143,6 +143,22 @@ def _read_wolken_golden():
     return out
 
 
+def test_batched_sweep_matches_single_beam_calls():
+    """get_scattering_matrices (one plan, grid built once) against
+    get_scattering_matrix per beam, three incidence angles of the He-LiF case."""
+    from multiscat_b200 import get_scattering_matrices
+    base = _wolken_condition(0.0)
+    conds = [ScatteringCondition.from_angles(
+        mass=sa.ALPHA_PARTICLE_MASS, theta=math.radians(th), phi=math.radians(ph),
+        energy=20e-3 * sa.ELECTRON_VOLT, potential_values=base.potential_values,
+        metadata=base.metadata) for th, ph in ((30.0, 0.0), (20.0, 10.0), (40.0, 5.0))]
+    cfg = OptimizationConfig(precision=1e-7, max_iterations=1000)
+    batch = get_scattering_matrices(conds, cfg)
+    for c, got in zip(conds, batch):
+        want = get_scattering_matrix(c, cfg)
+        np.testing.assert_allclose(got.real, want.real, rtol=0.0, atol=1e-9)
+
+
 @pytest.mark.parametrize("rotation", [0.0, 20.0])
 def test_api_reproduces_reference_golden(rotation):
     """tests/test_fixed_example.py:233-256 and :307-330 on the B200 API."""

@@ -138,3 +138,47 @@ def test_stacked_systems_match_the_per_system_arrays():
         assert sa["a_spec"][k] == sp.wave_a[sp.specular]
     with pytest.raises(ValueError):
         _stack_systems([])
+
+
+def _sweep_conditions(n: int, nz: int = 40):
+    from multiscat_b200.api import ScatteringCondition, ScatteringMetadata
+    nodes, _ = inputs.lobatto_rule(0.0, 8.0, nz)
+    v = inputs.wolken_potential(nodes, 10, 10) * sa.MEV
+    md = ScatteringMetadata(vectors=(np.array([2.84e-10, 0.0]), np.array([0.0, 2.84e-10])),
+                            shape=(10, 10, nz), z_delta=8e-10)
+    return [ScatteringCondition.from_angles(
+        mass=sa.ALPHA_PARTICLE_MASS, theta=math.radians(5.0 + 7.0 * i),
+        phi=math.radians(3.0 * i), energy=(20.0 + i) * 1e-3 * sa.ELECTRON_VOLT,
+        potential_values=v, metadata=md) for i in range(n)]
+
+
+@pytest.mark.parametrize("n_channels", [None, 37])
+def test_sweep_systems_match_per_condition_build(n_channels):
+    """get_scattering_matrices builds the grid once: every beam's system must
+    equal the one the per-condition path (natural_arrays) gives."""
+    from multiscat_b200.api import (OptimizationConfig, _sweep_systems, _system_for,
+                                    natural_arrays)
+    conds = _sweep_conditions(6)
+    cfg = OptimizationConfig(n_channels=n_channels)
+    grid, systems = _sweep_systems(conds, cfg)
+    ref0 = natural_arrays(conds[0])
+    np.testing.assert_array_equal(grid.kinetic, ref0.kinetic)
+    np.testing.assert_array_equal(grid.potential_values, ref0.potential_values)
+    for c, got in zip(conds, systems):
+        want = _system_for(natural_arrays(c), cfg)
+        for name in ("channel_ix", "channel_iy", "pkd", "wave_a", "wave_b", "wave_c"):
+            np.testing.assert_array_equal(getattr(got, name), getattr(want, name))
+        assert got.specular == want.specular
+
+
+def test_sweep_rejects_conditions_on_another_grid():
+    import dataclasses
+
+    from multiscat_b200.api import OptimizationConfig, _sweep_systems
+    conds = _sweep_conditions(3)
+    other = dataclasses.replace(conds[2], mass=conds[2].mass * 2.0)
+    with pytest.raises(ValueError):
+        _sweep_systems([conds[0], conds[1], other], OptimizationConfig())
+    shifted = dataclasses.replace(conds[1], potential_values=conds[1].potential_values * 1.5)
+    with pytest.raises(ValueError):
+        _sweep_systems([conds[0], shifted], OptimizationConfig())
