@@ -204,9 +204,14 @@ def _system_for(arr: NaturalArrays, config: OptimizationConfig):
     return full_grid_system(arr.pkd, arr.wave_a, arr.wave_b, arr.wave_c)
 
 
-def _to_grid(result: SolveResult, s: int, system, shape) -> np.ndarray:
+def _to_grid(result: SolveResult, s: int, system, shape, host_intensities=None) -> np.ndarray:
+    """System s's |S|^2 on the (nkx, nky) channel grid; `host_intensities` (all
+    rows, already on the host) saves one device read per system in sweeps."""
     out = np.zeros(shape, np.complex128)
-    vals = result.system_intensities(s).detach().cpu().numpy()
+    if host_intensities is None:
+        vals = result.system_intensities(s).detach().cpu().numpy()
+    else:
+        vals = host_intensities[result.row_offsets[s]:result.row_offsets[s + 1]]
     out[system.channel_ix, system.channel_iy] = vals
     return out
 
@@ -310,5 +315,6 @@ def get_scattering_matrices(conditions: Sequence[ScatteringCondition],
     bad = np.nonzero(result.status != 0)[0]
     if bad.size:
         raise RuntimeError(f"B200 GMRES did not converge for systems {bad.tolist()}")
-    return [_to_grid(result, s, systems[s], c.metadata.shape[:2])
+    host = result.intensities.detach().cpu().numpy()
+    return [_to_grid(result, s, systems[s], c.metadata.shape[:2], host)
             for s, c in enumerate(conditions)]

@@ -182,3 +182,24 @@ def test_sweep_rejects_conditions_on_another_grid():
     shifted = dataclasses.replace(conds[1], potential_values=conds[1].potential_values * 1.5)
     with pytest.raises(ValueError):
         _sweep_systems([conds[0], shifted], OptimizationConfig())
+
+
+def test_to_grid_from_host_intensities_matches_per_system_read():
+    """Sweeps read all intensities once and slice them per system."""
+    import torch
+
+    from multiscat_b200.api import OptimizationConfig, _sweep_systems, _to_grid
+    from multiscat_b200.solver import SolveResult
+    conds = _sweep_conditions(3)
+    _, systems = _sweep_systems(conds, OptimizationConfig(n_channels=30))
+    offsets = np.concatenate([[0], np.cumsum([len(sp.pkd) for sp in systems])])
+    inten = torch.rand(int(offsets[-1]), dtype=torch.float64)
+    res = SolveResult(psi=torch.zeros(0), intensities=inten, row_offsets=offsets,
+                      iterations=np.zeros(3), cycles=np.zeros(3), status=np.zeros(3),
+                      residual=np.zeros(3))
+    host = inten.numpy()
+    for s, sp in enumerate(systems):
+        a = _to_grid(res, s, sp, (10, 10))
+        b = _to_grid(res, s, sp, (10, 10), host)
+        np.testing.assert_array_equal(a, b)
+        assert np.count_nonzero(a) == len(sp.pkd)
