@@ -14,6 +14,7 @@ complex128, exactly as the reference's array does (``_multiscat.py:166-175``).
 from __future__ import annotations
 
 import math
+from collections import OrderedDict
 from dataclasses import dataclass, field
 from typing import Literal, Sequence
 
@@ -148,14 +149,35 @@ def _beam_arrays(condition: ScatteringCondition, a1, a2, weights, z0: float, dz:
     return pkd, wa, wb, wc
 
 
+_GRID_CACHE: "OrderedDict[tuple, tuple]" = OrderedDict()
+_GRID_CACHE_SIZE = 8
+
+
+def _lobatto_grid(z_min: float, z_max: float, n: int):
+    """(nodes, weights, kinetic matrix) of the n-point Lobatto grid, cached by
+    (z_min, z_max, n): one condition after another on the same grid (the
+    reference's usual loop) rebuilds nothing (n = 550: ~30 ms saved per call).
+    Returns copies, so callers may modify them."""
+    key = (float(z_min), float(z_max), int(n))
+    hit = _GRID_CACHE.get(key)
+    if hit is None:
+        nodes, weights = sa.lobatto_rule(z_min, z_max, n)
+        hit = (nodes, weights, sa.kinetic_matrix(nodes, weights))
+        _GRID_CACHE[key] = hit
+        while len(_GRID_CACHE) > _GRID_CACHE_SIZE:
+            _GRID_CACHE.popitem(last=False)
+    else:
+        _GRID_CACHE.move_to_end(key)
+    return tuple(a.copy() for a in hit)
+
+
 def natural_arrays(condition: ScatteringCondition) -> NaturalArrays:
     """Convert to hbar = 1, m = 1/2, Angstrom (``_multiscat.py:102-128``) and build arrays."""
     u = condition.units
     energy_to_nat = 2.0 * condition.mass / u.hbar**2 * u.angstrom**2   # energy -> 1/A^2
     nkx, nky, nz = condition.metadata.shape
     a1, a2, z0, dz = _lattice_frame(condition)
-    nodes, weights = sa.lobatto_rule(z0, z0 + dz, nz)
-    kinetic = sa.kinetic_matrix(nodes, weights)
+    nodes, weights, kinetic = _lobatto_grid(z0, z0 + dz, nz)
     pkd, wa, wb, wc = _beam_arrays(condition, a1, a2, weights, z0, dz)
     v = np.asarray(condition.potential_values, np.complex128).reshape(nkx, nky, nz) * energy_to_nat
     return NaturalArrays(v, kinetic, pkd, wa, wb, wc, nodes, weights)

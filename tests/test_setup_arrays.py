@@ -203,3 +203,21 @@ def test_to_grid_from_host_intensities_matches_per_system_read():
         b = _to_grid(res, s, sp, (10, 10), host)
         np.testing.assert_array_equal(a, b)
         assert np.count_nonzero(a) == len(sp.pkd)
+
+
+def test_lobatto_grid_cache_returns_fresh_copies_of_the_same_grid():
+    from multiscat_b200 import api
+    a = api._lobatto_grid(-1.5, 10.0, 33)
+    b = api._lobatto_grid(-1.5, 10.0, 33)
+    x, w = sa.lobatto_rule(-1.5, 10.0, 33)
+    np.testing.assert_array_equal(a[0], x)
+    np.testing.assert_array_equal(a[1], w)
+    np.testing.assert_array_equal(a[2], sa.kinetic_matrix(x, w))
+    for p, q in zip(a, b):
+        np.testing.assert_array_equal(p, q)
+        assert p is not q
+    a[2][0, 0] = 1e9                      # a caller's change does not reach the cache
+    assert api._lobatto_grid(-1.5, 10.0, 33)[2][0, 0] == b[2][0, 0]
+    for n in range(2, 2 + api._GRID_CACHE_SIZE + 3):
+        api._lobatto_grid(0.0, 1.0, n)
+    assert len(api._GRID_CACHE) <= api._GRID_CACHE_SIZE
