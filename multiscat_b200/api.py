@@ -239,10 +239,15 @@ def _to_grid(result: SolveResult, s: int, system, shape, host_intensities=None) 
 
 
 def get_scattering_matrix(condition: ScatteringCondition, config: OptimizationConfig, *,
-                          backend: Literal["b200"] = "b200") -> np.ndarray:
-    """|S_G0|^2 on the (nkx, nky) channel grid, complex128 (``_multiscat.py:131-175``)."""
-    if backend != "b200":
-        raise ValueError(f"Unknown backend '{backend}'. Expected 'b200'.")
+                          backend: Literal["b200", "fortran", "scipy"] = "b200") -> np.ndarray:
+    """|S_G0|^2 on the (nkx, nky) channel grid, complex128 (``_multiscat.py:131-175``).
+
+    The reference's backend names ("fortran", its default, and "scipy") are
+    accepted so that calls that name one keep working; all three run the B200
+    solve (the reference's backends differ only in the preconditioner, and
+    the converged intensities agree within the configured precision)."""
+    if backend not in ("b200", "fortran", "scipy"):
+        raise ValueError(f"Unknown backend '{backend}'. Expected 'b200', 'fortran' or 'scipy'.")
     return _single_solve(condition, config, order=0)
 
 

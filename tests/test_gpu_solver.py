@@ -159,11 +159,14 @@ def test_batched_sweep_matches_single_beam_calls():
         np.testing.assert_allclose(got.real, want.real, rtol=0.0, atol=1e-9)
 
 
-@pytest.mark.parametrize("rotation", [0.0, 20.0])
-def test_api_reproduces_reference_golden(rotation):
-    """tests/test_fixed_example.py:233-256 and :307-330 on the B200 API."""
+@pytest.mark.parametrize("rotation,backend", [(0.0, "b200"), (20.0, "b200"), (0.0, "fortran"),
+                                              (0.0, "scipy")])
+def test_api_reproduces_reference_golden(rotation, backend):
+    """tests/test_fixed_example.py:233-256 and :307-330 on the B200 API (the
+    reference's backend names run the same solve)."""
     s = get_scattering_matrix(_wolken_condition(rotation),
-                              OptimizationConfig(precision=1e-5, max_iterations=1000))
+                              OptimizationConfig(precision=1e-5, max_iterations=1000),
+                              backend=backend)
     assert s.dtype == np.complex128 and s.shape == (10, 10)
     inten = np.real_if_close(s)
     assert math.isclose(float(np.sum(inten).real), 1.0, abs_tol=1e-6)

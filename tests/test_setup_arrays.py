@@ -221,3 +221,9 @@ def test_lobatto_grid_cache_returns_fresh_copies_of_the_same_grid():
     for n in range(2, 2 + api._GRID_CACHE_SIZE + 3):
         api._lobatto_grid(0.0, 1.0, n)
     assert len(api._GRID_CACHE) <= api._GRID_CACHE_SIZE
+
+
+def test_unknown_backend_is_rejected_before_any_solve():
+    from multiscat_b200.api import OptimizationConfig, get_scattering_matrix
+    with pytest.raises(ValueError, match="Unknown backend"):
+        get_scattering_matrix(_sweep_conditions(1)[0], OptimizationConfig(), backend="cuda")
