@@ -57,12 +57,26 @@ class UnitSystem:
     atomic_mass: float = sa.ATOMIC_MASS
     angstrom: float = sa.ANGSTROM
 
+    @classmethod
+    def si(cls) -> "UnitSystem":
+        """The SI units (``config.py:69-72``)."""
+        return cls()
+
     @property
     def kinetic_energy_unit(self) -> float:
         return self.hbar**2 / (2 * self.atomic_mass * self.angstrom**2)
 
+    @property
+    def electron_volt(self) -> float:
+        """The reference's definition (``config.py:79-84``):
+        eV_SI * (kinetic_energy_unit of SI / kinetic_energy_unit of this system),
+        kept as is for drop-in parity.  It is 1.602e-19 for SI; for other
+        systems it is the inverse of the factor `with_units` applies to
+        energies, and the reference itself never reads it."""
+        return sa.ELECTRON_VOLT * (UnitSystem().kinetic_energy_unit / self.kinetic_energy_unit)
 
-SI_UNITS = UnitSystem()
+
+SI_UNITS = UnitSystem.si()
 
 
 @dataclass
@@ -108,6 +122,51 @@ class ScatteringCondition:
     def incident_energy(self) -> float:
         k2 = sum(k * k for k in self.incident_k)
         return self.units.hbar**2 * k2 / (2 * self.mass)
+
+    @property
+    def theta(self) -> float:
+        """Polar angle of the incident wavevector (radians, ``config.py:186-190``)."""
+        kx, ky, kz = self.incident_k
+        return float(np.arccos(kz / np.sqrt(kx * kx + ky * ky + kz * kz)))
+
+    @property
+    def phi(self) -> float:
+        """Azimuth of the incident wavevector (radians, ``config.py:192-196``)."""
+        kx, ky, _ = self.incident_k
+        return float(np.arctan2(ky, kx))
+
+    def with_units(self, units: UnitSystem) -> "ScatteringCondition":
+        """The same condition expressed in another unit system
+        (``config.py:198-200, 230-296``): masses scale with the atomic mass
+        unit, lengths with the angstrom, wavevectors inversely, and the
+        potential values with the kinetic-energy unit."""
+        mass_factor = units.atomic_mass / self.units.atomic_mass
+        length_factor = units.angstrom / self.units.angstrom
+        energy_factor = units.kinetic_energy_unit / self.units.kinetic_energy_unit
+        md = self.metadata
+        metadata = ScatteringMetadata(
+            vectors=tuple(np.asarray(v, float) * length_factor for v in md.vectors),
+            shape=tuple(md.shape), z_delta=md.z_delta * length_factor,
+            z_start=md.z_start * length_factor)
+        return ScatteringCondition(self.mass * mass_factor,
+                                   tuple(float(k) / length_factor for k in self.incident_k),
+                                   np.asarray(self.potential_values) * energy_factor, metadata,
+                                   units)
+
+    def __eq__(self, other: object) -> bool:
+        """Same mass, incident k, potential, grid and units (``config.py:202-210``)."""
+        if not isinstance(other, ScatteringCondition):
+            return False
+        m, o = self.metadata, other.metadata
+        return (self.mass == other.mass and tuple(self.incident_k) == tuple(other.incident_k)
+                and self.units == other.units and tuple(m.shape) == tuple(o.shape)
+                and m.z_start == o.z_start and m.z_delta == o.z_delta
+                and all(np.array_equal(np.asarray(a, float), np.asarray(b, float))
+                        for a, b in zip(m.vectors, o.vectors))
+                and np.array_equal(np.asarray(self.potential_values),
+                                   np.asarray(other.potential_values)))
+
+    __hash__ = None
 
 
 @dataclass

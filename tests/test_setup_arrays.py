@@ -227,3 +227,30 @@ def test_unknown_backend_is_rejected_before_any_solve():
     from multiscat_b200.api import OptimizationConfig, get_scattering_matrix
     with pytest.raises(ValueError, match="Unknown backend"):
         get_scattering_matrix(_sweep_conditions(1)[0], OptimizationConfig(), backend="cuda")
+
+
+def test_unit_system_and_condition_helpers():
+    """UnitSystem.si / electron_volt and ScatteringCondition.theta / phi /
+    with_units / == (config.py:61-84, 180-296)."""
+    from multiscat_b200.api import UnitSystem, natural_arrays
+    si = UnitSystem.si()
+    assert si == UnitSystem() and math.isclose(si.electron_volt, sa.ELECTRON_VOLT, rel_tol=1e-15)
+    nat_units = UnitSystem(hbar=1.0, atomic_mass=1.0, angstrom=1.0)
+    # the reference's definition, eV_SI * keu_SI / keu
+    assert math.isclose(nat_units.electron_volt,
+                        sa.ELECTRON_VOLT * si.kinetic_energy_unit / 0.5, rel_tol=1e-12)
+    energy_factor = nat_units.kinetic_energy_unit / si.kinetic_energy_unit
+    c = _sweep_conditions(4)[3]
+    assert math.isclose(c.theta, math.radians(26.0), rel_tol=1e-12)
+    assert math.isclose(c.phi, math.radians(9.0), rel_tol=1e-12)
+    other = c.with_units(nat_units)
+    assert other.units == nat_units and other != c
+    assert math.isclose(other.theta, c.theta, rel_tol=1e-12)
+    assert math.isclose(other.incident_energy, c.incident_energy * energy_factor, rel_tol=1e-12)
+    a, b = natural_arrays(c), natural_arrays(other)
+    for name in ("potential_values", "kinetic", "pkd", "wave_a", "wave_b", "wave_c", "nodes"):
+        np.testing.assert_allclose(getattr(b, name), getattr(a, name), rtol=1e-9,
+                                   atol=1e-12 * np.abs(getattr(a, name)).max())
+    back = other.with_units(si)
+    assert math.isclose(back.mass, c.mass, rel_tol=1e-15)
+    assert c == _sweep_conditions(4)[3]
