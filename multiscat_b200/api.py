@@ -21,7 +21,8 @@ from typing import Literal, Sequence
 import numpy as np
 
 from . import setup_arrays as sa
-from .solver import ScatteringPlan, SolveResult, channel_subset_system, full_grid_system
+from .solver import (ScatteringPlan, SolveResult, beam_systems, channel_subset_system,
+                     full_grid_system)
 
 
 @dataclass(frozen=True, kw_only=True)
@@ -267,14 +268,18 @@ def _sweep_systems(conditions: Sequence[ScatteringCondition], config: Optimizati
     c0 = conditions[0]
     grid = natural_arrays(c0)
     a1, a2, z0, dz = _lattice_frame(c0)
-    systems = [_system_for(grid, config)]
     for i, c in enumerate(conditions[1:], start=1):
         if not _shares_grid(c, c0):
             raise ValueError(f"condition {i} does not share condition 0's potential, grid, "
                              "units and mass (a batched sweep solves one potential)")
-        pkd, wa, wb, wc = _beam_arrays(c, a1, a2, grid.weights, z0, dz)
-        systems.append(_system_for(NaturalArrays(grid.potential_values, grid.kinetic, pkd, wa, wb,
-                                                 wc, grid.nodes, grid.weights), config))
+    # every beam's pkd at once, waves for the kept channels only (the same
+    # element-wise arithmetic as _beam_arrays)
+    nkx, nky, _ = c0.metadata.shape
+    ang = c0.units.angstrom
+    ks = np.array([[float(k) * ang for k in c.incident_k] for c in conditions])
+    pkd = sa.perpendicular_kinetic_difference_batch(ks, a1, a2, nkx, nky)
+    systems = beam_systems(pkd, lambda e: sa.waves(e, grid.weights, z0, dz),
+                           n_channels=config.n_channels)
     return grid, systems
 
 

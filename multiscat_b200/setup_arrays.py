@@ -147,6 +147,19 @@ def waves(pkd: np.ndarray, weights: np.ndarray, z_start: float, z_delta: float):
     return a, b, c
 
 
+def perpendicular_kinetic_difference_batch(incident_ks, a1, a2, nkx: int, nky: int) -> np.ndarray:
+    """pkd of many beams at once, [B, nkx, nky]: element for element the same
+    arithmetic as ``perpendicular_kinetic_difference`` (identical results)."""
+    b1, b2 = reciprocal_vectors(a1, a2)
+    ks = np.asarray(incident_ks, float).reshape(-1, 3)
+    mx = fft_modes(nkx)[None, :, None]
+    my = fft_modes(nky)[None, None, :]
+    gx = ks[:, 0, None, None] + mx * b1[0] + my * b2[0]
+    gy = ks[:, 1, None, None] + mx * b1[1] + my * b2[1]
+    kk = np.array([float(k @ k) for k in ks])
+    return gx * gx + gy * gy - kk[:, None, None]
+
+
 def momentum_from_angles(energy_mev: float, theta: float, phi: float, factor: float):
     """Incident k (1/A) for an energy in meV and angles in radians."""
     k = math.sqrt(factor * energy_mev)

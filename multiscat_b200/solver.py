@@ -349,6 +349,46 @@ def _device_rows(t, dtype, rows: int) -> torch.Tensor:
     return t
 
 
+def beam_systems(pkd, waves, n_channels: int | None = None,
+                 max_pkd: float | None = None) -> list[SystemSpec]:
+    """One system per beam from batched pkd [B, nkx, nky]: ``full_grid_system``
+    when neither ``n_channels`` nor ``max_pkd`` is given, else
+    ``channel_subset_system``, beam by beam, with the sort and gathers done for
+    all beams at once.  ``waves(e) -> (a, b, c)`` maps pkd values (1-D) to the
+    boundary waves element by element (``setup_arrays.waves``); it runs on the
+    kept channels only, so the results equal the per-beam builders'."""
+    pkd = np.asarray(pkd, float)
+    nb, nkx, nky = pkd.shape
+    flat = pkd.reshape(nb, -1)
+    if n_channels is None and max_pkd is None:
+        ix, iy = np.meshgrid(np.arange(nkx), np.arange(nky), indexing="ij")
+        ix = ix.ravel().astype(np.int32)
+        iy = iy.ravel().astype(np.int32)
+        wa, wb, wc = (np.asarray(w, complex).reshape(nb, -1) for w in waves(flat.ravel()))
+        return [SystemSpec(ix.copy(), iy.copy(), flat[b], wa[b], wb[b], wc[b], 0) for b in range(nb)]
+    order = np.argsort(flat, axis=1, kind="stable")
+    if n_channels is not None:
+        order = order[:, :n_channels]
+    spd = np.take_along_axis(flat, order, axis=1)
+    keep = np.full(nb, order.shape[1]) if max_pkd is None else (spd <= max_pkd).sum(axis=1)
+    mask = np.arange(order.shape[1])[None, :] < keep[:, None]
+    kept = spd[mask]                                  # kept channels, beam after beam
+    wa, wb, wc = (np.asarray(w, complex) for w in waves(kept))
+    ix, iy = np.unravel_index(order, (nkx, nky))
+    out = []
+    pos = 0
+    for b in range(nb):
+        k = int(keep[b])
+        spec = np.nonzero(order[b, :k] == 0)[0]
+        if spec.size == 0:
+            raise ValueError(f"beam {b}: the specular channel is not in the kept channel set")
+        sl = slice(pos, pos + k)
+        out.append(SystemSpec(ix[b, :k].astype(np.int32), iy[b, :k].astype(np.int32), kept[sl],
+                              wa[sl], wb[sl], wc[sl], int(spec[0])))
+        pos += k
+    return out
+
+
 def full_grid_system(pkd, wave_a, wave_b, wave_c) -> SystemSpec:
     """All nkx*nky channels in the reference's row-major (ix, iy) order."""
     pkd = np.asarray(pkd, float)
