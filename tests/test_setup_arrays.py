@@ -254,3 +254,30 @@ def test_unit_system_and_condition_helpers():
     back = other.with_units(si)
     assert math.isclose(back.mass, c.mass, rel_tol=1e-15)
     assert c == _sweep_conditions(4)[3]
+
+
+@pytest.mark.parametrize("mode", ["max_pkd", "n_channels", "full"])
+def test_beam_systems_match_per_beam_builders(mode):
+    """solver.beam_systems (all beams at once, waves for kept channels only)
+    against channel_subset_system / full_grid_system beam by beam."""
+    from multiscat_b200.solver import beam_systems, channel_subset_system, full_grid_system
+    fac = sa.natural_units_factor(sa.HE4_MASS)
+    a1, a2 = np.array([2.54, 0.0]), np.array([0.0, 2.54])
+    x, w = sa.lobatto_rule(-1.5, 10.0, 50)
+    rng = np.random.default_rng(9)
+    ks = [sa.momentum_from_angles(e, th, ph, fac) for e, th, ph in
+          zip(rng.uniform(8, 64, 12), np.radians(rng.uniform(0, 60, 12)),
+              np.radians(rng.uniform(0, 45, 12)))]
+    pkd = sa.perpendicular_kinetic_difference_batch(ks, a1, a2, 16, 16)
+    kw = {"max_pkd": {"max_pkd": fac * 120.0}, "n_channels": {"n_channels": 57}, "full": {}}[mode]
+    got = beam_systems(pkd, lambda e: sa.waves(e, w, -1.5, 11.5), **kw)
+    for k, sp in zip(ks, got):
+        p1 = sa.perpendicular_kinetic_difference(k, a1, a2, 16, 16)
+        wa, wb, wc = sa.waves(p1, w, -1.5, 11.5)
+        want = (full_grid_system(p1, wa, wb, wc) if mode == "full"
+                else channel_subset_system(p1, wa, wb, wc, **kw))
+        for name in ("channel_ix", "channel_iy", "pkd", "wave_a", "wave_b", "wave_c"):
+            np.testing.assert_array_equal(getattr(sp, name), getattr(want, name))
+        assert sp.specular == want.specular
+    with pytest.raises(ValueError):
+        beam_systems(pkd, lambda e: sa.waves(e, w, -1.5, 11.5), max_pkd=-1e9)
