@@ -11,7 +11,7 @@ solved to ||b - A psi|| <= 1e-10 ||b|| per beam in ONE batched call.
 
 - ``value``: solves/s of the mixed form (FP32 inner GMRES on tcgen05 BF16x3
   + FP32 coupling, FP64 iterative refinement), batched, inputs resident in
-  HBM.  Working set: Krylov basis 4.4 GB > the 126 MB L2.
+  HBM.  Working set: FP32 Krylov basis (21 vectors) 3.0 GB > the 126 MB L2.
 - ``plain_fp64``: the plain FP64 form on the same beams, batched and one
   beam at a time (the drop-in's way of working), and the ratio.
 - ``accuracy``: max |Delta |S|^2| mixed vs FP64 over the batch and flux error.
@@ -21,8 +21,9 @@ solved to ||b - A psi|| <= 1e-10 ||b|| per beam in ONE batched call.
   CUDA events recorded inside the solve graphs during a timed pass.
 - ``cpu_baseline``: the reference algorithm on one host core (the oracle, a
   C restatement of the reference Fortran solve), bounded sample.
-Multi-GPU (torchrun): independent replicas of the batch, time = max over
-ranks (weak scaling, no collective on the data path).
+Multi-GPU (torchrun): one seeded sweep of 512 x N beams split into N
+contiguous slices, one per rank (weak scaling: 512 beams per GPU), time =
+max over ranks; no collective on the data path.
 """
 
 from __future__ import annotations
@@ -114,8 +115,13 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def build_workload(name: str, beams: int = 512):
+def build_workload(name: str, beams: int = 512, rank: int = 0, world: int = 1):
+    """(case, systems) of this rank.  cfg2 on N ranks: one seeded sweep of
+    beams x N beams split into N contiguous slices (``replicas.shard``), so
+    every rank solves `beams` beams of its own; N = 1 is the headline batch
+    ``cfg2_batch(beams, seed=0)``."""
     from multiscat_b200 import workloads as wl
+    from multiscat_b200.replicas import shard
     if name == "cfg1":
         case = wl.cfg1_case()
         return case, [case.system()]
@@ -123,48 +129,128 @@ def build_workload(name: str, beams: int = 512):
         case = wl.cfg0_case()
         return case, [case.system()]
     if name == "cfg2":
-        return wl.cfg2_batch(n_solves=beams)
+        case, systems = wl.cfg2_batch(n_solves=beams * world)
+        return case, shard(systems, rank, world)
     raise ValueError(name)
 
 
-# FP32 FMA nominal peak of a B200 at its 1965 MHz boost clock (148 SMs x 128
-# lanes x 2 flop); the channel coupling runs on CUDA cores, not tensor cores.
-FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
-# DRAM bytes of one full-batch cfg2 launch measured by ncu (profiles/), used
-# as the `traffic` of the roofline line for that workload.
-NCU_TRAFFIC_FULL_LAUNCH = {
-    ("cfg2", "coupling"): 439.8e6 + 138.9e6,
-    ("cfg2", "block_inverse"): 148.2e6 + 94.3e6,
+def oracle_fixture_error(res, workload: str, beams: int, world: int) -> dict | None:
+    """max |Delta |S|^2| of a cfg2 result against the oracle on the 64 beams of
+    tests/golden/oracle_cfg2_batch.npz (beams of cfg2_batch(512, seed=0))."""
+    path = ROOT / "tests" / "golden" / "oracle_cfg2_batch.npz"
+    if workload != "cfg2" or beams != 512 or world != 1 or not path.exists():
+        return None
+    fx = np.load(path)
+    inten = res.intensities.cpu().numpy()
+    err, flux = 0.0, 0.0
+    for k, b in enumerate(fx["beams"]):
+        want = fx["intensities"][fx["offsets"][k]:fx["offsets"][k + 1]]
+        got = inten[res.row_offsets[b]:res.row_offsets[b + 1]]
+        err = max(err, float(np.abs(got - want).max()))
+        flux = max(flux, abs(float(got.sum()) - 1.0))
+    return {"max_abs_dI": err, "max_flux_error": flux, "beams_checked": int(len(fx["beams"])),
+            "oracle_eps": float(fx["eps"]),
+            "fixture": "tests/golden/oracle_cfg2_batch.npz (oracle on 64 beams of this batch: "
+                       "8 largest-theta, 8 lowest-E, 8 most-iterations, 40 random)"}
+
+
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one launch
+# of a kernel kind over the given number of channel rows, from the captures
+# summarised in profiles/ (file named beside each entry).  Used as the
+# `traffic` of a kernel's roofline line, scaled to the rows of an average
+# launch of this run.
+NCU_TRAFFIC = {
+    # (workload, kind): (bytes, rows of the captured launch, profile)
+    ("cfg2", "coupling"): (439.8e6 + 138.9e6, 119741, "k_coupling_halo_f32_cfg2.md"),
+    ("cfg2", "block_inverse"): (148.2e6 + 94.3e6, 119741, "k_block_inverse_tc_cfg2.md"),
 }
 
 
-def kernel_work(name: str, n: int, rows: float, taps: int, mixed: bool) -> tuple[float, float]:
-    """Algorithmic (flops, bytes) for `rows` channel rows processed.
+def measure_fma_peaks() -> dict:
+    """FP32 and FP64 CUDA-core FMA throughput of this GPU (TFLOP/s), from the
+    library's msc_measure_fma_peak kernel timed with CUDA events (best of 3)."""
+    import ctypes
+    from multiscat_b200 import _native as nat
+    lib = nat.load()
+    out = {}
+    for name, prec in (("fp32", nat.PRECISION_MIXED), ("fp64", nat.PRECISION_FP64)):
+        best = 0.0
+        for _ in range(3):
+            fl = ctypes.c_double(0.0)
+            ms = ctypes.c_float(0.0)
+            nat.check("msc_measure_fma_peak",
+                      lib.msc_measure_fma_peak(prec, 200000, ctypes.byref(fl), ctypes.byref(ms), None))
+            best = max(best, fl.value / (ms.value / 1e3) / 1e12)
+        out[name] = best
+    return out
 
-    block inverse: two real GEMMs (n x n)(n x 2 rows) = 8 n^2 rows flop (x3 for
-    the BF16x3 split on tensor cores); bytes: x in, u out.  coupling: 8 taps
-    flop per complex output; bytes: source, addend and result vectors.
-    Arnoldi kernels are byte-bound; their bytes depend on the step j and are
-    not attributed here.
+
+def kernel_records(kt: dict, res, n: int, taps: int, mixed: bool, dcgs: bool, tensor: bool,
+                   peaks: dict, fma: dict, workload: str) -> dict:
+    """Per timed kernel kind: its bound, algorithmic work of the rows it
+    actually processed, achieved rate and fraction of the measured peak.
+
+    block inverse: 8 n^2 flop per row (two real GEMMs of the complex row),
+      x3 for the BF16x3 split on tcgen05 (bound: tensor; else the FMA pipe);
+    coupling: 8 K n flop per row (K taps, one complex MAC each), ~27 flop per
+      byte at K = 80, so the FMA pipe bounds it, not HBM;
+    Arnoldi passes: HBM bytes, one read or write of a row of a Krylov vector
+      per vector touched: DCGS2 reduction (j + 1) + 1 reads at step j, update
+      (j + 1) + 1 reads and 2 writes; CGS2 first projection (j + 1) + 1 reads,
+      update/re-projection and normalisation (j + 1) + 1 reads and 1 write.
     """
     es = 8 if mixed else 16
-    nv = float(n) * rows
-    if name == "block_inverse":
-        return 8.0 * n * n * rows * (3 if mixed else 1), 2 * es * nv
-    if name == "coupling":
-        return 8.0 * taps * nv, 3 * es * nv
-    return 0.0, 0.0
-
-
-def rows_processed(res, name: str) -> float:
-    """Channel rows a kernel kind processed in one solve: each Krylov step of a
-    system runs the coupling over its rows; the block inverse also runs once
-    per restart / refinement cycle (the solution update)."""
     rows = np.diff(res.row_offsets).astype(float)
-    steps = float(np.dot(rows, res.iterations))
-    if name == "block_inverse":
-        return steps + float(np.dot(rows, res.cycles))
-    return steps
+    steps_rows = float(np.dot(rows, res.iterations))
+    vec_rows = float(np.dot(rows, res.basis_vectors))
+    cyc_rows = float(np.dot(rows, res.cycles))
+    fma_peak = fma["fp32" if mixed else "fp64"]
+    hbm = peaks["hbm_gbs"]
+    bf16 = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
+    total_ms = sum(v["ms"] for v in kt.values()) or 1.0
+    names = dict(KERNEL_NAMES)
+    if dcgs:
+        names["arnoldi_project"] = "Arnoldi reduction (DCGS2: Q^H v, Q^H w, norms, coefficients)"
+        names["arnoldi_update_project"] = "Arnoldi update (DCGS2: q_j, next candidate, norm, Givens)"
+    out = {}
+    for k, v in kt.items():
+        if not v["launches"]:
+            continue
+        t_s = v["ms"] / 1e3
+        rec = {"what": names[k], "launches": v["launches"], "avg_us": 1e6 * t_s / v["launches"],
+               "share_of_timed_kernels": v["ms"] / total_ms}
+        if k == "block_inverse":
+            r_done = steps_rows + cyc_rows
+            fl = 8.0 * n * n * r_done * (3 if tensor else 1)
+            rec.update({"bound": "tensor" if tensor else "fma", "unit": "TFLOP/s",
+                        "achieved": fl / t_s / 1e12, "peak": bf16 if tensor else fma_peak,
+                        "algorithmic": f"{8 * n * n * (3 if tensor else 1)} flop per row",
+                        "rows": r_done, "bytes": 2.0 * es * n * r_done})
+        elif k == "coupling":
+            fl = 8.0 * taps * n * steps_rows
+            rec.update({"bound": "fma", "unit": "TFLOP/s", "achieved": fl / t_s / 1e12,
+                        "peak": fma_peak, "algorithmic": f"8 K n = {8 * taps * n} flop per row",
+                        "rows": steps_rows, "bytes": 3.0 * es * n * steps_rows})
+        else:
+            if k == "arnoldi_project":
+                vecs = vec_rows + steps_rows
+            elif k == "arnoldi_update_project":
+                vecs = vec_rows + (3 if dcgs else 2) * steps_rows
+            else:
+                vecs = vec_rows + 2 * steps_rows
+            nbytes = vecs * n * es
+            rec.update({"bound": "hbm", "unit": "GB/s", "achieved": nbytes / t_s / 1e9,
+                        "peak": hbm, "algorithmic": "one pass per Krylov vector row touched",
+                        "rows": steps_rows, "bytes": nbytes})
+        rec["frac"] = rec["achieved"] / rec["peak"]
+        tr = NCU_TRAFFIC.get((workload, k))
+        if tr and mixed and "bytes" in rec:
+            per_row = tr[0] / tr[1]
+            alg_per_row = (3.0 if k == "coupling" else 2.0) * es * n
+            rec["traffic_over_algorithmic"] = per_row / alg_per_row
+            rec["traffic_profile"] = f"profiles/{tr[2]}"
+        out[k] = rec
+    return out
 
 
 def timed_steps(plan, steps: int, stream, torch) -> float:
@@ -197,12 +283,13 @@ def run_b200(args) -> None:
         from multiscat_b200.replicas import max_over_ranks as mor
         return mor(x, device="cuda")
 
-    case, systems = build_workload(args.workload, args.beams)
+    case, systems = build_workload(args.workload, args.beams, rank, world)
     nsys = len(systems)
     stream = torch.cuda.current_stream()
     plan = ScatteringPlan(case.v, case.t, systems, rtol=args.rtol, restart=args.restart,
                           precision=args.precision, inner_restart=args.inner_restart,
-                          inner_rtol=args.inner_rtol, preconditioner_order=args.precond_order)
+                          inner_rtol=args.inner_rtol, preconditioner_order=args.precond_order,
+                          gram_schmidt=args.gram_schmidt)
     for _ in range(args.warmup):
         res = plan.solve()
     torch.cuda.synchronize()
@@ -216,6 +303,8 @@ def run_b200(args) -> None:
     launches = plan.launches_per_solve() * args.steps
     iters = res.iterations
     inten = res.intensities.clone()
+    vs_oracle = oracle_fixture_error(res, args.workload, args.beams, world)
+    fallbacks = int(plan.info().fallbacks_last)
 
     # kernel shares from a separate pass with event pairs inside the graphs
     plan.enable_kernel_timing(True)
@@ -228,58 +317,36 @@ def run_b200(args) -> None:
     rows = plan.total_rows
     taps = plan.n_taps
     peaks, peak_kind = load_peaks()
-    total_ms = sum(v["ms"] for v in kt.values()) or 1.0
-    kernels = {}
-    for k, v in kt.items():
-        if not v["launches"]:
-            continue
-        t_s = v["ms"] / 1e3
-        flops, nbytes = kernel_work(k, n, rows_processed(res, k), taps, mixed)
-        kernels[k] = {"what": KERNEL_NAMES[k], "launches": v["launches"],
-                      "avg_us": 1e6 * t_s / v["launches"],
-                      "share_of_timed_kernels": v["ms"] / total_ms}
-        if flops:
-            kernels[k]["achieved_tflops"] = flops / t_s / 1e12
-            kernels[k]["achieved_gbs"] = nbytes / t_s / 1e9
-    dom = max(kt.items(), key=lambda kv: kv[1]["ms"])[0] if kt else None
+    fma = measure_fma_peaks()
+    tensor = mixed and "tc_" in tuning.get("chosen", "")
+    kernels = kernel_records(kt, res, n, taps, mixed, args.gram_schmidt == "dcgs2", tensor,
+                             peaks, fma, args.workload)
     roof = None
-    if dom and kt[dom]["launches"]:
-        nl = kt[dom]["launches"]
-        t_s = kt[dom]["ms"] / 1e3
-        rows_done = rows_processed(res, dom)
-        flops, nbytes = kernel_work(dom, n, rows_done, taps, mixed)
-        traffic = NCU_TRAFFIC_FULL_LAUNCH.get((args.workload, dom))
-        if traffic is not None and mixed:
-            traffic = traffic * (rows_done / nl) / rows      # at this run's average rows per launch
-        else:
-            traffic = None
-        if dom == "block_inverse" and mixed and "tc_" in tuning.get("chosen", ""):
-            achieved = flops / t_s / 1e12
-            roof = {"kernel": f"{dom}: {KERNEL_NAMES[dom]} (tcgen05 BF16x3)", "bound": "tensor",
-                    "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                    "frac": achieved / peaks["bf16_tflops"], "traffic": traffic}
-        else:
-            achieved = nbytes / t_s / 1e9
-            roof = {"kernel": f"{dom}: {KERNEL_NAMES[dom]}", "bound": "hbm",
-                    "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": achieved / peaks["hbm_gbs"], "traffic": traffic}
-            if flops:
-                roof["achieved_tflops"] = flops / t_s / 1e12
-                if dom == "coupling" and mixed:
-                    roof["fp32_fma_nominal_tflops"] = FP32_NOMINAL_TFLOPS
-                    roof["frac_of_fp32_fma_nominal"] = roof["achieved_tflops"] / FP32_NOMINAL_TFLOPS
-                    roof["note"] = ("the coupling is arithmetic on CUDA cores (FP32 FMA); its HBM "
-                                    "fraction is low by design, the FP32 fraction is the one "
-                                    "that bounds it")
-        roof.update({"peak_source": f"{peak_kind} (MEASURED_PEAKS.json)",
-                     "avg_launch_us": 1e6 * t_s / nl, "launches_timed": nl,
-                     "per_launch_work": (f"{rows_done / nl:.0f} channel rows per launch on "
-                                         f"average ({rows} in the batch; converged systems "
-                                         "skip their rows), x algorithmic work per row"),
-                     "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of a "
-                                        "full-batch launch (profiles/), scaled to the average "
-                                        "rows per launch") if traffic else None,
-                     "share": kt[dom]["ms"] / total_ms})
+    if kernels:
+        dom = max(kernels, key=lambda k: kernels[k]["share_of_timed_kernels"])
+        kr = kernels[dom]
+        nl = kr["launches"]
+        traffic = None
+        tr = NCU_TRAFFIC.get((args.workload, dom))
+        if tr and mixed:
+            traffic = tr[0] / tr[1] * (kr["rows"] / nl)      # at this run's average rows per launch
+        roof = {"kernel": f"{dom}: {kr['what']}", "bound": kr["bound"], "achieved": kr["achieved"],
+                "peak": kr["peak"], "unit": kr["unit"], "frac": kr["frac"], "traffic": traffic,
+                "peak_source": ("CUDA-core FMA throughput measured in this run "
+                                "(msc_measure_fma_peak, best of 3)" if kr["bound"] == "fma" else
+                                f"{peak_kind} (MEASURED_PEAKS.json)"),
+                "avg_launch_us": kr["avg_us"], "launches_timed": nl,
+                "per_launch_work": (f"{kr['rows'] / nl:.0f} channel rows per launch on average "
+                                    f"({rows} in the batch; converged systems skip their rows) "
+                                    f"x {kr['algorithmic']}"),
+                "algorithmic_bytes_per_launch": kr["bytes"] / nl,
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                   f"launch (profiles/{tr[2]}), scaled to the average rows per "
+                                   "launch") if traffic else None,
+                "share": kr["share_of_timed_kernels"],
+                "hbm_frac": kr["bytes"] / (kr["avg_us"] * nl / 1e6) / 1e9 / peaks["hbm_gbs"]}
+        if traffic:
+            roof["traffic_over_algorithmic"] = traffic / (kr["bytes"] / nl)
 
     extra = {}
     if not args.quick and rank == 0:
@@ -293,6 +360,7 @@ def run_b200(args) -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_sample(args.workload, case, systems)
 
+    krylov_m = (args.inner_restart or min(args.restart, 20)) if mixed else args.restart
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
@@ -304,11 +372,17 @@ def run_b200(args) -> None:
                        "n_z": n, "taps": taps, "restart": args.restart, "rtol": args.rtol,
                        "precision": args.precision,
                        "l2": "inputs larger than L2: Krylov basis "
-                             f"{(args.restart + 1) * rows * n * (8 if mixed else 16) / 1e9:.2f} GB",
-                       "parallelism": f"independent replicas x{world}"},
+                             f"{(krylov_m + 1) * rows * n * (8 if mixed else 16) / 1e9:.2f} GB "
+                             f"({krylov_m + 1} vectors of {rows} x {n} "
+                             f"{'complex64' if mixed else 'complex128'})",
+                       "parallelism": (f"beam-sharded sweep over {world} GPUs "
+                                       f"({nsys} beams each)" if world > 1 else "1 GPU")},
             "iterations": {"mean": float(np.mean(iters)), "max": int(np.max(iters)),
                            "min": int(np.min(iters))},
+            "accuracy_vs_oracle": vs_oracle,
+            "fp64_fallbacks_per_step": fallbacks,
             "roofline": roof, "kernels": kernels, "autotune": tuning,
+            "fma_peak_tflops": fma,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
             "gpu_launches": launches,
         }
@@ -327,7 +401,7 @@ def secondary_measurements(args, case, systems, plan, inten, value, torch, strea
     fp64 = ScatteringPlan(case.v, case.t, systems, rtol=args.rtol, restart=args.restart)
     fp64.solve()
     r64 = fp64.solve()
-    ms64 = timed_steps(fp64, 2, stream, torch) / 2
+    ms64 = timed_steps(fp64, args.steps, stream, torch) / args.steps
     d = (inten - r64.intensities).abs()
     flux_err = []
     for s in range(len(systems)):
@@ -357,6 +431,8 @@ def secondary_measurements(args, case, systems, plan, inten, value, torch, strea
     batched_rate = len(systems) / (ms64 / 1e3)
     out["plain_fp64"] = {
         "batched_solves_per_s": batched_rate,
+        "batched_steps_timed": args.steps,
+        "batched_vs_oracle": oracle_fixture_error(r64, args.workload, args.beams, 1),
         "one_beam_at_a_time_solves_per_s": single_rate,
         "one_beam_sample": f"{len(sample)} beams, one FP64 plan each, solved back to back",
         "mixed_batched_over_fp64_one_at_a_time": value / single_rate,
@@ -432,9 +508,10 @@ def cfg4_measurement(args, torch, stream) -> dict:
         p = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, restart=args.restart,
                            precision=prec)
         r = p.solve()
-        ms = timed_steps(p, 1, stream, torch)
+        steps = max(2, args.steps // 2)
+        ms = timed_steps(p, steps, stream, torch) / steps
         inten[prec] = r.intensities
-        out[prec] = {"solves_per_s": len(systems) / (ms / 1e3), "ms": ms,
+        out[prec] = {"solves_per_s": len(systems) / (ms / 1e3), "ms": ms, "steps_timed": steps,
                      "iterations_max": int(r.iterations.max()),
                      "all_converged": bool((r.status == 0).all()),
                      "autotune": p.tuning_report()}
@@ -465,7 +542,7 @@ def e2e_measurement(args, case, systems, torch, stream, barrier, max_over_ranks,
     one()
     torch.cuda.synchronize()
     barrier()
-    steps = max(1, min(args.steps, 3))
+    steps = args.steps
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     start.record(stream)
@@ -475,7 +552,7 @@ def e2e_measurement(args, case, systems, torch, stream, barrier, max_over_ranks,
     torch.cuda.synchronize()
     ms = max_over_ranks(start.elapsed_time(stop))
     return {"value": world * len(systems) * steps / (ms / 1e3), "unit": "solves/s",
-            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps_timed": steps,
             "path": "ScatteringPlan(host numpy V, T, beams).solve() -> |S|^2 to host, "
                     "plan built inside every step (eigen/autotune caches warm)"}
 
@@ -595,6 +672,8 @@ def main() -> None:
                     help="mixed form: inner FP32 reduction per refinement step (0 = the library default)")
     ap.add_argument("--precond-order", type=int, default=0,
                     help="von Neumann order of the preconditioner (0 = block-diagonal)")
+    ap.add_argument("--gram-schmidt", default="dcgs2", choices=["dcgs2", "cgs2"],
+                    help="Arnoldi orthogonalisation (dcgs2: two basis passes per step; cgs2: three)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true",
                     help="only the main timed steps (no secondary rates, no e2e)")

@@ -70,11 +70,24 @@ typedef struct {
                                bit 2: mixed form with ONE Gram-Schmidt pass
                                (Pythagorean norm) in the inner solve instead
                                of two; fewer bytes per iteration, but on
-                               ill-conditioned batches more iterations        */
-    int32_t precond_order;  /* von Neumann order k of the preconditioner
-                               M = sum_{i<=k} (-D^-1 V)^i D^-1 (0 = block-diagonal
-                               D^-1; 0..8), the reference's
-                               _scipy_von_neumann.py:40-58                    */
+                               ill-conditioned batches more iterations;
+                               bit 3: mixed form without the FP64 recovery of
+                               systems left unconverged (see msc_solve);
+                               bit 4: Arnoldi step by classical Gram-Schmidt
+                               with two full passes (CGS2, three passes over
+                               the basis per step) instead of the default
+                               delayed re-orthogonalisation (DCGS2, two);
+                               bit 5: block Gauss-Seidel preconditioner, the
+                               reference's: L = D + V^lower in each system's
+                               channel order, M = L^-1 by a forward sweep
+                               (multiscat_gmres.f90:641-687)                  */
+    int32_t precond_order;  /* order k of the preconditioner series
+                               M = sum_{i<=k} (-B^-1 N)^i B^-1 with B = D,
+                               N = V (von Neumann, the reference's
+                               _scipy_von_neumann.py:40-58; 0 = block-diagonal
+                               D^-1) or, with flag bit 5, B = L, N = V^upper
+                               (k = 1 is the reference's Neumann flag on top
+                               of Gauss-Seidel, _gmres.py:55-71); 0..8       */
 } msc_plan_desc;
 
 typedef struct msc_plan msc_plan;
@@ -84,8 +97,12 @@ typedef struct {
     int32_t iterations;     /* Krylov iterations (inner iterations for mixed) */
     int32_t refinements;    /* FP64 outer steps (mixed), restart cycles (FP64)*/
     int32_t status;         /* msc_status of this system                      */
-    int32_t reserved;
+    int32_t fp64_fallback;  /* mixed: 1 if the FP64 recovery re-solved it     */
     double residual;        /* final true relative residual ||b-A psi||/||b|| */
+    int32_t basis_vectors;  /* Krylov basis vectors the Arnoldi steps projected
+                               against, summed over the steps (j + 1 at step
+                               j): the per-step basis traffic for rooflines  */
+    int32_t reserved;
 } msc_result;
 
 /* Create a plan on the current CUDA device.  Allocates all device memory
@@ -105,8 +122,9 @@ msc_status msc_release_cached_memory(void);
 /* Set the potential (host arrays, C order):
  *   potential_values  complex [nkx][nky][n_z]  V_G(z_k) in 1/Angstrom^2
  *   kinetic           double  [n_z][n_z]       positive Lobatto kinetic T
- * Builds H0 = T + diag Re V_00, its eigen-decomposition (FP64) and the
- * coupling taps (every offset G != 0 with V_G or V_-G nonzero).
+ * Builds H0 = T + diag Re V_00, its FP64 eigen-decomposition (on the
+ * device; see msc_debug_symmetric_eigh) and the coupling taps (every offset
+ * G != 0 with V_G or V_-G nonzero).
  * Replaces build_preconditioner, multiscat_gmres.f90:226-273. */
 msc_status msc_plan_set_potential(msc_plan *plan, const double *potential_values,
                                   const double *kinetic);
@@ -141,7 +159,15 @@ msc_status msc_plan_set_systems(msc_plan *plan, int32_t first, int32_t count,
 /* Solve all systems.  psi_out (device, may be NULL): complex FP64 packed
  * rows [sum_s C_s][n_z] in system order.  intensities_out (device, may be
  * NULL): double [sum_s C_s] = |S_G0|^2.  results (host, may be NULL):
- * msc_result [n_systems].  stream is a cudaStream_t (NULL = legacy). */
+ * msc_result [n_systems].  stream is a cudaStream_t (NULL = legacy).
+ * Mixed plans: a system still unconverged (or non-finite) after
+ * max_refinements FP64 refinement steps is solved again in plain FP64 on the
+ * same operator and right-hand side, starting from its mixed-precision
+ * state (from zero if that went non-finite), before the results are
+ * returned; its msc_result has fp64_fallback = 1 and counts both solves'
+ * iterations.  Only a system the FP64 solve cannot converge either is
+ * reported as MSC_ERR_NOT_CONVERGED, the reference's ierr 2
+ * (multiscat_python_bindings.f90:58-60).  Flag bit 3 turns this off. */
 msc_status msc_solve(msc_plan *plan, double *psi_out, double *intensities_out,
                      msc_result *results, void *stream);
 
@@ -182,6 +208,20 @@ msc_status msc_debug_apply_coupling(msc_plan *plan, const double *x, double *y, 
 msc_status msc_debug_apply_block_inverse(msc_plan *plan, const double *x, double *y, void *stream);
 msc_status msc_debug_apply_operator(msc_plan *plan, const double *x, double *y, void *stream);
 
+/* The reference's block Gauss-Seidel splitting A = L + U on device buffers
+ * x, y (complex FP64 [total_rows][n_z], plan row order, x != y), system by
+ * system, with "lower" meaning an earlier row of the same system (the
+ * channel order the system was given in):
+ *   msc_apply_lower_block: y = L x,    L = D + V^lower
+ *   msc_solve_lower_block: y = L^-1 x  (forward sweep, one CTA per system,
+ *                          rows in level sets)
+ * Replace debug_solve_lower_block / _apply_lower_block /
+ * _apply_inverse_lower_block (multiscat_gmres.f90:641-687,
+ * multiscat/multiscat/_scipy.py:262-297, 357-380).  The reference's
+ * interior state convention is L psi (_gmres.py:127, _multiscat.py:86-88). */
+msc_status msc_apply_lower_block(msc_plan *plan, const double *x, double *y, void *stream);
+msc_status msc_solve_lower_block(msc_plan *plan, const double *x, double *y, void *stream);
+
 /* Allocation-free twin of msc_debug_apply_operator (no counterpart in the
  * reference): y = A x = D x + V_off x for ONE full-grid system, without a
  * plan and without allocating anything.  For callers that cannot call
@@ -196,9 +236,12 @@ msc_status msc_debug_apply_operator(msc_plan *plan, const double *x, double *y, 
  * MSC_ERR_DIMS (nkx*nky <= 2049 channels, and about
  * 32 (nkx*nky) n_z + 4 (nkx*nky)^2 bytes in total).  The first call on each
  * device looks up the array's device address and sets kernel limits; make
- * it before any stream capture.  The call waits on `stream` once (to read
- * the number of nonzero taps).  All calls share the array and keep the last
- * call's contents: calls that overlap on the GPU race. */
+ * it before any stream capture.  Every call waits on `stream` once: it
+ * reads the number of nonzero taps and a non-finite-input flag back to the
+ * host, and returns MSC_ERR_NONFINITE (as msc_plan_set_potential and
+ * msc_plan_set_system do) when V, the kinetic matrix, pkd or wave_c holds a
+ * NaN or infinity.  All calls share the array and keep the last call's
+ * contents: calls that overlap on the GPU race. */
 msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32_t n_z,
                                       const double *potential_values, const double *kinetic,
                                       const double *pkd, const double *wave_c, const double *x,
@@ -207,6 +250,14 @@ msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32_t n_z,
 /* Mixed-precision plans: y = D^-1 x with the FP32 kernel the inner solve
  * uses (tcgen05 BF16x3 when available), x and y complex FP32 packed rows. */
 msc_status msc_debug_apply_block_inverse_f32(msc_plan *plan, const float *x, float *y, void *stream);
+
+/* The FP64 eigen-decomposition msc_plan_set_potential uses for H0, on any
+ * symmetric n x n host matrix a (row-major, 2 <= n <= 1024): w[n] ascending
+ * eigenvalues, v[n*n] row-major with eigenvector k in column k.  Householder
+ * tridiagonalisation and the eigenvector accumulations run on the current
+ * device; the tridiagonal QR iteration (O(n^2)) on the host.  Replaces the
+ * reference's rs (tred2 + tql2), diagsub.f90:5-262. */
+msc_status msc_debug_symmetric_eigh(int32_t n, const double *a, double *w, double *v);
 
 /* Tile width N of the tcgen05 block inverse the plan uses (0 = not used).
  * Valid after the first msc_solve or debug call. */
@@ -227,7 +278,7 @@ typedef struct {
     int32_t n_tiles;           /* row tiles (kernel grid size)                     */
     int64_t launches_last;     /* kernel launches issued by the last msc_solve     */
     int32_t cycles_last;       /* restart cycles run by the last msc_solve         */
-    int32_t reserved;
+    int32_t fallbacks_last;    /* systems the last msc_solve re-solved in FP64     */
 } msc_plan_info;
 
 msc_status msc_plan_get_info(const msc_plan *plan, msc_plan_info *info);
@@ -241,6 +292,16 @@ msc_status msc_plan_get_info(const msc_plan *plan, msc_plan_info *info);
  * previous call and resets them. */
 msc_status msc_plan_set_kernel_timing(msc_plan *plan, int enable);
 msc_status msc_plan_kernel_timing(msc_plan *plan, double *ms, int64_t *launches);
+
+/* CUDA-core FMA throughput of the current GPU (measurement only; the
+ * roofline denominator of the kernels that run on the FMA pipes, such as the
+ * channel coupling).  Runs a kernel of independent fused multiply-adds on
+ * every SM, FP32 for precision = MSC_PRECISION_MIXED and FP64 for
+ * MSC_PRECISION_FP64, `iterations` FMAs per chain, timed with CUDA events on
+ * `stream`; *flops = its floating-point operations (2 per FMA), *ms = its
+ * device time.  No counterpart in the reference. */
+msc_status msc_measure_fma_peak(int32_t precision, int32_t iterations, double *flops, float *ms,
+                                void *stream);
 
 /* ---- Adjoint differentiation (no counterpart in the reference, which has
  * no derivatives; the operator transposed is the one of

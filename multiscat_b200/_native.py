@@ -23,7 +23,8 @@ EXPORTED = (
     "msc_plan_uses_tensor_cores", "msc_plan_tuning_report", "msc_plan_set_adjoint",
     "msc_plan_is_adjoint", "msc_plan_set_boundary_rhs", "msc_plan_set_adjoint_rhs",
     "msc_potential_gradient", "msc_release_cached_memory", "msc_plan_set_initial_guess",
-    "msc_plan_set_systems",
+    "msc_plan_set_systems", "msc_measure_fma_peak", "msc_debug_symmetric_eigh",
+    "msc_apply_lower_block", "msc_solve_lower_block",
 )
 
 MSC_OK = 0
@@ -62,8 +63,10 @@ class Result(ctypes.Structure):
         ("iterations", ctypes.c_int32),
         ("refinements", ctypes.c_int32),
         ("status", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("fp64_fallback", ctypes.c_int32),
         ("residual", ctypes.c_double),
+        ("basis_vectors", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -74,7 +77,7 @@ class PlanInfo(ctypes.Structure):
         ("n_tiles", ctypes.c_int32),
         ("launches_last", ctypes.c_int64),
         ("cycles_last", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("fallbacks_last", ctypes.c_int32),
     ]
 
 
@@ -122,7 +125,8 @@ def load() -> ctypes.CDLL:
                                       ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                       ctypes.POINTER(ctypes.c_int)]
     for name in ("msc_debug_apply_coupling", "msc_debug_apply_block_inverse",
-                 "msc_debug_apply_operator", "msc_debug_apply_block_inverse_f32"):
+                 "msc_debug_apply_operator", "msc_debug_apply_block_inverse_f32",
+                 "msc_apply_lower_block", "msc_solve_lower_block"):
         f = getattr(lib, name)
         f.restype = ctypes.c_int
         f.argtypes = [_vp, _vp, _vp, _vp]
@@ -153,6 +157,11 @@ def load() -> ctypes.CDLL:
     lib.msc_potential_gradient.argtypes = [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp]
     lib.msc_plan_set_initial_guess.restype = ctypes.c_int
     lib.msc_plan_set_initial_guess.argtypes = [_vp, _vp, ctypes.c_int32, _vp]
+    lib.msc_debug_symmetric_eigh.restype = ctypes.c_int
+    lib.msc_debug_symmetric_eigh.argtypes = [ctypes.c_int32, _dp, _dp, _dp]
+    lib.msc_measure_fma_peak.restype = ctypes.c_int
+    lib.msc_measure_fma_peak.argtypes = [ctypes.c_int32, ctypes.c_int32, _dp,
+                                         ctypes.POINTER(ctypes.c_float), _vp]
     lib.msc_release_cached_memory.restype = ctypes.c_int
     lib.msc_release_cached_memory.argtypes = []
     lib.msc_last_error.restype = ctypes.c_char_p

@@ -19,10 +19,11 @@ from dataclasses import dataclass, field
 from typing import Literal, Sequence
 
 import numpy as np
+import torch
 
 from . import setup_arrays as sa
-from .solver import (ScatteringPlan, SolveResult, beam_systems, channel_subset_system,
-                     full_grid_system)
+from .solver import (ScatteringPlan, SolveResult, SystemSpec, beam_systems,
+                     channel_subset_system, full_grid_system)
 
 
 @dataclass(frozen=True, kw_only=True)
@@ -344,19 +345,50 @@ def _single_solve(condition: ScatteringCondition, config: OptimizationConfig, *,
     return _to_grid(result, 0, system, condition.metadata.shape[:2])
 
 
+def _reference_order_system(arr: NaturalArrays, n_channels: int | None):
+    """The channel list of the reference's state functions: ``np.argsort`` of
+    pkd with numpy's default sort, the first ``n_channels`` of it
+    (``_scipy.py:414-416``).  Its order defines the lower block L of the
+    reference's state convention, so it is reproduced call for call (the
+    solver's own ``n_channels`` path sorts stably instead)."""
+    flat = np.asarray(arr.pkd, float).ravel()
+    order = np.argsort(flat)
+    if n_channels is not None:
+        order = order[:n_channels]
+    hit = np.nonzero(order == 0)[0]
+    if hit.size == 0:
+        raise ValueError("the specular channel is not in the kept channel set")
+    ix, iy = np.unravel_index(order, arr.pkd.shape)
+    return SystemSpec(ix.astype(np.int32), iy.astype(np.int32), flat[order],
+                      np.asarray(arr.wave_a, complex).ravel()[order],
+                      np.asarray(arr.wave_b, complex).ravel()[order],
+                      np.asarray(arr.wave_c, complex).ravel()[order], int(hit[0]))
+
+
+def _check_convention(convention: str) -> None:
+    if convention not in ("reference", "psi"):
+        raise ValueError(f"Unknown state convention '{convention}'. Expected 'reference' or 'psi'.")
+
+
 def get_scattering_state(condition: ScatteringCondition, config: OptimizationConfig, *,
-                         initial_state: np.ndarray | None = None) -> np.ndarray:
-    """The full interior state psi_G(z_k), complex128 (nkx, nky, nz)
+                         initial_state: np.ndarray | None = None,
+                         convention: Literal["reference", "psi"] = "reference") -> np.ndarray:
+    """The full interior state, complex128 (nkx, nky, nz)
     (``_multiscat.py:227-246``); channels outside an ``n_channels`` set are 0.
 
-    ``initial_state`` (same shape) warm-starts the solve, e.g. with the state of
-    a neighbouring energy or angle (the reference's ``x0``, ``_gmres.py:106-108``).
-    Convention: this returns psi itself.  The reference's state is L psi, its
-    Gauss-Seidel lower block applied to psi (``_gmres.py:127``), because its
-    solver works in that variable; the intensities that both states lead to
-    are the same."""
+    ``convention="reference"`` (default) returns what the reference returns:
+    L psi, its block Gauss-Seidel lower block L = D + V^lower applied to the
+    solution psi, with the channels in the reference's argsort(pkd) order
+    (``_gmres.py:127``, ``_scipy.py:580-613``); ``"psi"`` returns psi itself.
+    ``initial_state`` (same shape, same convention) warm-starts the solve,
+    e.g. with the state of a neighbouring energy or angle (the reference's
+    ``x0``, which it maps through L^-1 as well, ``_gmres.py:106-108``)."""
+    _check_convention(convention)
     arr = natural_arrays(condition)
-    system = _system_for(arr, config)
+    if convention == "reference":
+        system = _reference_order_system(arr, config.n_channels)
+    else:
+        system = _system_for(arr, config)
     nkx, nky, nz = arr.potential_values.shape
     plan = ScatteringPlan(arr.potential_values, arr.kinetic, [system],
                           rtol=config.residual_tolerance, restart=config.restart,
@@ -364,25 +396,49 @@ def get_scattering_state(condition: ScatteringCondition, config: OptimizationCon
     try:
         if initial_state is not None:
             guess = np.asarray(initial_state, np.complex128).reshape(nkx, nky, nz)
-            plan.set_initial_guess(guess[system.channel_ix, system.channel_iy])
+            rows = torch.as_tensor(np.ascontiguousarray(guess[system.channel_ix, system.channel_iy]),
+                                   device=torch.device("cuda", torch.cuda.current_device()))
+            plan.set_initial_guess(plan.solve_lower_block(rows) if convention == "reference"
+                                   else rows)
         result = plan.solve(raise_on_error=False)
+        if result.status[0] != 0:
+            raise RuntimeError(f"B200 GMRES did not converge (status={result.status[0]})")
+        psi = result.system_psi(0)
+        if convention == "reference":
+            psi = plan.apply_lower_block(psi)
+        rows = psi.cpu().numpy()
     finally:
         plan.close()
-    if result.status[0] != 0:
-        raise RuntimeError(f"B200 GMRES did not converge (status={result.status[0]})")
     out = np.zeros((nkx, nky, nz), np.complex128)
-    out[system.channel_ix, system.channel_iy] = result.system_psi(0).cpu().numpy()
+    out[system.channel_ix, system.channel_iy] = rows
     return out
 
 
-def get_scattering_matrix_from_state(state: np.ndarray,
-                                     condition: ScatteringCondition) -> np.ndarray:
+def get_scattering_matrix_from_state(state: np.ndarray, condition: ScatteringCondition, *,
+                                     n_channels: int | None = None,
+                                     convention: Literal["reference", "psi"] = "reference"
+                                     ) -> np.ndarray:
     """|S_G0|^2 on the channel grid from a state of ``get_scattering_state``
     (``_multiscat.py:63-99``; S_G = 2i b_G psi_G(z_n) + delta_G0 a_0,
-    ``_multiscat.py:40-60``)."""
+    ``_multiscat.py:40-60``).  A reference-convention state (L psi) is mapped
+    back to psi by the forward Gauss-Seidel sweep L^-1 on the GPU, over the
+    channel set of ``n_channels`` as the reference does (``_multiscat.py:79-88``)."""
+    _check_convention(convention)
     arr = natural_arrays(condition)
     nkx, nky, nz = arr.potential_values.shape
-    psi_n = np.asarray(state, np.complex128).reshape(nkx, nky, nz)[:, :, -1]
+    grid = np.asarray(state, np.complex128).reshape(nkx, nky, nz)
+    if convention == "reference":
+        system = _reference_order_system(arr, n_channels)
+        plan = ScatteringPlan(arr.potential_values, arr.kinetic, [system], restart=1)
+        try:
+            rows = torch.as_tensor(np.ascontiguousarray(grid[system.channel_ix, system.channel_iy]),
+                                   device=torch.device("cuda", torch.cuda.current_device()))
+            psi = plan.solve_lower_block(rows).cpu().numpy()
+        finally:
+            plan.close()
+        grid = grid.copy()
+        grid[system.channel_ix, system.channel_iy] = psi
+    psi_n = grid[:, :, -1]
     b = np.asarray(arr.wave_b, np.complex128).reshape(nkx, nky)
     a = np.asarray(arr.wave_a, np.complex128).reshape(nkx, nky)
     s = 2.0j * b * psi_n

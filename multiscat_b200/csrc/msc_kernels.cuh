@@ -308,6 +308,152 @@ k_coupling(Tiles tiles, const int *__restrict__ gate, int n, int K,
 }
 
 // ---------------------------------------------------------------------------
+// Triangular parts of the channel coupling in plan row order (the row order
+// of a system is its channel order):
+//   mask 1 (lower): out = in0 + sgn * sum_{t: nbr < row} V_t src[nbr]
+//   mask 2 (upper): out = in0 + sgn * sum_{t: nbr > row} V_t src[nbr]
+// the reference's V^lower and V^upper of its block Gauss-Seidel splitting
+// A = L + U, L = D + V^lower (multiscat_gmres.f90:620-660, _scipy.py:81-102,
+// 262-297).  Same layout as k_coupling.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256)
+k_coupling_masked(Tiles tiles, const int *__restrict__ gate, int n, int K,
+                  const typename CT<R>::t *__restrict__ Vt, const int *__restrict__ nbr,
+                  const typename CT<R>::t *__restrict__ src,
+                  const typename CT<R>::t *__restrict__ in0, R sgn, int mask,
+                  typename CT<R>::t *__restrict__ out)
+{
+    using C2 = typename CT<R>::t;
+    extern __shared__ int nbm_s[];   // [kTileRows][K]
+    const int tile = blockIdx.x;
+    const int sys = tiles.sys[tile];
+    if (gate && gate[sys] == 0) return;
+    const int row0 = tiles.row0[tile];
+    const int nrow = tiles.nrow[tile];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int i = tid; i < nrow * K; i += blockDim.x * blockDim.y) {
+        const int row = row0 + i / K;
+        const int j = nbr[(size_t)row0 * K + i];
+        const bool keep = j >= 0 && (mask == 1 ? j < row : j > row);
+        nbm_s[i] = keep ? j : -1;
+    }
+    __syncthreads();
+    const int r = threadIdx.y;
+    const int z = blockIdx.y * blockDim.x + threadIdx.x;
+    if (r >= nrow || z >= n) return;
+    const int *nb = nbm_s + r * K;
+    R ar = 0, ai = 0;
+    for (int t = 0; t < K; ++t) {
+        const int j = nb[t];
+        if (j < 0) continue;
+        const C2 v = Vt[(size_t)t * n + z];
+        const C2 sv = src[(size_t)j * n + z];
+        ar = fma(v.x, sv.x, ar); ar = fma(-v.y, sv.y, ar);
+        ai = fma(v.x, sv.y, ai); ai = fma(v.y, sv.x, ai);
+    }
+    const size_t o = (size_t)(row0 + r) * n + z;
+    C2 base = in0 ? in0[o] : mk2<R>(0, 0);
+    out[o] = mk2<R>(base.x + sgn * ar, base.y + sgn * ai);
+}
+
+// ---------------------------------------------------------------------------
+// Block Gauss-Seidel forward sweep y = L^-1 x, L = D + V^lower: the
+// reference's solve_lower_block / _apply_inverse_lower_block
+// (multiscat_gmres.f90:641-687, _scipy.py:262-297), channel after channel
+//   y_r = D_r^-1 (x_r - sum_{r' < r} V_{r r'} y_{r'}).
+// One CTA per system.  Rows are taken level by level (a row's level is one
+// more than the highest level among its lower neighbours, so the rows of a
+// level do not depend on each other); the warps share a level's rows, one
+// row per warp, and a barrier closes every level.  D_r^-1 in the eigenbasis
+// of H0 with the Sherman-Morrison boundary term, as k_block_inverse:
+//   xt = E^T s, sigma = sum_k en_k xt_k / (pkd + lam_k),
+//   beta = c sigma / (1 - c f_n), y = E (xt + beta en) / (pkd + lam).
+// Vectors in R (FP32 in the mixed form's inner solve), arithmetic in FP64.
+// Dynamic shared memory: 2 n double2 per warp.
+// ---------------------------------------------------------------------------
+struct GsLevels {
+    const int *sys_lvl;     // [B + 1]  first level of each system
+    const int *lvl_start;   // [levels + 1]  first entry of each level in lvl_rows
+    const int *lvl_rows;    // [R]  rows, system by system, level by level
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+k_gs_sweep(int nsys, const int *__restrict__ gate, int n, int K,
+           const typename CT<R>::t *__restrict__ Vt, const int *__restrict__ nbr, GsLevels lv,
+           const double *__restrict__ E, const double *__restrict__ ET,
+           const double *__restrict__ lam, const double *__restrict__ en,
+           const double *__restrict__ row_pkd, const double2 *__restrict__ row_c,
+           const double *__restrict__ row_fn, const typename CT<R>::t *__restrict__ x,
+           typename CT<R>::t *__restrict__ y)
+{
+    using C2 = typename CT<R>::t;
+    extern __shared__ double2 gs_sm[];
+    const int s = blockIdx.x;
+    if (s >= nsys || (gate && gate[s] == 0)) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    double2 *sv = gs_sm + (size_t)warp * 2 * n;
+    double2 *tv = sv + n;
+    for (int L = lv.sys_lvl[s]; L < lv.sys_lvl[s + 1]; ++L) {
+        for (int i = lv.lvl_start[L] + warp; i < lv.lvl_start[L + 1]; i += nw) {
+            const int r = lv.lvl_rows[i];
+            const int *nb = nbr + (size_t)r * K;
+            for (int z = lane; z < n; z += 32) {
+                const C2 xv = x[(size_t)r * n + z];
+                double ar = (double)xv.x, ai = (double)xv.y;
+                for (int t = 0; t < K; ++t) {
+                    const int j = nb[t];
+                    if (j < 0 || j >= r) continue;
+                    const C2 v = Vt[(size_t)t * n + z];
+                    const C2 u = y[(size_t)j * n + z];
+                    ar -= (double)v.x * (double)u.x - (double)v.y * (double)u.y;
+                    ai -= (double)v.x * (double)u.y + (double)v.y * (double)u.x;
+                }
+                sv[z] = make_double2(ar, ai);
+            }
+            __syncwarp();
+            const double pk = row_pkd[r];
+            double sr = 0.0, si = 0.0;
+            for (int k = lane; k < n; k += 32) {
+                double ar = 0.0, ai = 0.0;
+                for (int z = 0; z < n; ++z) {
+                    const double e = __ldg(E + (size_t)z * n + k);
+                    ar = fma(e, sv[z].x, ar);
+                    ai = fma(e, sv[z].y, ai);
+                }
+                tv[k] = make_double2(ar, ai);
+                const double w = en[k] / (pk + lam[k]);
+                sr = fma(w, ar, sr);
+                si = fma(w, ai, si);
+            }
+            sr = warp_sum(sr);
+            si = warp_sum(si);
+            const double2 c = row_c[r];
+            const double fn = row_fn[r];
+            const double2 beta = cdiv(cmul(c, make_double2(sr, si)), make_double2(1.0 - c.x * fn, -c.y * fn));
+            for (int k = lane; k < n; k += 32) {
+                const double inv = 1.0 / (pk + lam[k]);
+                const double2 t = tv[k];
+                tv[k] = make_double2((t.x + beta.x * en[k]) * inv, (t.y + beta.y * en[k]) * inv);
+            }
+            __syncwarp();
+            for (int z = lane; z < n; z += 32) {
+                double ar = 0.0, ai = 0.0;
+                for (int k = 0; k < n; ++k) {
+                    const double e = __ldg(ET + (size_t)k * n + z);
+                    ar = fma(e, tv[k].x, ar);
+                    ai = fma(e, tv[k].y, ai);
+                }
+                y[(size_t)r * n + z] = mk2<R>((R)ar, (R)ai);
+            }
+            __syncwarp();
+        }
+        __syncthreads();    // this level's rows are written before the next level reads them
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Channel coupling with shared-memory halo tiles (the hot form of k_coupling).
 //
 // A block owns an 8 x BX patch of torus positions of ONE system and ZC
@@ -681,6 +827,7 @@ struct GmresState {
     int *active;      // [B]  iterating in this cycle
     int *kcyc;        // [B]  iterations done in this cycle
     int *iters;       // [B]  total iterations
+    int *projv;       // [B]  basis vectors projected against, summed over steps (j + 1 at step j)
     int *cycles;      // [B]  restart cycles started
     int *unfinished;  // [B]  1 until converged or failed
     int *status;      // [B]  msc_status
@@ -796,6 +943,7 @@ __device__ void arnoldi_givens(GmresState &st, int s, int m, int j, double rtol,
     st.est[s] = est;
     st.kcyc[s] = j + 1;
     st.iters[s] += 1;
+    st.projv[s] += j + 1;
     st.scale[s] = (beta > 0.0) ? 1.0 / beta : 0.0;
     bool stop = false;
     if (!isfinite(est) || !isfinite(beta)) stop = true;
@@ -1063,6 +1211,352 @@ k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
     }
     if (last_block_reduce(a, s, nvec + 1, st.h2 + (size_t)s * hs)) {
         if (threadIdx.x == 0) arnoldi_givens(st, s, m, j, rtol, max_iter, inner_rtol, cgs2 != 0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Arnoldi step with delayed re-orthogonalisation (DCGS2): two passes over the
+// basis per step instead of the three of CGS2.  Gram-Schmidt with the
+// second projection of q_j delayed to step j + 1 (Bielich, Langou, Thomas,
+// Swirydowicz, Yamazaki, Boman, "Low-synch Gram-Schmidt with delayed
+// reorthogonalization for Krylov solvers", Parallel Computing 112, 2022).
+//
+// At step j the basis slots hold q_0 .. q_{j-1} (final) and, in slot j, the
+// candidate v: the next vector projected once and not normalised; w = A M v.
+//   reduction  s = Q_{j-1}^H v, t = Q_{j-1}^H w, ||v||^2, v^H w
+//              nu = sqrt(||v||^2 - ||s||^2)   (q_j = (v - Q_{j-1} s) / nu)
+//              column j-1 of H is final: H[:j, j-1] += s, H[j, j-1] = nu
+//              Hs = Hbar s (unrotated Hessenberg, A M Q_{j-1} = Q_j Hbar)
+//              h_j[:j] = (t - Hs[:j]) / nu
+//              h_j[j]  = ((v^H w - s^H t) / nu - Hs[j]) / nu
+//   update     q_j     = v / nu - Q_{j-1} s / nu
+//              v_{j+1} = w / nu - (d / nu) v - Q_{j-1} (c - s d / nu),
+//              e = Hs / nu + h_j, c = e[:j], d = e[j]
+//              ||v_{j+1}||^2 -> provisional column j (H[j+1, j] = ||v_{j+1}||),
+//              its Givens rotation and the GMRES residual estimate.
+// The provisional column is made final (and its rotation redone) by the next
+// step's reduction, so the stop test runs on the step it belongs to: a
+// system that stops at step j never pays for the matvec of step j + 1.  The
+// column a cycle ends on stays provisional: its only difference from the
+// final one is the second projection of v_{j+1}, the loss-of-orthogonality
+// level that the FP64 true residual of the next cycle absorbs.
+// ---------------------------------------------------------------------------
+struct DcgsState {
+    double2 *Hraw;    // [B][(m+1)*m]  unrotated Hessenberg (column j at j*(m+1))
+    double2 *dsum;    // [B][2(m+1)]   per-system reduction results of the step
+    double2 *coef;    // [B][cstride]  update coefficients (see dcgs_coefficients)
+    double2 *gsave;   // [B]           g[j] before the provisional rotation j
+    int cstride;      // 2 m + 4
+};
+
+// Column j of H from its unrotated entries: apply rotations 0..j-1, make
+// rotation j from (H[j], H[j+1]) and update g (g[j] is taken from gsave,
+// g[j+1] starts at 0).  Returns the new residual estimate |g[j+1]|.
+__device__ double dcgs_rotate_column(GmresState &st, const DcgsState &ds, int s, int m, int j)
+{
+    const double2 *raw = ds.Hraw + (size_t)s * (m + 1) * m + (size_t)j * (m + 1);
+    double2 *H = st.H + (size_t)s * (m + 1) * m + (size_t)j * (m + 1);
+    double2 *cs = st.cs + (size_t)s * m;
+    double2 *sn = st.sn + (size_t)s * m;
+    double2 *g = st.g + (size_t)s * (m + 1);
+    for (int i = 0; i <= j + 1; ++i) H[i] = raw[i];
+    for (int i = 0; i < j; ++i) {
+        const double c = cs[i].x;
+        const double2 sv = sn[i];
+        const double2 a = H[i], b = H[i + 1];
+        H[i] = cadd(cscale(a, c), cmul(sv, b));
+        H[i + 1] = csub(cscale(b, c), cmul(cconj(sv), a));
+    }
+    const double2 a = H[j];
+    const double beta = H[j + 1].x;            // real, >= 0 (a norm)
+    const double aa = sqrt(cabs2(a));
+    const double r = hypot(aa, beta);
+    double c;
+    double2 sv;
+    if (r == 0.0) {
+        c = 1.0;
+        sv = make_double2(0.0, 0.0);
+    } else if (aa == 0.0) {
+        c = 0.0;
+        sv = make_double2(1.0, 0.0);
+    } else {
+        c = aa / r;
+        sv = cscale(cscale(a, 1.0 / aa), beta / r);
+    }
+    cs[j] = make_double2(c, 0.0);
+    sn[j] = sv;
+    H[j] = (aa == 0.0) ? make_double2(beta, 0.0) : cscale(a, r / aa);
+    H[j + 1] = make_double2(0.0, 0.0);
+    const double2 gj = ds.gsave[s];
+    g[j] = cscale(gj, c);
+    g[j + 1] = make_double2(-(sv.x * gj.x + sv.y * gj.y), -(sv.x * gj.y - sv.y * gj.x));
+    return sqrt(cabs2(g[j + 1]));
+}
+
+__device__ __forceinline__ bool dcgs_stop(const GmresState &st, int s, double est, double rtol,
+                                          double inner_rtol)
+{
+    return !isfinite(est) || est <= fmax(rtol * st.bnorm[s], inner_rtol * st.beta0[s]);
+}
+
+// Per-system scalar work of the reduction (one thread): finalise column j-1,
+// redo its rotation, form h_j and the update coefficients:
+//   coef[0..j)        a_i = -s_i / nu            (q_j = v / nu + sum a_i Q_i)
+//   coef[j+1 .. 2j+1) b_i = -(c_i - s_i d / nu)  (v_{j+1} = w / nu - (d / nu) v + sum b_i Q_i)
+//   coef[2m+2] = (1 / nu, 0), coef[2m+3] = -d / nu
+__device__ void dcgs_coefficients(GmresState &st, const DcgsState &ds, int s, int m, int j,
+                                  double rtol, double inner_rtol)
+{
+    const double2 *sum = ds.dsum + (size_t)s * 2 * (m + 1);
+    const double2 *sv = sum;               // s_i = q_i^H v, i < j;  sum[j] = ||v||^2
+    const double2 *tv = sum + (j + 1);     // t_i = q_i^H w, i < j;  tv[j] = v^H w
+    double2 *raw = ds.Hraw + (size_t)s * (m + 1) * m;
+    double2 *cf = ds.coef + (size_t)s * ds.cstride;
+    double ss = 0.0;
+    for (int i = 0; i < j; ++i) ss += cabs2(sv[i]);
+    const double nu2 = sum[j].x - ss;
+    const double nu = sqrt(fmax(nu2, 0.0));
+    if (j == 0) {
+        // v = q_0 up to rounding; g[0] = beta follows q_0 = v / nu
+        double2 *g = st.g + (size_t)s * (m + 1);
+        g[0] = cscale(g[0], nu);
+    } else {
+        double2 *col = raw + (size_t)(j - 1) * (m + 1);
+        for (int i = 0; i < j; ++i) col[i] = cadd(col[i], sv[i]);
+        col[j] = make_double2(nu, 0.0);
+        const double est = dcgs_rotate_column(st, ds, s, m, j - 1);
+        st.est[s] = est;
+        if (dcgs_stop(st, s, est, rtol, inner_rtol)) {
+            st.active[s] = 0;              // q_0 .. q_{j-1} are final; kcyc = j
+            return;
+        }
+    }
+    if (!(nu > 1e-300) || !isfinite(nu)) {
+        st.active[s] = 0;
+        return;
+    }
+    const double inu = 1.0 / nu;
+    // Hs = Hbar[:j+1, :j] s (column k has entries 0..k+1)
+    double2 hs[kMaxRestart + 1];
+    for (int i = 0; i <= j; ++i) hs[i] = make_double2(0.0, 0.0);
+    for (int k = 0; k < j; ++k) {
+        const double2 *col = raw + (size_t)k * (m + 1);
+        for (int i = 0; i <= k + 1; ++i) hs[i] = cadd(hs[i], cmul(col[i], sv[k]));
+    }
+    double2 sht = make_double2(0.0, 0.0);   // s^H t
+    for (int i = 0; i < j; ++i) sht = cadd(sht, cmul(cconj(sv[i]), tv[i]));
+    double2 *colj = raw + (size_t)j * (m + 1);
+    for (int i = 0; i < j; ++i) colj[i] = cscale(csub(tv[i], hs[i]), inu);
+    colj[j] = cscale(csub(cscale(csub(tv[j], sht), inu), hs[j]), inu);
+    const double2 d = cadd(cscale(hs[j], inu), colj[j]);
+    const double2 dn = cscale(d, inu);
+    for (int i = 0; i < j; ++i) {
+        const double2 ci = cadd(cscale(hs[i], inu), colj[i]);
+        cf[i] = cscale(sv[i], -inu);
+        cf[j + 1 + i] = make_double2(-(ci.x - (sv[i].x * dn.x - sv[i].y * dn.y)),
+                                     -(ci.y - (sv[i].x * dn.y + sv[i].y * dn.x)));
+    }
+    cf[2 * m + 2] = make_double2(inu, 0.0);
+    cf[2 * m + 3] = make_double2(-dn.x, -dn.y);
+}
+
+template <typename R> struct DcgsUnroll { static constexpr int value = 8; };
+template <> struct DcgsUnroll<double> { static constexpr int value = 4; };
+
+// Reduction pass of step j over row chunks.  Each warp takes sub-ranges of
+// 32 U elements of the block's chunk, holds v and w there in registers and
+// streams q_0 .. q_{j-1} and v itself (the basis slots 0 .. j), two dots per
+// vector (q_i^H v, q_i^H w), reduced across the warp per vector and added in
+// a fixed order (deterministic).  The last block of a system reduces the
+// per-block partials and runs dcgs_coefficients.
+template <typename R>
+__global__ void __launch_bounds__(256, 3)
+k_dcgs_reduce(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int j,
+              const typename CT<R>::t *__restrict__ W, GmresState st, DcgsState ds, int m,
+              double rtol, double inner_rtol)
+{
+    using C2 = typename CT<R>::t;
+    constexpr int U = DcgsUnroll<R>::value;
+    constexpr int NW = 8;
+    __shared__ double2 red[2 * (kMaxRestart + 1)][NW];
+    const int blk = blockIdx.x;
+    const int s = a.tiles.sys[blk];
+    if (a.gate && a.gate[s] == 0) return;
+    size_t e0;
+    int ne;
+    elem_range<R>(a, blk, 0, e0, ne);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nv = j + 1;                        // basis slots 0..j (slot j holds v)
+    for (int i = threadIdx.x; i < 2 * nv * NW; i += blockDim.x)
+        red[i / NW][i % NW] = make_double2(0.0, 0.0);
+    __syncthreads();
+    const C2 *vp = Q + (size_t)j * a.qstride + e0;
+    const C2 *wp = W + e0;
+    for (int base = warp * 32 * U; base < ne; base += NW * 32 * U) {
+        C2 vv[U], ww[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = base + u * 32 + lane;
+            vv[u] = (e < ne) ? vp[e] : mk2<R>(0, 0);
+            ww[u] = (e < ne) ? wp[e] : mk2<R>(0, 0);
+        }
+        for (int i = 0; i < nv; ++i) {
+            const C2 *q = Q + (size_t)i * a.qstride + e0;
+            C2 qv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = base + u * 32 + lane;
+                qv[u] = (e < ne) ? q[e] : mk2<R>(0, 0);
+            }
+            double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double qx = (double)qv[u].x, qy = (double)qv[u].y;
+                ar = fma(qx, (double)vv[u].x, fma(qy, (double)vv[u].y, ar));
+                ai = fma(qx, (double)vv[u].y, fma(-qy, (double)vv[u].x, ai));
+                br = fma(qx, (double)ww[u].x, fma(qy, (double)ww[u].y, br));
+                bi = fma(qx, (double)ww[u].y, fma(-qy, (double)ww[u].x, bi));
+            }
+            ar = warp_sum(ar);
+            ai = warp_sum(ai);
+            br = warp_sum(br);
+            bi = warp_sum(bi);
+            if (lane == 0) {
+                double2 &x = red[i][warp];
+                double2 &y = red[nv + i][warp];
+                x.x += ar; x.y += ai;
+                y.x += br; y.y += bi;
+            }
+        }
+    }
+    __syncthreads();
+    double2 *out = a.partial + (size_t)blk * a.pstride;
+    for (int i = threadIdx.x; i < 2 * nv; i += blockDim.x) {
+        double2 acc = red[i][0];
+        for (int w = 1; w < NW; ++w) {
+            acc.x += red[i][w].x;
+            acc.y += red[i][w].y;
+        }
+        out[i] = acc;
+    }
+    if (last_block_reduce(a, s, 2 * nv, ds.dsum + (size_t)s * 2 * (m + 1))) {
+        if (threadIdx.x == 0) dcgs_coefficients(st, ds, s, m, j, rtol, inner_rtol);
+    }
+}
+
+// Update pass of step j over row chunks: slot j <- q_j, slot j + 1 <- v_{j+1}
+// (one read of q_0 .. q_{j-1}, v, w; two writes), ||v_{j+1}||^2 reduced per
+// system; the last block forms the provisional column j and its rotation,
+// counts the iteration and applies the stop rules.
+template <typename R>
+__global__ void __launch_bounds__(256)
+k_dcgs_update(ArnoldiArgs a, typename CT<R>::t *__restrict__ Q, int j,
+              const typename CT<R>::t *__restrict__ W, GmresState st, DcgsState ds, int m,
+              double rtol, int max_iter, double inner_rtol)
+{
+    using C2 = typename CT<R>::t;
+    constexpr int UQ = 4;                        // basis vectors loaded per batch
+    __shared__ C2 ca[kMaxRestart], cb[kMaxRestart];
+    __shared__ double wsum[8];
+    const int blk = blockIdx.x;
+    const int s = a.tiles.sys[blk];
+    if (a.gate && a.gate[s] == 0) return;
+    const double2 *cf = ds.coef + (size_t)s * ds.cstride;
+    for (int i = threadIdx.x; i < j; i += blockDim.x) {
+        ca[i] = mk2<R>((R)cf[i].x, (R)cf[i].y);
+        cb[i] = mk2<R>((R)cf[j + 1 + i].x, (R)cf[j + 1 + i].y);
+    }
+    const R inu = (R)cf[2 * m + 2].x;
+    const C2 dv = mk2<R>((R)cf[2 * m + 3].x, (R)cf[2 * m + 3].y);
+    __syncthreads();
+    size_t e0;
+    int ne;
+    elem_range<R>(a, blk, 0, e0, ne);
+    C2 *vq = Q + (size_t)j * a.qstride + e0;           // v in, q_j out
+    C2 *vn = Q + (size_t)(j + 1) * a.qstride + e0;     // v_{j+1} out
+    const C2 *wp = W + e0;
+    // FP32: two consecutive elements per thread (16-byte loads) when every
+    // vector's chunk starts on an even element
+    const bool pairs = std::is_same<R, float>::value && (e0 % 2 == 0) && (a.qstride % 2 == 0);
+    const int step = pairs ? 2 : 1;
+    double nrm = 0.0;
+    for (int e = threadIdx.x * step; e < ne; e += blockDim.x * step) {
+        const bool two = pairs && e + 1 < ne;
+        C2 v0 = vq[e], v1 = two ? vq[e + 1] : mk2<R>(0, 0);
+        C2 w0 = wp[e], w1 = two ? wp[e + 1] : mk2<R>(0, 0);
+        // q = v / nu ; n = w / nu + dv v
+        C2 q0 = mk2<R>(v0.x * inu, v0.y * inu), q1 = mk2<R>(v1.x * inu, v1.y * inu);
+        C2 n0 = mk2<R>(w0.x * inu + (dv.x * v0.x - dv.y * v0.y), w0.y * inu + (dv.x * v0.y + dv.y * v0.x));
+        C2 n1 = mk2<R>(w1.x * inu + (dv.x * v1.x - dv.y * v1.y), w1.y * inu + (dv.x * v1.y + dv.y * v1.x));
+        for (int i0 = 0; i0 < j; i0 += UQ) {
+            C2 b0[UQ], b1[UQ];
+#pragma unroll
+            for (int u = 0; u < UQ; ++u) {
+                const int i = i0 + u;
+                b0[u] = mk2<R>(0, 0);
+                b1[u] = mk2<R>(0, 0);
+                if (i < j) {
+                    const C2 *qp = Q + (size_t)i * a.qstride + e0 + e;
+                    if (two) {
+                        const float4 t = *reinterpret_cast<const float4 *>(qp);
+                        b0[u] = mk2<R>((R)t.x, (R)t.y);
+                        b1[u] = mk2<R>((R)t.z, (R)t.w);
+                    } else {
+                        b0[u] = *qp;
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UQ; ++u) {
+                // past the last vector b0 = b1 = 0, so any coefficient works
+                const int i = min(i0 + u, j - 1);
+                const C2 x = ca[i], y = cb[i];
+                const C2 p0 = b0[u], p1 = b1[u];
+                q0.x = fma(p0.x, x.x, fma(-p0.y, x.y, q0.x));
+                q0.y = fma(p0.x, x.y, fma(p0.y, x.x, q0.y));
+                q1.x = fma(p1.x, x.x, fma(-p1.y, x.y, q1.x));
+                q1.y = fma(p1.x, x.y, fma(p1.y, x.x, q1.y));
+                n0.x = fma(p0.x, y.x, fma(-p0.y, y.y, n0.x));
+                n0.y = fma(p0.x, y.y, fma(p0.y, y.x, n0.y));
+                n1.x = fma(p1.x, y.x, fma(-p1.y, y.y, n1.x));
+                n1.y = fma(p1.x, y.y, fma(p1.y, y.x, n1.y));
+            }
+        }
+        vq[e] = q0;
+        vn[e] = n0;
+        nrm += (double)n0.x * n0.x + (double)n0.y * n0.y;
+        if (two) {
+            vq[e + 1] = q1;
+            vn[e + 1] = n1;
+            nrm += (double)n1.x * n1.x + (double)n1.y * n1.y;
+        }
+    }
+    nrm = warp_sum(nrm);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = nrm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += wsum[w];
+        a.partial[(size_t)blk * a.pstride] = make_double2(t, 0.0);
+    }
+    if (last_block_reduce(a, s, 1, st.h2 + (size_t)s * (m + 2))) {
+        if (threadIdx.x == 0) {
+            const double vn2 = st.h2[(size_t)s * (m + 2)].x;
+            const double beta = sqrt(fmax(vn2, 0.0));
+            double2 *col = ds.Hraw + (size_t)s * (m + 1) * m + (size_t)j * (m + 1);
+            col[j + 1] = make_double2(beta, 0.0);
+            ds.gsave[s] = st.g[(size_t)s * (m + 1) + j];
+            const double est = dcgs_rotate_column(st, ds, s, m, j);
+            st.est[s] = est;
+            st.kcyc[s] = j + 1;
+            st.iters[s] += 1;
+            st.projv[s] += j + 1;
+            bool stop = dcgs_stop(st, s, est, rtol, inner_rtol) || !isfinite(beta);
+            if (j + 1 >= m) stop = true;
+            if (st.iters[s] >= max_iter) stop = true;
+            if (beta <= 1e-300) stop = true;
+            if (stop) st.active[s] = 0;
+        }
     }
 }
 

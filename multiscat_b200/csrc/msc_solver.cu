@@ -26,6 +26,7 @@
 #include <map>
 #include <mutex>
 #include <new>
+#include <numeric>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -33,6 +34,7 @@
 #include "../../include/multiscat_b200.h"
 #include "msc_common.cuh"
 #include "msc_eigh.hpp"
+#include "msc_eigh_gpu.cuh"
 #include "msc_kernels.cuh"
 #include "msc_tc.cuh"
 
@@ -167,6 +169,14 @@ struct msc_plan {
     // solver state
     DevBuf<double2> X, W, U, TMP, Q, partial;
     DevBuf<double2> H, cs, sn, g, h1, h2, y;
+    DevBuf<double2> Hraw, dsum, dcoef, gsave;   // DCGS2 Arnoldi step (see k_dcgs_reduce)
+    // block Gauss-Seidel (flags bit 5, and the lower-block entry points):
+    // level sets of every system's rows (k_gs_sweep)
+    bool gs = false;
+    bool gs_ready = false;
+    int gs_warps = 8;
+    DevBuf<int> gs_sys_lvl, gs_lvl_start, gs_lvl_rows;
+    bool dcgs = true;              // DCGS2 (two basis passes per step); false: CGS2
     DevBuf<double> scale, bnorm, resid, est, beta0;
     // mixed form: FP32 copies of the operator data and the FP32 Krylov space
     bool mixed = false;
@@ -187,7 +197,7 @@ struct msc_plan {
     size_t tc_smem = 0, tc2_smem = 0;
     DevBuf<__nv_bfloat16> e_img;
     DevBuf<int> tc_error;
-    DevBuf<int> active, kcyc, iters, cycles, unfinished, status, counter;
+    DevBuf<int> active, kcyc, iters, projv, cycles, unfinished, status, counter;
     int *counter_host = nullptr;   // pinned
     // Arnoldi blocks: runs of rows of one system ("chunks", first projection)
     // and row tiles split `split` ways (update + second projection)
@@ -216,6 +226,7 @@ struct msc_plan {
     int *kcyc_host = nullptr;            // pinned [B]
     int64_t launches_last = 0;
     int cycles_last = 0;
+    int fallbacks_last = 0;              // systems re-solved in FP64 by the last msc_solve
     int64_t launches_start = 0, launches_start0 = 0, launches_iter = 0;   // kernel nodes per graph
 
     ~msc_plan()
@@ -236,13 +247,16 @@ struct msc_plan {
         row_sys.release(); X.release(); W.release(); U.release(); TMP.release(); Q.release();
         partial.release(); H.release(); cs.release(); sn.release(); g.release(); h1.release();
         h2.release(); y.release(); scale.release(); bnorm.release(); resid.release();
-        est.release(); active.release(); kcyc.release(); iters.release(); cycles.release();
+        est.release(); active.release(); kcyc.release(); iters.release(); projv.release();
+        cycles.release();
         unfinished.release(); status.release(); counter.release(); beta0.release();
         sys_counter.release(); work.release(); tap_window.release(); taps_d.release();
         E32.release(); ET32.release(); lam32.release(); en32.release(); row_pkd32.release();
         row_fn32.release(); Vt32.release(); row_c32.release(); Q32.release(); W32.release();
         T32.release(); T64.release(); X0.release();
         U32.release(); R64.release(); e_img.release(); tc_error.release();
+        Hraw.release(); dsum.release(); dcoef.release(); gsave.release();
+        gs_sys_lvl.release(); gs_lvl_start.release(); gs_lvl_rows.release();
     }
 
     msc::Tiles tiles() const
@@ -258,9 +272,17 @@ struct msc_plan {
         msc::GmresState s;
         s.H = H.p; s.cs = cs.p; s.sn = sn.p; s.g = g.p; s.h1 = h1.p; s.h2 = h2.p; s.y = y.p;
         s.scale = scale.p; s.bnorm = bnorm.p; s.resid = resid.p; s.est = est.p; s.beta0 = beta0.p;
-        s.active = active.p; s.kcyc = kcyc.p; s.iters = iters.p; s.cycles = cycles.p;
+        s.active = active.p; s.kcyc = kcyc.p; s.iters = iters.p; s.projv = projv.p;
+        s.cycles = cycles.p;
         s.unfinished = unfinished.p; s.status = status.p; s.counter = counter.p;
         return s;
+    }
+    msc::DcgsState dstate() const
+    {
+        msc::DcgsState d;
+        d.Hraw = Hraw.p; d.dsum = dsum.p; d.coef = dcoef.p; d.gsave = gsave.p;
+        d.cstride = 2 * m + 4;
+        return d;
     }
 };
 
@@ -460,6 +482,29 @@ void launch_coupling(msc_plan *p, const int *gate, const double2 *src, const dou
     launch_coupling_t<double>(p, gate, src, in0, sgn, out, st);
 }
 
+// Lower (mask 1) or upper (mask 2) part of the coupling in plan row order.
+template <typename R>
+void launch_coupling_masked_t(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0,
+                              R sgn, int mask, C2<R> *out, cudaStream_t st)
+{
+    dim3 grid(p->ntiles, (p->n + 31) / 32);
+    dim3 block(32, msc::kTileRows);
+    msc::k_coupling_masked<R><<<grid, block, smem_coupling(std::max(p->K, 1)), st>>>(
+        p->tiles(), gate, p->n, p->K, OpData<R>::Vt(p), p->nbr.p, src, in0, sgn, mask, out);
+}
+
+size_t gs_smem(int n, int warps) { return (size_t)warps * 2 * n * sizeof(double2); }
+
+// y = L^-1 x (block Gauss-Seidel forward sweep), one CTA per system.
+template <typename R>
+void launch_gs_sweep_t(msc_plan *p, const int *gate, const C2<R> *x, C2<R> *y, cudaStream_t st)
+{
+    const msc::GsLevels lv{p->gs_sys_lvl.p, p->gs_lvl_start.p, p->gs_lvl_rows.p};
+    msc::k_gs_sweep<R><<<p->B, 32 * p->gs_warps, gs_smem(p->n, p->gs_warps), st>>>(
+        p->B, gate, p->n, p->K, OpData<R>::Vt(p), p->nbr.p, lv, p->E.p, p->ET.p, p->lam.p, p->en.p,
+        p->row_pkd.p, p->row_c.p, p->row_fn.p, x, y);
+}
+
 template <typename R>
 void launch_dots_t(msc_plan *p, const int *gate, const C2<R> *Q, int nvec, const C2<R> *W,
                    int with_norm, cudaStream_t st)
@@ -574,15 +619,28 @@ void apply_precond_t(msc_plan *p, const int *gate, const C2<R> *x, C2<R> *out, C
                      C2<R> *term, cudaStream_t st)
 {
     const int k = p->desc.precond_order;
+    // block-diagonal form: base D^-1, coupling V; Gauss-Seidel form: base
+    // L^-1 (forward sweep), coupling U (strictly upper part), so that order 1
+    // is the reference's Neumann-preconditioned Gauss-Seidel operator
+    // (multiscat_gmres.f90:452-475, _gmres.py:55-71)
+    auto base = [&](const C2<R> *in, C2<R> *o) {
+        if (p->gs)
+            launch_gs_sweep_t<R>(p, gate, in, o, st);
+        else
+            launch_block_inverse_t<R>(p, gate, in, o, 0, st);
+    };
     if (k <= 0) {
-        launch_block_inverse_t<R>(p, gate, x, out, 0, st);
+        base(x, out);
         return;
     }
-    launch_block_inverse_t<R>(p, gate, x, term, 0, st);
+    base(x, term);
     msc::k_copy_add<R><<<elementwise_grid(p), 256, 0, st>>>(p->tiles(), gate, p->n, term, out, 0);
     for (int i = 0; i < k; ++i) {
-        launch_coupling_t<R>(p, gate, term, nullptr, R(-1), scratch, st);
-        launch_block_inverse_t<R>(p, gate, scratch, term, 0, st);
+        if (p->gs)
+            launch_coupling_masked_t<R>(p, gate, term, nullptr, R(-1), 2, scratch, st);
+        else
+            launch_coupling_t<R>(p, gate, term, nullptr, R(-1), scratch, st);
+        base(scratch, term);
         msc::k_copy_add<R><<<elementwise_grid(p), 256, 0, st>>>(p->tiles(), gate, p->n, term, out, 1);
     }
 }
@@ -607,12 +665,32 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
         // w = A M q_j.  (D + V) M_k = I + (-1)^k (V D^-1)^{k+1} telescopes, so
         // w = q_j + V term_k with term_k = (-D^-1 V)^k D^-1 q_j the last term
         // of the series (for k = 0, term_0 = U = D^-1 q_j).
+        // Gauss-Seidel form: (L + U) M_k = I + (-1)^k (U L^-1)^{k+1} likewise,
+        // so w = q_j + U term_k with the strictly upper coupling only
         const C2<R> *last = p->desc.precond_order > 0 ? precond_term<R>(p) : U;
-        launch_coupling_t<R>(p, p->active.p, last, Qj, R(1), W, st);
+        if (p->gs)
+            launch_coupling_masked_t<R>(p, p->active.p, last, Qj, R(1), 2, W, st);
+        else
+            launch_coupling_t<R>(p, p->active.p, last, Qj, R(1), W, st);
         if (tm) mark(p, 1, j, 1, st);
         const msc::ArnoldiArgs a1 = arnoldi_args(p, p->active.p, true);
         const msc::ArnoldiArgs a2 = arnoldi_args(p, p->active.p, false);
         const unsigned nblk1 = (unsigned)p->nchunks;
+        if (p->dcgs) {
+            // DCGS2: the reduction finalises column j - 1 and forms the
+            // update coefficients; the update writes q_j and the next
+            // candidate into slots j and j + 1 and runs the stop test.
+            if (tm) mark(p, 2, j, 0, st);
+            msc::k_dcgs_reduce<R><<<nblk1, 256, 0, st>>>(a1, Q, j, W, p->state(), p->dstate(),
+                                                         p->m, p->desc.rtol, inner);
+            if (tm) mark(p, 2, j, 1, st);
+            if (tm) mark(p, 3, j, 0, st);
+            msc::k_dcgs_update<R><<<nblk1, 256, 0, st>>>(a1, Q, j, W, p->state(), p->dstate(),
+                                                         p->m, p->desc.rtol,
+                                                         p->desc.max_iterations, inner);
+            if (tm) mark(p, 3, j, 1, st);
+            continue;
+        }
         const unsigned nblk2 = (unsigned)(p->ntiles * p->split);
         // Two Gram-Schmidt passes; the mixed form may opt into one pass with
         // the Pythagorean norm (the FP64 true residual of the next refinement
@@ -636,7 +714,7 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
     msc::k_trisolve<<<sys_blocks(p->B), 128, 0, st>>>(p->state(), p->B, p->m);
     launch_update_t<R>(p, p->kcyc.p, Q, 0, p->kcyc.p, p->y.p, p->m, nullptr, nullptr, U, 1, st);
     if (tm) mark(p, 0, p->m, 0, st);
-    if (p->desc.precond_order > 0) {
+    if (p->gs || p->desc.precond_order > 0) {
         // W = M U (U is free after the first block inverse and serves as scratch)
         apply_precond_t<R>(p, p->kcyc.p, U, W, U, precond_term<R>(p), st);
         if (!p->mixed)
@@ -1129,6 +1207,8 @@ struct SetupTimer {
     }
 };
 
+msc_status ensure_gs_levels(msc_plan *p);
+
 msc_status finalize(msc_plan *p)
 {
     if (p->finalized) return MSC_OK;
@@ -1280,7 +1360,7 @@ msc_status finalize(msc_plan *p)
     tm.mark("tile uploads");
     const size_t vs = (size_t)p->R * n;
     const int m = p->m;
-    p->pstride = m + 2;
+    p->pstride = 2 * m + 2;      // slots per block: 2 (m + 1) dots of a DCGS2 reduction
     MSC_CUDA(p->X.alloc(vs));
     MSC_CUDA(p->TMP.alloc(vs));
     if (p->mixed) {
@@ -1337,6 +1417,12 @@ msc_status finalize(msc_plan *p)
     MSC_CUDA(p->h1.alloc((size_t)p->B * (m + 2)));
     MSC_CUDA(p->h2.alloc((size_t)p->B * (m + 2)));
     MSC_CUDA(p->y.alloc((size_t)p->B * m));
+    MSC_CUDA(p->Hraw.alloc((size_t)p->B * (m + 1) * m));
+    MSC_CUDA(p->dsum.alloc((size_t)p->B * 2 * (m + 1)));
+    MSC_CUDA(p->dcoef.alloc((size_t)p->B * (2 * m + 4)));
+    MSC_CUDA(p->gsave.alloc(p->B));
+    MSC_CUDA(cudaMemset(p->Hraw.p, 0, p->Hraw.count * sizeof(double2)));
+    MSC_CUDA(cudaMemset(p->dcoef.p, 0, p->dcoef.count * sizeof(double2)));
     MSC_CUDA(p->scale.alloc(p->B));
     MSC_CUDA(p->resid.alloc(p->B));
     MSC_CUDA(p->beta0.alloc(p->B));
@@ -1344,6 +1430,7 @@ msc_status finalize(msc_plan *p)
     MSC_CUDA(p->active.alloc(p->B));
     MSC_CUDA(p->kcyc.alloc(p->B));
     MSC_CUDA(p->iters.alloc(p->B));
+    MSC_CUDA(p->projv.alloc(p->B));
     MSC_CUDA(p->cycles.alloc(p->B));
     MSC_CUDA(p->unfinished.alloc(p->B));
     MSC_CUDA(p->status.alloc(p->B));
@@ -1363,6 +1450,11 @@ msc_status finalize(msc_plan *p)
         if (tst != MSC_OK) return tst;
     }
     tm.mark("autotune");
+    if (p->gs) {
+        msc_status gst = ensure_gs_levels(p);
+        if (gst != MSC_OK) return gst;
+        tm.mark("Gauss-Seidel levels");
+    }
     MSC_CUDA(cudaMallocHost(&p->kcyc_host, p->B * sizeof(int)));
     for (int s = 0; s < p->B; ++s) p->kcyc_host[s] = 0;
     p->tev.resize((size_t)msc_plan::kKinds * (m + 1) * 2);
@@ -1375,6 +1467,146 @@ msc_status finalize(msc_plan *p)
     if (st != MSC_OK) return st;
     tm.mark("graph capture");
     p->finalized = true;
+    return MSC_OK;
+}
+
+// Level sets of the block Gauss-Seidel sweep: a row's level is one more
+// than the highest level among its lower neighbours (neighbour rows of the
+// same system with a smaller row index, through any coupling tap), so the
+// rows of one level can be solved at the same time.  Built once per plan.
+msc_status ensure_gs_levels(msc_plan *p)
+{
+    if (p->gs_ready) return MSC_OK;
+    const int ntor = p->nkx * p->nky;
+    std::vector<int> sys_lvl(p->B + 1, 0), lvl_start, rows;
+    rows.reserve(p->R);
+    std::vector<int> pos_row(ntor, -1);
+    for (int s = 0; s < p->B; ++s) {
+        const SystemHost &sh = p->sys[s];
+        for (int j = 0; j < sh.C; ++j) pos_row[sh.ix[j] * p->nky + sh.iy[j]] = j;
+        std::vector<int> lvl(sh.C, 0);
+        int nlvl = 0;
+        for (int j = 0; j < sh.C; ++j) {
+            int best = -1;
+            for (int t = 0; t < p->K; ++t) {
+                int sx = sh.ix[j] - p->taps[t].first;
+                sx += sx < 0 ? p->nkx : 0;
+                int sy = sh.iy[j] - p->taps[t].second;
+                sy += sy < 0 ? p->nky : 0;
+                const int q = pos_row[sx * p->nky + sy];
+                if (q >= 0 && q < j) best = std::max(best, lvl[q]);
+            }
+            lvl[j] = best + 1;
+            nlvl = std::max(nlvl, lvl[j] + 1);
+        }
+        sys_lvl[s] = (int)lvl_start.size();
+        std::vector<int> count(nlvl + 1, 0);
+        for (int j = 0; j < sh.C; ++j) ++count[lvl[j] + 1];
+        for (int l = 0; l < nlvl; ++l) count[l + 1] += count[l];
+        const int base = (int)rows.size();
+        rows.resize(base + sh.C);
+        std::vector<int> fill(count.begin(), count.end() - 1);
+        for (int j = 0; j < sh.C; ++j) rows[base + fill[lvl[j]]++] = p->sys_row0_h[s] + j;
+        for (int l = 0; l < nlvl; ++l) lvl_start.push_back(base + count[l]);
+        for (int j = 0; j < sh.C; ++j) pos_row[sh.ix[j] * p->nky + sh.iy[j]] = -1;
+    }
+    sys_lvl[p->B] = (int)lvl_start.size();
+    lvl_start.push_back((int)rows.size());
+    MSC_CUDA(upload(p->gs_sys_lvl, sys_lvl));
+    MSC_CUDA(upload(p->gs_lvl_start, lvl_start));
+    MSC_CUDA(upload(p->gs_lvl_rows, rows));
+    int dev = 0, optin = 0;
+    MSC_CUDA(cudaGetDevice(&dev));
+    MSC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    p->gs_warps = 8;
+    while (p->gs_warps > 1 && gs_smem(p->n, p->gs_warps) > (size_t)optin - 4096) p->gs_warps /= 2;
+    const int bytes = (int)gs_smem(p->n, p->gs_warps);
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_gs_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_gs_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_masked<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_coupling(msc::kMaxTaps)));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_masked<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_coupling(msc::kMaxTaps)));
+    p->gs_ready = true;
+    return MSC_OK;
+}
+
+// FP64 eigen-decomposition H = E diag(w) E^T of a symmetric n x n host
+// matrix on the current device (msc_eigh_gpu.cuh): Householder reduction and
+// both O(n^3) accumulations on the GPU, the O(n^2) tridiagonal QR iteration
+// on the host.  w ascending; E row-major, eigenvector k in column k.
+msc_status device_symmetric_eigh(int n, const double *H, double *w, double *E)
+{
+    namespace eg = msc::eig;
+    DevBuf<double> A, R, d, e, Zt, Ed, rc, rs;
+    DevBuf<int> applied, rk, dest;
+    std::vector<double> Hh(H, H + (size_t)n * n);
+    MSC_CUDA(upload(A, Hh));
+    MSC_CUDA(R.alloc((size_t)n * n));
+    MSC_CUDA(d.alloc(n));
+    MSC_CUDA(e.alloc(n));
+    MSC_CUDA(applied.alloc(n));
+    MSC_CUDA(cudaMemset(R.p, 0, (size_t)n * n * sizeof(double)));
+    MSC_CUDA(cudaMemset(e.p, 0, (size_t)n * sizeof(double)));
+    const size_t tri_smem = n <= eg::kTriSmemMaxN ? (size_t)n * n * sizeof(double) : 0;
+    MSC_CUDA(cudaFuncSetAttribute(eg::k_tridiagonalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((size_t)eg::kTriSmemMaxN * eg::kTriSmemMaxN * sizeof(double))));
+    eg::k_tridiagonalize<<<1, eg::kTriThreads, tri_smem>>>(n, A.p, R.p, d.p, e.p, applied.p);
+    MSC_CUDA(cudaGetLastError());
+    std::vector<double> dh(n), eh(n);
+    MSC_CUDA(cudaMemcpy(dh.data(), d.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    MSC_CUDA(cudaMemcpy(eh.data(), e.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    eh[n - 1] = 0.0;
+    std::vector<int> rkh;
+    std::vector<double> rch, rsh;
+    rkh.reserve((size_t)n * n);
+    rch.reserve((size_t)n * n);
+    rsh.reserve((size_t)n * n);
+    if (msc::tridiagonal_qr_rotations(n, dh, eh, rkh, rch, rsh) != 0)
+        return fail(MSC_ERR_EIGEN, "eigensolver did not converge");
+    const int nrot = (int)rkh.size();
+    if (nrot > 0) {
+        MSC_CUDA(upload(rk, rkh));
+        MSC_CUDA(upload(rc, rch));
+        MSC_CUDA(upload(rs, rsh));
+    }
+    MSC_CUDA(Zt.alloc((size_t)n * n));
+    // rows of Z per CTA: as many as fit 200 KB of shared memory (32 or 16)
+    if ((size_t)n * 32 * sizeof(double) <= 200 * 1024) {
+        const size_t sm = (size_t)n * 32 * sizeof(double);
+        MSC_CUDA(cudaFuncSetAttribute(eg::k_apply_rotations<32>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        eg::k_apply_rotations<32><<<(n + 31) / 32, 32, sm>>>(n, nrot, rk.p, rc.p, rs.p, Zt.p);
+    } else {
+        const size_t sm = (size_t)n * 16 * sizeof(double);
+        MSC_CUDA(cudaFuncSetAttribute(eg::k_apply_rotations<16>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        eg::k_apply_rotations<16><<<(n + 15) / 16, 16, sm>>>(n, nrot, rk.p, rc.p, rs.p, Zt.p);
+    }
+    MSC_CUDA(cudaGetLastError());
+    // ascending order: column j of Q_H Z goes to column dest[j]
+    std::vector<int> order(n), desth(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int i, int j) { return dh[i] < dh[j]; });
+    for (int k = 0; k < n; ++k) {
+        desth[order[k]] = k;
+        w[k] = dh[order[k]];
+    }
+    MSC_CUDA(upload(dest, desth));
+    MSC_CUDA(Ed.alloc((size_t)n * n));
+    if ((size_t)n * 32 * sizeof(double) <= 200 * 1024) {
+        const size_t sm = (size_t)n * 32 * sizeof(double);
+        MSC_CUDA(cudaFuncSetAttribute(eg::k_back_transform<32>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        eg::k_back_transform<32><<<(n + 31) / 32, 256, sm>>>(n, R.p, applied.p, Zt.p, dest.p, Ed.p);
+    } else {
+        const size_t sm = (size_t)n * 16 * sizeof(double);
+        MSC_CUDA(cudaFuncSetAttribute(eg::k_back_transform<16>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        eg::k_back_transform<16><<<(n + 15) / 16, 256, sm>>>(n, R.p, applied.p, Zt.p, dest.p, Ed.p);
+    }
+    MSC_CUDA(cudaGetLastError());
+    MSC_CUDA(cudaMemcpy(E, Ed.p, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToHost));
     return MSC_OK;
 }
 
@@ -1405,6 +1637,82 @@ void eigen_cache_store(const std::vector<double> &H, const std::vector<double> &
     std::lock_guard<std::mutex> lock(g_cache_mutex);
     if (g_eigen_cache.size() >= 8) g_eigen_cache.erase(g_eigen_cache.begin());
     g_eigen_cache.push_back({H, lam, E});
+}
+
+// FP64 recovery of the systems a mixed-precision solve left unconverged.
+// The FP32 inner solve of a hard beam can stall near its own rounding level
+// (residual ~1e-5) before max_refinements runs out.  Those systems are
+// solved again by a plain FP64 plan over the same potential, holding only
+// them: same operator (forward or adjoint), same right-hand sides, the mixed
+// solution as the initial guess (zero for a system whose state went
+// non-finite), FP64 restart and iteration limits of the parent's options.
+// Their rows of the parent's x are then replaced by the FP64 solution and
+// their iteration counts, status and residual by the FP64 solve's.
+msc_status fp64_recover(msc_plan *p, const std::vector<int> &failed, const std::vector<int> &status,
+                        std::vector<msc_result> &out)
+{
+    const int nf = (int)failed.size();
+    const int n = p->n;
+    msc_plan_desc d = p->desc;
+    d.precision = MSC_PRECISION_FP64;
+    d.n_systems = nf;
+    d.flags = 0;
+    msc_plan *c = nullptr;
+    msc_status st = msc_plan_create(&c, &d);
+    if (st != MSC_OK) return st;
+    struct Guard {
+        msc_plan *c;
+        ~Guard() { msc_plan_destroy(c); }
+    } guard{c};
+    // the potential in its [nkx][nky][n] layout from the parent's taps and V_00
+    std::vector<double2> V((size_t)p->nkx * p->nky * n, double2{0.0, 0.0});
+    for (int k = 0; k < n; ++k) V[k] = double2{p->v00_host[k], 0.0};
+    for (int t = 0; t < p->K; ++t) {
+        double2 *dst = V.data() + ((size_t)p->taps[t].first * p->nky + p->taps[t].second) * n;
+        std::copy(p->Vt_host.begin() + (size_t)t * n, p->Vt_host.begin() + (size_t)(t + 1) * n, dst);
+    }
+    st = msc_plan_set_potential(c, reinterpret_cast<const double *>(V.data()), p->T_host.data());
+    if (st != MSC_OK) return st;
+    for (int k = 0; k < nf; ++k) {
+        const SystemHost &sh = p->sys[failed[k]];
+        c->sys[k] = sh;
+    }
+    st = finalize(c);
+    if (st != MSC_OK) return st;
+    if (p->adjoint) {
+        st = msc_plan_set_adjoint(c, 1);
+        if (st != MSC_OK) return st;
+    }
+    // right-hand sides and initial guesses: the parent's rows of each system
+    const size_t vs = (size_t)c->R * n;
+    MSC_CUDA(c->X0.alloc(vs));
+    cudaStream_t cs = c->stream;
+    for (int k = 0; k < nf; ++k) {
+        const int s = failed[k];
+        const int r0 = p->sys_row0_h[s], C = p->sys[s].C, q0 = c->sys_row0_h[k];
+        MSC_CUDA(cudaMemcpyAsync(c->row_rhs.p + q0, p->row_rhs.p + r0, C * sizeof(double2),
+                                 cudaMemcpyDeviceToDevice, cs));
+        if (status[s] == MSC_ERR_NONFINITE)
+            MSC_CUDA(cudaMemsetAsync(c->X0.p + (size_t)q0 * n, 0, (size_t)C * n * sizeof(double2), cs));
+        else
+            MSC_CUDA(cudaMemcpyAsync(c->X0.p + (size_t)q0 * n, p->X.p + (size_t)r0 * n,
+                                     (size_t)C * n * sizeof(double2), cudaMemcpyDeviceToDevice, cs));
+    }
+    msc::k_system_norms<<<c->B, 256, 0, cs>>>(c->sys_row0.p, c->row_rhs.p, c->bnorm.p);
+    MSC_CUDA(cudaGetLastError());
+    MSC_CUDA(cudaStreamSynchronize(cs));
+    c->has_x0 = true;
+    out.assign(nf, msc_result{});
+    st = msc_solve(c, nullptr, nullptr, out.data(), cs);
+    if (st != MSC_OK && st != MSC_ERR_NOT_CONVERGED && st != MSC_ERR_NONFINITE) return st;
+    for (int k = 0; k < nf; ++k) {
+        const int s = failed[k];
+        const int r0 = p->sys_row0_h[s], C = p->sys[s].C, q0 = c->sys_row0_h[k];
+        MSC_CUDA(cudaMemcpyAsync(p->X.p + (size_t)r0 * n, c->X.p + (size_t)q0 * n,
+                                 (size_t)C * n * sizeof(double2), cudaMemcpyDeviceToDevice, cs));
+    }
+    MSC_CUDA(cudaStreamSynchronize(cs));
+    return MSC_OK;
 }
 
 }  // namespace
@@ -1448,8 +1756,11 @@ msc_status msc_plan_create(msc_plan **plan, const msc_plan_desc *desc)
         p->m = desc->inner_restart > 0 ? desc->inner_restart : std::min(desc->restart, 20);
         p->inner_rtol = desc->inner_rtol > 0.0 ? desc->inner_rtol : 1e-5;
         p->cgs1_inner = (desc->flags & 4) != 0;
+        if (p->cgs1_inner) p->dcgs = false;
         p->max_cycles = desc->max_refinements > 0 ? desc->max_refinements : 30;
     }
+    if (desc->flags & 16) p->dcgs = false;     // classical Gram-Schmidt, two passes (CGS2)
+    if (desc->flags & 32) p->gs = true;        // block Gauss-Seidel preconditioner M = L^-1
     p->sys.resize(p->B);
     msc_status st = set_kernel_attributes(p->n, 0);
     if (st != MSC_OK) { delete p; return st; }
@@ -1502,8 +1813,8 @@ msc_status msc_plan_set_potential(msc_plan *p, const double *potential_values, c
     if (!eigen_cache_lookup(H, p->lam_host, p->E_host)) {
         p->lam_host.resize(n);
         p->E_host.resize((size_t)n * n);
-        if (msc::symmetric_eigh(n, H.data(), p->lam_host.data(), p->E_host.data()) != 0)
-            return fail(MSC_ERR_EIGEN, "eigensolver did not converge");
+        msc_status est = device_symmetric_eigh(n, H.data(), p->lam_host.data(), p->E_host.data());
+        if (est != MSC_OK) return est;
         eigen_cache_store(H, p->lam_host, p->E_host);
     }
     p->en_host.resize(n);
@@ -1654,6 +1965,7 @@ msc_status msc_solve(msc_plan *p, double *psi_out, double *intensities_out, msc_
     else
         MSC_CUDA(cudaMemsetAsync(p->X.p, 0, vs * sizeof(double2), ps));
     MSC_CUDA(cudaMemsetAsync(p->iters.p, 0, p->B * sizeof(int), ps));
+    MSC_CUDA(cudaMemsetAsync(p->projv.p, 0, p->B * sizeof(int), ps));
     MSC_CUDA(cudaMemsetAsync(p->cycles.p, 0, p->B * sizeof(int), ps));
     MSC_CUDA(cudaMemsetAsync(p->status.p, 0, p->B * sizeof(int), ps));
     MSC_CUDA(cudaMemsetAsync(p->kcyc.p, 0, p->B * sizeof(int), ps));
@@ -1687,6 +1999,42 @@ msc_status msc_solve(msc_plan *p, double *psi_out, double *intensities_out, msc_
         MSC_CUDA(cudaMemcpy(&tc_err, p->tc_error.p, sizeof(int), cudaMemcpyDeviceToHost));
         if (tc_err) return fail(MSC_ERR_CUDA, "tensor-core block inverse timed out on an mbarrier wait");
     }
+    std::vector<int> iters(p->B), cycles(p->B), status(p->B), unfinished(p->B), fallback(p->B, 0);
+    std::vector<int> projv(p->B);
+    std::vector<double> resid(p->B);
+    MSC_CUDA(cudaMemcpyAsync(iters.data(), p->iters.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaMemcpyAsync(projv.data(), p->projv.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaMemcpyAsync(cycles.data(), p->cycles.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaMemcpyAsync(status.data(), p->status.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaMemcpyAsync(unfinished.data(), p->unfinished.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaMemcpyAsync(resid.data(), p->resid.p, p->B * sizeof(double), cudaMemcpyDeviceToHost, ps));
+    MSC_CUDA(cudaStreamSynchronize(ps));
+    for (int s = 0; s < p->B; ++s)
+        if (unfinished[s]) status[s] = MSC_ERR_NOT_CONVERGED;
+    p->fallbacks_last = 0;
+    if (p->mixed && !(p->desc.flags & 8)) {
+        std::vector<int> failed;
+        for (int s = 0; s < p->B; ++s)
+            if (status[s] == MSC_ERR_NOT_CONVERGED || status[s] == MSC_ERR_NONFINITE) failed.push_back(s);
+        if (!failed.empty()) {
+            std::vector<msc_result> rec;
+            msc_status rst = fp64_recover(p, failed, status, rec);
+            if (rst != MSC_OK) {
+                cudaEventDestroy(ev);
+                return rst;
+            }
+            for (size_t k = 0; k < failed.size(); ++k) {
+                const int s = failed[k];
+                iters[s] += rec[k].iterations;
+                projv[s] += rec[k].basis_vectors;
+                cycles[s] += rec[k].refinements;
+                status[s] = rec[k].status;
+                resid[s] = rec[k].residual;
+                fallback[s] = 1;
+            }
+            p->fallbacks_last = (int)failed.size();
+        }
+    }
     if (psi_out)
         MSC_CUDA(cudaMemcpyAsync(psi_out, p->X.p, vs * sizeof(double2), cudaMemcpyDeviceToDevice, ps));
     if (intensities_out) {
@@ -1695,26 +2043,21 @@ msc_status msc_solve(msc_plan *p, double *psi_out, double *intensities_out, msc_
             intensities_out);
         MSC_CUDA(cudaGetLastError());
     }
-    std::vector<int> iters(p->B), cycles(p->B), status(p->B), unfinished(p->B);
-    std::vector<double> resid(p->B);
-    MSC_CUDA(cudaMemcpyAsync(iters.data(), p->iters.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
-    MSC_CUDA(cudaMemcpyAsync(cycles.data(), p->cycles.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
-    MSC_CUDA(cudaMemcpyAsync(status.data(), p->status.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
-    MSC_CUDA(cudaMemcpyAsync(unfinished.data(), p->unfinished.p, p->B * sizeof(int), cudaMemcpyDeviceToHost, ps));
-    MSC_CUDA(cudaMemcpyAsync(resid.data(), p->resid.p, p->B * sizeof(double), cudaMemcpyDeviceToHost, ps));
     MSC_CUDA(cudaEventRecord(ev, ps));
     MSC_CUDA(cudaStreamWaitEvent(user, ev, 0));
     MSC_CUDA(cudaStreamSynchronize(ps));
     cudaEventDestroy(ev);
     msc_status worst = MSC_OK;
     for (int s = 0; s < p->B; ++s) {
-        int sst = unfinished[s] ? MSC_ERR_NOT_CONVERGED : status[s];
+        const int sst = status[s];
         if (results) {
             results[s].iterations = iters[s];
             results[s].refinements = cycles[s];
             results[s].status = sst;
-            results[s].reserved = 0;
+            results[s].fp64_fallback = fallback[s];
             results[s].residual = resid[s];
+            results[s].basis_vectors = projv[s];
+            results[s].reserved = 0;
         }
         if (sst != MSC_OK && worst == MSC_OK) worst = (msc_status)sst;
     }
@@ -1730,7 +2073,7 @@ msc_status msc_plan_get_info(const msc_plan *p, msc_plan_info *info)
     info->n_tiles = p->ntiles;
     info->launches_last = p->launches_last;
     info->cycles_last = p->cycles_last;
-    info->reserved = 0;
+    info->fallbacks_last = p->fallbacks_last;
     return MSC_OK;
 }
 
@@ -1803,6 +2146,40 @@ msc_status msc_debug_apply_operator(msc_plan *p, const double *x, double *y, voi
     return MSC_OK;
 }
 
+msc_status msc_apply_lower_block(msc_plan *p, const double *x, double *y, void *stream)
+{
+    if (!p || !x || !y) return fail(MSC_ERR_ARG, "null argument");
+    if (x == y) return fail(MSC_ERR_ARG, "x and y must be different buffers");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    st = ensure_gs_levels(p);
+    if (st != MSC_OK) return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    // y = -(-D x - V^lower x)
+    launch_residual_diag(p, nullptr, reinterpret_cast<const double2 *>(x), p->TMP.p, 0, s);
+    launch_coupling_masked_t<double>(p, nullptr, reinterpret_cast<const double2 *>(x), p->TMP.p,
+                                     -1.0, 1, reinterpret_cast<double2 *>(y), s);
+    const size_t cnt = (size_t)p->R * p->n;
+    msc::k_scale<<<(unsigned)std::min<size_t>((cnt + 255) / 256, 4096), 256, 0, s>>>(
+        reinterpret_cast<double2 *>(y), cnt, -1.0);
+    MSC_CUDA(cudaGetLastError());
+    return MSC_OK;
+}
+
+msc_status msc_solve_lower_block(msc_plan *p, const double *x, double *y, void *stream)
+{
+    if (!p || !x || !y) return fail(MSC_ERR_ARG, "null argument");
+    if (x == y) return fail(MSC_ERR_ARG, "x and y must be different buffers");
+    msc_status st = finalize(p);
+    if (st != MSC_OK) return st;
+    st = ensure_gs_levels(p);
+    if (st != MSC_OK) return st;
+    launch_gs_sweep_t<double>(p, nullptr, reinterpret_cast<const double2 *>(x),
+                              reinterpret_cast<double2 *>(y), reinterpret_cast<cudaStream_t>(stream));
+    MSC_CUDA(cudaGetLastError());
+    return MSC_OK;
+}
+
 const char *msc_plan_tuning_report(msc_plan *p)
 {
     if (!p) return "";
@@ -1841,6 +2218,15 @@ msc_status msc_debug_apply_block_inverse_f32(msc_plan *p, const float *x, float 
 }
 
 int msc_plan_uses_tensor_cores(const msc_plan *p) { return (p && p->use_tc) ? p->tc_n : 0; }
+
+msc_status msc_debug_symmetric_eigh(int32_t n, const double *a, double *w, double *v)
+{
+    if (!a || !w || !v) return fail(MSC_ERR_ARG, "null argument");
+    if (n < 2 || n > msc::kMaxNz) return fail(MSC_ERR_DIMS, "n must be in 2..1024");
+    for (size_t i = 0; i < (size_t)n * n; ++i)
+        if (!std::isfinite(a[i])) return fail(MSC_ERR_NONFINITE, "non-finite matrix entry");
+    return device_symmetric_eigh(n, a, w, v);
+}
 
 // ---------------------------------------------------------------------------
 // Adjoint solves and the potential gradient (no counterpart in the reference;
@@ -2065,7 +2451,10 @@ k_noalloc_scan_taps(int nkx, int nky, int n, const double2 *__restrict__ V, int 
     __shared__ int warp_off[32];
     __shared__ int base;
     for (int z = threadIdx.x; z < n; z += blockDim.x) v00[z] = V[z].x;
-    if (threadIdx.x == 0) base = 0;
+    if (threadIdx.x == 0) {
+        base = 0;
+        count[1] = 0;   // non-finite flag, raised by k_noalloc_check_finite
+    }
     __syncthreads();
     const int total = nkx * nky;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -2127,6 +2516,22 @@ __global__ void k_noalloc_tables(int nkx, int nky, int n, int K, const double2 *
     }
 }
 
+// Raise *flag if any input of the operator is NaN or infinite (the plan
+// builder rejects such inputs with MSC_ERR_NONFINITE; so does this path).
+__global__ void k_noalloc_check_finite(int C, int n, const double2 *__restrict__ V,
+                                       const double *__restrict__ T, const double *__restrict__ pkd,
+                                       const double2 *__restrict__ wc, int *flag)
+{
+    const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    bool bad = false;
+    for (size_t i = tid; i < (size_t)C * n; i += stride) bad |= !isfinite(V[i].x) || !isfinite(V[i].y);
+    for (size_t i = tid; i < (size_t)n * n; i += stride) bad |= !isfinite(T[i]);
+    for (size_t i = tid; i < (size_t)C; i += stride)
+        bad |= !isfinite(pkd[i]) || !isfinite(wc[i].x) || !isfinite(wc[i].y);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Device address of the scratch array on the current device (set-up on the
@@ -2162,14 +2567,15 @@ extern "C" msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32
         return fail(MSC_ERR_ARG, "null argument");
     if (nkx <= 0 || nky <= 0 || n_z < 2 || n_z > msc::kMaxNz)
         return fail(MSC_ERR_DIMS, "bad dimensions");
+    // channel count in 64 bits before any other arithmetic uses it
+    if ((int64_t)nkx * nky - 1 > msc::kMaxTaps) return fail(MSC_ERR_DIMS, "more than 2049 channels");
     const int C = nkx * nky;
-    if (C - 1 > msc::kMaxTaps) return fail(MSC_ERR_DIMS, "more than 2049 channels");
     const int n = n_z;
     const int kmax = std::max(C - 1, 1);
     const int ntiles = (C + msc::kTileRows - 1) / msc::kTileRows;
     // scratch layout (256-byte aligned pieces)
     size_t off = 0;
-    const size_t o_count = off;  off += round256(sizeof(int));
+    const size_t o_count = off;  off += round256(2 * sizeof(int));   // tap count, non-finite flag
     const size_t o_taps = off;   off += round256(sizeof(int2) * (size_t)kmax);
     const size_t o_v00 = off;    off += round256(sizeof(double) * (size_t)n);
     const size_t o_vt = off;     off += round256(sizeof(double2) * (size_t)kmax * n);
@@ -2199,9 +2605,14 @@ extern "C" msc_status msc_apply_operator_noalloc(int32_t nkx, int32_t nky, int32
 
     k_noalloc_scan_taps<<<1, 1024, 0, s>>>(nkx, nky, n, V, count, taps, v00);
     MSC_CUDA(cudaGetLastError());
-    int K = 0;
-    MSC_CUDA(cudaMemcpyAsync(&K, count, sizeof(int), cudaMemcpyDeviceToHost, s));
+    k_noalloc_check_finite<<<128, 256, 0, s>>>(C, n, V, kinetic, pkd,
+                                               reinterpret_cast<const double2 *>(wave_c), count + 1);
+    MSC_CUDA(cudaGetLastError());
+    int kf[2] = {0, 0};
+    MSC_CUDA(cudaMemcpyAsync(kf, count, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     MSC_CUDA(cudaStreamSynchronize(s));
+    const int K = kf[0];
+    if (kf[1]) return fail(MSC_ERR_NONFINITE, "non-finite potential, kinetic or channel data");
     if (K < 0 || K > kmax) return fail(MSC_ERR_CUDA, "tap scan returned an invalid count");
     k_noalloc_tables<<<256, 256, 0, s>>>(nkx, nky, n, K, V, taps, Vt, nbr, t0, tn, ts, ntiles);
     MSC_CUDA(cudaGetLastError());

@@ -110,6 +110,8 @@ class SolveResult:
     cycles: np.ndarray
     status: np.ndarray
     residual: np.ndarray
+    fp64_fallback: np.ndarray | None = None   # mixed: systems re-solved in FP64
+    basis_vectors: np.ndarray | None = None   # sum over Arnoldi steps of j + 1
 
     def system_intensities(self, s: int) -> torch.Tensor:
         return self.intensities[self.row_offsets[s]:self.row_offsets[s + 1]]
@@ -125,7 +127,9 @@ class ScatteringPlan:
                  rtol: float = 1e-10, restart: int = 30, max_iterations: int = 2000,
                  precision: str = "fp64", inner_rtol: float = 0.0, inner_restart: int = 0,
                  max_refinements: int = 0, tensor_cores: bool | None = None,
-                 inner_gram_schmidt_passes: int = 2, preconditioner_order: int = 0):
+                 inner_gram_schmidt_passes: int = 2, preconditioner_order: int = 0,
+                 fp64_recovery: bool = True, gram_schmidt: str = "dcgs2",
+                 gauss_seidel: bool = False):
         self._lib = nat.load()
         v = np.ascontiguousarray(np.asarray(potential_values), dtype=np.complex128)
         nkx, nky, nz = v.shape
@@ -151,6 +155,20 @@ class ScatteringPlan:
             raise ValueError("inner_gram_schmidt_passes must be 1 or 2")
         if inner_gram_schmidt_passes == 1:
             desc.flags |= 4
+        # mixed form: re-solve in FP64 the systems the refinement leaves unconverged
+        if not fp64_recovery:
+            desc.flags |= 8
+        # Arnoldi orthogonalisation: "dcgs2" (delayed re-orthogonalisation, two
+        # passes over the basis per step) or "cgs2" (two full CGS passes, three)
+        if gram_schmidt not in ("dcgs2", "cgs2"):
+            raise ValueError("gram_schmidt must be 'dcgs2' or 'cgs2'")
+        if gram_schmidt == "cgs2":
+            desc.flags |= 16
+        # the reference's block Gauss-Seidel preconditioner M = L^-1 (with
+        # preconditioner_order = 1: its Neumann flag on top) instead of the
+        # block-diagonal D^-1 series
+        if gauss_seidel:
+            desc.flags |= 32
         # von Neumann order k: M = sum_{i<=k} (-D^-1 V)^i D^-1 (0 = block-diagonal D^-1)
         desc.precond_order = int(preconditioner_order)
         self._plan = ctypes.c_void_p()
@@ -212,7 +230,9 @@ class ScatteringPlan:
             iterations=np.array([r.iterations for r in res]),
             cycles=np.array([r.refinements for r in res]),
             status=np.array([r.status for r in res]),
-            residual=np.array([r.residual for r in res]))
+            residual=np.array([r.residual for r in res]),
+            fp64_fallback=np.array([r.fp64_fallback for r in res]),
+            basis_vectors=np.array([r.basis_vectors for r in res]))
 
     # ---- adjoint differentiation -------------------------------------------------
     def set_adjoint(self, on: bool) -> None:
@@ -319,6 +339,14 @@ class ScatteringPlan:
 
     def apply_operator(self, x: torch.Tensor) -> torch.Tensor:
         return self._debug("msc_debug_apply_operator", x)
+
+    def apply_lower_block(self, x: torch.Tensor) -> torch.Tensor:
+        """L x, L = D + V^lower of the block Gauss-Seidel splitting in plan row order."""
+        return self._debug("msc_apply_lower_block", x)
+
+    def solve_lower_block(self, x: torch.Tensor) -> torch.Tensor:
+        """L^-1 x (the reference's forward sweep, solve_lower_block)."""
+        return self._debug("msc_solve_lower_block", x)
 
     def apply_block_inverse_f32(self, x: torch.Tensor) -> torch.Tensor:
         """D^-1 x with the mixed form's FP32 kernel (x: complex64 [R, nz])."""

@@ -1,6 +1,10 @@
 """Generate the golden fixtures in this folder (run here, where the reference is mounted).
 
-    python tests/golden/make_golden.py [--cfg1]
+    python tests/golden/make_golden.py [--reference PATH] [--cfg1] [--cfg3] [--cfg2-batch]
+
+``--reference PATH`` (or the environment variable MULTISCAT_REFERENCE) names
+the checkout of the reference project whose golden files are copied; without
+it the two ``wolken_*`` files are left as they are.
 
 Writes
 - ``wolken_expected_intensities.txt``: copy of the reference's golden file
@@ -13,6 +17,15 @@ Writes
   intensities for the 11x11-channel square Morse case at precision 1e-12.
 - ``oracle_subsets.json``: oracle intensities for channel subsets (the
   ``n_channels`` truncation) of two seeded beams over the same potential.
+- ``oracle_cfg2_stall.json``: oracle intensities of beam 1 of
+  ``cfg2_batch(n_solves=3, seed=1, nz=41)``, a beam on which the
+  block-diagonal FP32 inner solve stalls near a residual of 1e-5.
+- ``oracle_cfg2_batch.npz`` (with --cfg2-batch, about a minute on 8 cores):
+  the oracle on every beam of the benchmarked batch ``cfg2_batch(512,
+  seed=0)`` at eps 0.5e-12; the intensities of 64 of them are kept: the 8
+  largest-theta, the 8 lowest-energy and the 8 most-iterations beams plus 40
+  more drawn with ``default_rng(2024)`` from the rest; the iteration counts
+  of all 512 are kept too.
 - ``oracle_cfg1.json`` (with --cfg1, minutes of CPU): oracle intensities of
   the 41x41-channel hexagonal case at precision 1e-10.
 - ``oracle_cfg3_fd.json`` (with --cfg3, minutes of CPU on all cores): central
@@ -41,13 +54,20 @@ sys.path.insert(0, str(ROOT))
 from oracle import inputs, solver  # noqa: E402
 from tests.cases import cfg0_case, cfg1_case, subset_case  # noqa: E402
 
-REF = pathlib.Path("/root/reference")
+
+def reference_root() -> pathlib.Path | None:
+    """The reference checkout named by --reference PATH or MULTISCAT_REFERENCE."""
+    import os
+    if "--reference" in sys.argv:
+        return pathlib.Path(sys.argv[sys.argv.index("--reference") + 1])
+    env = os.environ.get("MULTISCAT_REFERENCE")
+    return pathlib.Path(env) if env else None
 
 
-def wolken_files() -> None:
-    src = REF / "tests" / "data" / "expected_intensities.txt"
+def wolken_files(ref: pathlib.Path) -> None:
+    src = ref / "tests" / "data" / "expected_intensities.txt"
     shutil.copyfile(src, HERE / "wolken_expected_intensities.txt")
-    fixture = np.load(REF / "tests" / "data" / "expected_potential.npy").reshape(10, 10, 550)
+    fixture = np.load(ref / "tests" / "data" / "expected_potential.npy").reshape(10, 10, 550)
     nodes, _ = inputs.lobatto_rule(0.0, 8.0, 550)
     model = inputs.wolken_potential(nodes, 10, 10)
     rel = float(np.abs(model - fixture).max() / np.abs(fixture).max())
@@ -199,10 +219,78 @@ def oracle_cfg3_fd() -> None:
     print("cfg3 fd", json.dumps(out))
 
 
+# ---------------------------------------------------------------------------
+# cfg2: the benchmarked 512-beam batch itself, and the beam that stalls the
+# FP32 inner solve
+# ---------------------------------------------------------------------------
+CFG2_EPS = 0.5e-12
+
+
+def _subset_oracle(case, sp):
+    psi, info, iters, _ = solver.solve_channels(
+        case.v, sp.channel_ix, sp.channel_iy, sp.pkd, sp.wave_c, sp.specular,
+        sp.wave_b[sp.specular], case.t, eps=CFG2_EPS)
+    s = 2.0j * sp.wave_b * psi[:, -1]
+    s[sp.specular] += sp.wave_a[sp.specular]
+    return np.abs(s) ** 2, int(info), int(iters)
+
+
+def _cfg2_beam_job(b):
+    sys.path.insert(0, str(ROOT))
+    from multiscat_b200.workloads import cfg2_batch
+    case, systems = cfg2_batch(512, seed=0)
+    inten, info, iters = _subset_oracle(case, systems[b])
+    return b, inten, info, iters
+
+
+def oracle_cfg2_batch() -> None:
+    import multiprocessing as mp
+    from multiscat_b200.workloads import cfg2_batch
+    t0 = time.time()
+    case, systems = cfg2_batch(512, seed=0)
+    with mp.get_context("spawn").Pool(8) as pool:
+        res = sorted(pool.map(_cfg2_beam_job, range(512), chunksize=4), key=lambda r: r[0])
+    iters = np.array([r[3] for r in res], np.int32)
+    info = np.array([r[2] for r in res], np.int32)
+    theta, energy = case.extra["theta"], case.extra["energy"]
+    picks: list[int] = []
+    for order in (np.argsort(-theta, kind="stable"), np.argsort(energy, kind="stable"),
+                  np.argsort(-iters, kind="stable")):
+        picks += [int(b) for b in order if int(b) not in picks][:8]
+    rest = np.array([b for b in range(512) if b not in picks])
+    picks += sorted(np.random.default_rng(2024).choice(rest, 64 - len(picks), replace=False).tolist())
+    picks = np.array(picks, np.int32)
+    counts = np.array([len(res[b][1]) for b in picks], np.int64)
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    inten = np.concatenate([res[b][1] for b in picks])
+    np.savez_compressed(HERE / "oracle_cfg2_batch.npz", beams=picks, offsets=offsets,
+                        intensities=inten, iterations_all=iters, info_all=info,
+                        eps=np.float64(CFG2_EPS))
+    print("cfg2 batch: all converged", bool((info == 0).all()), "iterations", int(iters.min()),
+          "-", int(iters.max()), "flux-1 max", max(abs(res[b][1].sum() - 1) for b in picks),
+          "s", time.time() - t0)
+
+
+def oracle_cfg2_stall() -> None:
+    from multiscat_b200.workloads import cfg2_batch
+    case, systems = cfg2_batch(n_solves=3, seed=1, nz=41)
+    inten, info, iters = _subset_oracle(case, systems[1])
+    out = {"case": "beam 1 of cfg2_batch(n_solves=3, seed=1, nz=41)", "oracle_eps": CFG2_EPS,
+           "info": info, "iterations": iters, "n_channels": int(len(inten)),
+           "intensities": inten.tolist(), "flux": float(inten.sum())}
+    (HERE / "oracle_cfg2_stall.json").write_text(json.dumps(out))
+    print("cfg2 stall beam: info", info, "iters", iters, "flux-1", inten.sum() - 1)
+
+
 if __name__ == "__main__":
-    wolken_files()
+    ref = reference_root()
+    if ref is not None:
+        wolken_files(ref)
     oracle_case(cfg0_case(), 12, "oracle_cfg0.json")
     oracle_subsets()
+    oracle_cfg2_stall()
+    if "--cfg2-batch" in sys.argv:
+        oracle_cfg2_batch()
     if "--cfg1" in sys.argv:
         oracle_case(cfg1_case(), 10, "oracle_cfg1.json")
     if "--cfg3" in sys.argv:

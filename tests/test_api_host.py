@@ -28,7 +28,7 @@ def test_scattering_matrix_from_state_is_the_boundary_formula():
         potential_values=inputs.wolken_potential(nodes, nkx, nky) * sa.MEV, metadata=md)
     rng = np.random.default_rng(11)
     state = rng.normal(size=(nkx, nky, nz)) + 1j * rng.normal(size=(nkx, nky, nz))
-    got = get_scattering_matrix_from_state(state, cond)
+    got = get_scattering_matrix_from_state(state, cond, convention="psi")
     assert got.dtype == np.complex128 and got.shape == (nkx, nky)
     arr = natural_arrays(cond)
     wa, wb, _ = inputs.waves(arr.pkd.ravel(), arr.weights, 0.0, 8.0)
@@ -203,3 +203,66 @@ def test_beam_systems_match_per_beam_builders(mode):
         assert sp.specular == want.specular
     with pytest.raises(ValueError):
         beam_systems(pkd, lambda e: sa.waves(e, w, -1.5, 11.5), max_pkd=-1e9)
+
+
+def test_reference_order_system_is_the_reference_channel_list():
+    """The state convention's channel list: numpy's default argsort of pkd, the
+    first n_channels of it (_scipy.py:414-416), specular located in it."""
+    from multiscat_b200.api import _reference_order_system
+    from multiscat_b200.workloads import cfg0_case
+    case = cfg0_case(nz=20)
+
+    class Arr:
+        pkd, wave_a, wave_b, wave_c = case.pkd, case.wa, case.wb, case.wc
+    for n_channels in (None, 40):
+        sp = _reference_order_system(Arr, n_channels)
+        order = np.argsort(case.pkd.ravel())
+        if n_channels:
+            order = order[:n_channels]
+        assert np.array_equal(sp.channel_ix * 11 + sp.channel_iy, order)
+        assert np.array_equal(sp.pkd, case.pkd.ravel()[order])
+        assert sp.channel_ix[sp.specular] == 0 and sp.channel_iy[sp.specular] == 0
+        assert np.array_equal(sp.wave_c, np.asarray(case.wc).ravel()[order])
+    with pytest.raises(ValueError):
+        from multiscat_b200.api import _check_convention
+        _check_convention("lpsi")
+
+
+def test_bench_kernel_records_classify_each_kernel_by_its_bound():
+    """bench.py's roofline arithmetic on a synthetic result: the coupling and
+    the SIMT block inverse are FMA-bound, the tcgen05 block inverse tensor-bound,
+    the Arnoldi passes HBM-bound with one pass per Krylov vector row touched."""
+    import importlib.util
+    import pathlib
+    spec = importlib.util.spec_from_file_location(
+        "bench", pathlib.Path(__file__).resolve().parents[1] / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+
+    class Res:
+        row_offsets = np.array([0, 100, 300])
+        iterations = np.array([10, 20])
+        basis_vectors = np.array([55, 150])
+        cycles = np.array([2, 3])
+    kt = {k: {"ms": 1.0, "launches": 10} for k in
+          ("block_inverse", "coupling", "arnoldi_project", "arnoldi_update_project")}
+    peaks = {"hbm_gbs": 6000.0, "bf16_tflops": 1600.0, "bf16_tflops_sustained": 1400.0}
+    fma = {"fp32": 70.0, "fp64": 35.0}
+    n, taps = 150, 80
+    rec = bench.kernel_records(kt, Res, n, taps, True, True, True, peaks, fma, "cfg2")
+    steps_rows = 100 * 10 + 200 * 20
+    vec_rows = 100 * 55 + 200 * 150
+    assert rec["coupling"]["bound"] == "fma" and rec["coupling"]["peak"] == 70.0
+    assert rec["coupling"]["achieved"] == pytest.approx(8 * taps * n * steps_rows / 1e-3 / 1e12)
+    bi = rec["block_inverse"]
+    assert bi["bound"] == "tensor" and bi["peak"] == 1400.0
+    assert bi["achieved"] == pytest.approx(24 * n * n * (steps_rows + 100 * 2 + 200 * 3) / 1e-3 / 1e12)
+    red = rec["arnoldi_project"]
+    assert red["bound"] == "hbm"
+    assert red["achieved"] == pytest.approx((vec_rows + steps_rows) * n * 8 / 1e-3 / 1e9)
+    upd = rec["arnoldi_update_project"]
+    assert upd["achieved"] == pytest.approx((vec_rows + 3 * steps_rows) * n * 8 / 1e-3 / 1e9)
+    for r in rec.values():
+        assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
+    simt = bench.kernel_records(kt, Res, n, taps, False, False, False, peaks, fma, "cfg2")
+    assert simt["block_inverse"]["bound"] == "fma" and simt["block_inverse"]["peak"] == 35.0

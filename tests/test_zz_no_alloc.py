@@ -17,9 +17,9 @@ import numpy as np
 import pytest
 import torch
 
-from multiscat_b200 import ScatteringPlan
+from multiscat_b200 import ScatteringPlan, full_grid_system
 from multiscat_b200 import _native as nat
-from multiscat_b200.workloads import cfg0_case
+from multiscat_b200.workloads import Case, cfg0_case
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +30,7 @@ def _call_noalloc(lib, case, x, y, stream):
     v = torch.as_tensor(np.ascontiguousarray(case.v), device=dev)
     t = torch.as_tensor(np.ascontiguousarray(case.t), device=dev)
     pkd = torch.as_tensor(np.ascontiguousarray(case.pkd.ravel()), device=dev)
-    wc = torch.as_tensor(np.ascontiguousarray(case.wc), device=dev)
+    wc = torch.as_tensor(np.ascontiguousarray(np.asarray(case.wc).ravel()), device=dev)
     st = lib.msc_apply_operator_noalloc(nkx, nky, nz, ctypes.c_void_p(v.data_ptr()),
                                         ctypes.c_void_p(t.data_ptr()),
                                         ctypes.c_void_p(pkd.data_ptr()),
@@ -72,3 +72,49 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                         ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(0))
     assert st == nat.MSC_ERR_DIMS
     assert "scratch" in nat.last_error()
+
+
+def _asymmetric_case(nkx=5, nky=7, nz=12, seed=5):
+    """A random complex potential on a 5 x 7 torus: no x <-> y or d <-> -d
+    symmetry, so a swapped axis or a tap applied with the wrong sign in the
+    neighbour table would change y."""
+    rng = np.random.default_rng(seed)
+    v = 0.3 * (rng.standard_normal((nkx, nky, nz)) + 1j * rng.standard_normal((nkx, nky, nz)))
+    a = rng.standard_normal((nz, nz))
+    t = a @ a.T + nz * np.eye(nz)
+    pkd = rng.uniform(-2.0, 5.0, (nkx, nky))
+    c = nkx * nky
+    wa, wb, wc = (rng.standard_normal(c) + 1j * rng.standard_normal(c) for _ in range(3))
+    return Case("asymmetric 5x7", v, t, pkd, wa, wb, wc, np.arange(nz, dtype=float),
+                np.ones(nz))
+
+
+def test_noalloc_operator_matches_plan_on_an_asymmetric_torus():
+    lib = nat.load()
+    case = _asymmetric_case()
+    rng = np.random.default_rng(22)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    plan = ScatteringPlan(case.v, case.t, [full_grid_system(case.pkd, case.wa, case.wb, case.wc)])
+    for call in range(2):
+        x_np = rng.standard_normal((35, 12)) + 1j * rng.standard_normal((35, 12))
+        x = torch.as_tensor(x_np, device=dev)
+        want = plan.apply_operator(x).cpu().numpy()
+        y = torch.full_like(x, complex(float("nan"), float("nan")))
+        st = _call_noalloc(lib, case, x, y, stream)
+        assert st == nat.MSC_OK, nat.last_error()
+        np.testing.assert_allclose(y.cpu().numpy(), want, rtol=1e-11,
+                                   atol=1e-11 * np.abs(want).max(), err_msg=f"call {call}")
+    plan.close()
+
+
+def test_noalloc_rejects_a_nonfinite_potential():
+    lib = nat.load()
+    case = _asymmetric_case()
+    case.v[2, 3, 4] = complex(float("nan"), 0.0)
+    dev = torch.device("cuda", 0)
+    x = torch.zeros((35, 12), dtype=torch.complex128, device=dev)
+    y = torch.zeros_like(x)
+    st = _call_noalloc(lib, case, x, y, torch.cuda.current_stream(dev).cuda_stream)
+    assert st == nat.MSC_ERR_NONFINITE
+    assert "non-finite" in nat.last_error()
