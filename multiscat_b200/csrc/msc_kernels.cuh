@@ -626,6 +626,179 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
 }
 
 // ---------------------------------------------------------------------------
+// Channel coupling of a separable potential: when every z's tap window
+// factorises as V_(sdx, sdy)(z) = p_sdx(z) q_sdy(z) off the centre (the
+// corrugated Morse potential of a square lattice, xi = (h/2)(cos X + cos Y),
+// gives exactly that: the FFT of e^{2 alpha xi} is a product of two 1-D
+// transforms), the 2-D convolution is a pass along x and a pass along y:
+//   t(x, y')  = sum_sdx p_sdx src(x - sdx, y')            (y' over the halo)
+//   out(x, y) = in0 + sgn [sum_sdy q_sdy t(x, y - sdy) - kappa src(x, y)]
+// with kappa = p_0 q_0 the product's value at the centre, which is no tap.
+// (2 HX + 1) (8 + 2 HY) + 8 (2 HY + 2) complex MACs per thread for 8
+// outputs instead of 8 K: 28 instead of 80 per output for |m|,|n| <= 4, 43
+// instead of 288 for |m|,|n| <= 8.  A thread owns one (x, z) column of the
+// 8 x 8 patch: pass 1 keeps the column's 8 + 2 HY values of t in registers,
+// pass 2 reads nothing but its own registers and the q row.  The halo of the
+// patch is staged as in k_coupling_halo.
+// ---------------------------------------------------------------------------
+struct SepTaps {
+    const void *p;       // [2 HX + 1][n] complex (R), p_sdx at sdx + HX
+    const void *q;       // [2 HY + 1][n] complex (R), q_sdy at sdy + HY
+    const void *kappa;   // [n] complex (R)
+};
+
+template <int HY, int BX, int ZC, typename R>
+__global__ void __launch_bounds__(BX * ZC)
+k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps sep,
+               const typename CT<R>::t *__restrict__ src, const typename CT<R>::t *__restrict__ in0,
+               R sgn, typename CT<R>::t *__restrict__ out)
+{
+    using C2 = typename CT<R>::t;
+    constexpr int BY = 8;
+    constexpr int HYW = BY + 2 * HY;
+    constexpr int WY = 2 * HY + 1;
+    constexpr int NT = BX * ZC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int HX = ct.hx;
+    const int HXW = BX + 2 * HX;
+    const int WX = 2 * HX + 1;
+    C2 *halo = reinterpret_cast<C2 *>(smem_raw);                       // [HXW][HYW][ZC]
+    C2 *pw = halo + (size_t)HXW * HYW * ZC;                            // [WX][ZC]
+    C2 *qw = pw + (size_t)WX * ZC;                                     // [WY][ZC]
+    C2 *kw = qw + (size_t)WY * ZC;                                     // [ZC]
+    int *rows = reinterpret_cast<int *>(kw + ZC);                      // [HXW][HYW]
+    __shared__ int colany[BX];
+
+    const int w = blockIdx.x;
+    const int s = ct.work[3 * w];
+    if (gate && gate[s] == 0) return;
+    const int x0 = ct.work[3 * w + 1], y0 = ct.work[3 * w + 2];
+    const int z0 = blockIdx.y * ZC;
+    const int nkx = ct.nkx, nky = ct.nky;
+    const int *pr = ct.pos_row + (size_t)s * nkx * nky;
+    const C2 *P = reinterpret_cast<const C2 *>(sep.p);
+    const C2 *Qv = reinterpret_cast<const C2 *>(sep.q);
+    const C2 *Kp = reinterpret_cast<const C2 *>(sep.kappa);
+    for (int i = threadIdx.x; i < (WX + WY + 1) * ZC; i += NT) {
+        const int row = i / ZC, z = z0 + (i % ZC);
+        C2 v = mk2<R>(0, 0);
+        if (z < n) v = row < WX ? P[(size_t)row * n + z]
+                     : row < WX + WY ? Qv[(size_t)(row - WX) * n + z] : Kp[z];
+        pw[i] = v;          // pw, qw and kw are consecutive
+    }
+    const int npos = HXW * HYW;
+    for (int pidx = threadIdx.x; pidx < npos; pidx += NT) {
+        const int hy = pidx % HYW, hx = pidx / HYW;
+        int gx = (x0 + hx - HX) % nkx;
+        if (gx < 0) gx += nkx;
+        int gy = (y0 + hy - HY) % nky;
+        if (gy < 0) gy += nky;
+        rows[pidx] = pr[gx * nky + gy];
+    }
+    if (threadIdx.x < BX) {
+        const int gx = x0 + threadIdx.x;
+        int any = 0;
+        if (gx < nkx)
+            for (int y = 0; y < BY && !any; ++y) any = (y0 + y < nky) && pr[gx * nky + y0 + y] >= 0;
+        colany[threadIdx.x] = any;
+    }
+    __syncthreads();
+    constexpr int kU = 8;
+    const int total = npos * ZC;
+    if (std::is_same<R, float>::value && (n % 2) == 0) {
+        const int total2 = total / 2;
+        float4 *halo4 = reinterpret_cast<float4 *>(halo);
+        for (int base = threadIdx.x; base < total2; base += NT * kU) {
+            float4 v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (idx < total2) {
+                    const int row = rows[(2 * idx) / ZC];
+                    const int z = z0 + ((2 * idx) % ZC);
+                    if (row >= 0 && z < n)
+                        v[u] = *reinterpret_cast<const float4 *>(src + (size_t)row * n + z);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                if (idx < total2) halo4[idx] = v[u];
+            }
+        }
+    } else {
+        for (int base = threadIdx.x; base < total; base += NT * kU) {
+            C2 v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                v[u] = mk2<R>(0, 0);
+                if (idx < total) {
+                    const int row = rows[idx / ZC];
+                    const int z = z0 + (idx % ZC);
+                    if (row >= 0 && z < n) v[u] = src[(size_t)row * n + z];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                if (idx < total) halo[idx] = v[u];
+            }
+        }
+    }
+    __syncthreads();
+
+    const int zl = threadIdx.x % ZC;
+    const int tx = threadIdx.x / ZC;
+    const int z = z0 + zl;
+    if (x0 + tx >= nkx || z >= n || !colany[tx]) return;
+    // pass 1: t(hy) = sum_sdx p_sdx halo(tx - sdx + HX, hy) over the halo column
+    R tr[HYW], ti[HYW];
+#pragma unroll
+    for (int i = 0; i < HYW; ++i) {
+        tr[i] = 0;
+        ti[i] = 0;
+    }
+    for (int sdx = -HX; sdx <= HX; ++sdx) {
+        const C2 pv = pw[(sdx + HX) * ZC + zl];
+        const C2 *colp = halo + (size_t)(tx - sdx + HX) * HYW * ZC + zl;
+#pragma unroll
+        for (int i = 0; i < HYW; ++i) {
+            const C2 v = colp[(size_t)i * ZC];
+            tr[i] = fma(pv.x, v.x, fma(-pv.y, v.y, tr[i]));
+            ti[i] = fma(pv.x, v.y, fma(pv.y, v.x, ti[i]));
+        }
+    }
+    // pass 2: out(y) = sum_sdy q_sdy t(y - sdy + HY) - kappa src(x, y)
+    C2 qv[WY];
+#pragma unroll
+    for (int i = 0; i < WY; ++i) qv[i] = qw[i * ZC + zl];
+    const C2 kap = kw[zl];
+    const C2 *own = halo + (size_t)(tx + HX) * HYW * ZC + zl;
+    const int gx = x0 + tx;
+#pragma unroll
+    for (int y = 0; y < BY; ++y) {
+        const int gy = y0 + y;
+        if (gy >= nky) continue;
+        const int row = pr[gx * nky + gy];
+        if (row < 0) continue;
+        const C2 c = own[(size_t)(y + HY) * ZC];
+        R ar = -(kap.x * c.x - kap.y * c.y), ai = -(kap.x * c.y + kap.y * c.x);
+#pragma unroll
+        for (int sdy = -HY; sdy <= HY; ++sdy) {
+            const C2 q = qv[sdy + HY];
+            const R xr = tr[y - sdy + HY], xi = ti[y - sdy + HY];
+            ar = fma(q.x, xr, fma(-q.y, xi, ar));
+            ai = fma(q.x, xi, fma(q.y, xr, ai));
+        }
+        const size_t o = (size_t)row * n + z;
+        const C2 base = in0 ? in0[o] : mk2<R>(0, 0);
+        out[o] = mk2<R>(base.x + sgn * ar, base.y + sgn * ai);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Arnoldi reductions.  partial[tile][i] = sum conj(Q_i) W over the tile for
 // i < nvec; slot nvec holds ||W||^2 when with_norm.  One warp per vector;
 // FP64 accumulation for both precisions.

@@ -208,6 +208,12 @@ struct msc_plan {
     bool use_halo = false;             // halo tables built (taps reach <= 8)
     int halo32 = 0, halo64 = 0;    // autotuned coupling kind per precision (0 nbr, 1/2 halo)
     int halo_hx = 0, halo_hy = 0, nwork = 0;
+    // separable coupling (coupling kind 3): p, q, kappa per z when every tap
+    // window factorises (see k_coupling_sep); host copies for the adjoint
+    bool sep_ok = false;
+    std::vector<double2> sep_p_h, sep_q_h, sep_k_h;   // [2hx+1][n], [2HY+1][n], [n]
+    DevBuf<double2> sep64;                           // p | q | kappa
+    DevBuf<float2> sep32;
     // autotuning record: microseconds per candidate
     std::vector<std::pair<std::string, float>> tune_log;
     std::string tune_report;
@@ -257,6 +263,7 @@ struct msc_plan {
         U32.release(); R64.release(); e_img.release(); tc_error.release();
         Hraw.release(); dsum.release(); dcoef.release(); gsave.release();
         gs_sys_lvl.release(); gs_lvl_start.release(); gs_lvl_rows.release();
+        sep64.release(); sep32.release();
     }
 
     msc::Tiles tiles() const
@@ -462,14 +469,52 @@ void launch_halo_ys(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> 
     }
 }
 
+size_t sep_smem(int hx, int hy, int zc, size_t elem)
+{
+    const size_t hxw = kHaloBX + 2 * hx, hyw = 8 + 2 * hy;
+    return (hxw * hyw + (2 * hx + 1) + (2 * hy + 1) + 1) * zc * elem + hxw * hyw * sizeof(int);
+}
+
+template <int HY, typename R>
+void launch_sep(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
+                C2<R> *out, cudaStream_t st)
+{
+    constexpr int ZC = halo_zc<R>();
+    msc::CouplingTiles ct{p->work.p, p->pos_map.p, p->tap_window.p, p->nwork, p->nkx, p->nky,
+                          p->halo_hx, p->K};
+    const size_t np = (size_t)(2 * p->halo_hx + 1) * p->n, nq = (size_t)(2 * p->halo_hy + 1) * p->n;
+    const C2<R> *base = std::is_same<R, float>::value
+                            ? reinterpret_cast<const C2<R> *>(p->sep32.p)
+                            : reinterpret_cast<const C2<R> *>(p->sep64.p);
+    const msc::SepTaps sep{base, base + np, base + np + nq};
+    dim3 grid(p->nwork, (p->n + ZC - 1) / ZC);
+    msc::k_coupling_sep<HY, kHaloBX, ZC, R>
+        <<<grid, kHaloBX * ZC, sep_smem(p->halo_hx, HY, ZC, sizeof(C2<R>)), st>>>(
+            ct, gate, p->n, sep, src, in0, sgn, out);
+}
+
+template <typename R>
+void launch_sep_hy(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
+                   C2<R> *out, cudaStream_t st)
+{
+    switch (p->halo_hy) {
+    case 1: launch_sep<1, R>(p, gate, src, in0, sgn, out, st); return;
+    case 2: launch_sep<2, R>(p, gate, src, in0, sgn, out, st); return;
+    case 4: launch_sep<4, R>(p, gate, src, in0, sgn, out, st); return;
+    default: launch_sep<8, R>(p, gate, src, in0, sgn, out, st); return;
+    }
+}
+
 template <typename R>
 void launch_coupling_t(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
                        C2<R> *out, cudaStream_t st)
 {
-    // coupling kind per precision: 0 neighbour table, 1 halo (8 y/thread), 2 halo (4 y/thread)
+    // coupling kind per precision: 0 neighbour table, 1 halo (8 y/thread), 2 halo (4 y/thread),
+    // 3 separable (two 1-D passes; only when the tap windows factorise)
     const int kind = p->use_halo ? (std::is_same<R, float>::value ? p->halo32 : p->halo64) : 0;
     if (kind == 1) { launch_halo_ys<8, R>(p, gate, src, in0, sgn, out, st); return; }
     if (kind == 2) { launch_halo_ys<4, R>(p, gate, src, in0, sgn, out, st); return; }
+    if (kind == 3 && p->sep_ok) { launch_sep_hy<R>(p, gate, src, in0, sgn, out, st); return; }
     dim3 grid(p->ntiles, (p->n + 31) / 32);
     dim3 block(32, msc::kTileRows);
     msc::k_coupling<R><<<grid, block, smem_coupling(std::max(p->K, 1)), st>>>(
@@ -824,6 +869,19 @@ msc_status set_kernel_attributes(int n, int K)
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_halo<HY, kHaloBX, halo_zc<R>(), 4, R>,        \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
                                   (int)std::min<size_t>(halo_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448)));;
+#define MSC_SEP_ATTR(HY, R)                                                                      \
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>(), R>,              \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                  (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448)));
+    MSC_SEP_ATTR(1, float)
+    MSC_SEP_ATTR(2, float)
+    MSC_SEP_ATTR(4, float)
+    MSC_SEP_ATTR(8, float)
+    MSC_SEP_ATTR(1, double)
+    MSC_SEP_ATTR(2, double)
+    MSC_SEP_ATTR(4, double)
+    MSC_SEP_ATTR(8, double)
+#undef MSC_SEP_ATTR
     MSC_HALO_ATTR(1, float)
     MSC_HALO_ATTR(2, float)
     MSC_HALO_ATTR(4, float)
@@ -1021,11 +1079,12 @@ float time_launch(msc_plan *p, F f)
 // precision the solve uses.  Mixed form: tcgen05 tile width N (and the SIMT
 // FP32 kernel).  Runs once per plan, before the solve graphs are captured.
 struct TuneKey {
-    int n, R, K, nkx, nky, B, mixed, hx, hy, tcmax, flags;
+    int n, R, K, nkx, nky, B, mixed, hx, hy, tcmax, flags, sep;
     bool operator<(const TuneKey &o) const
     {
-        return std::tie(n, R, K, nkx, nky, B, mixed, hx, hy, tcmax, flags) <
-               std::tie(o.n, o.R, o.K, o.nkx, o.nky, o.B, o.mixed, o.hx, o.hy, o.tcmax, o.flags);
+        return std::tie(n, R, K, nkx, nky, B, mixed, hx, hy, tcmax, flags, sep) <
+               std::tie(o.n, o.R, o.K, o.nkx, o.nky, o.B, o.mixed, o.hx, o.hy, o.tcmax, o.flags,
+                        o.sep);
     }
 };
 struct TuneChoice {
@@ -1062,8 +1121,9 @@ bool tune_from_env(msc_plan *p)
     if (!env || !*env) return false;
     int c64 = p->halo64, c32 = p->halo32, bi = p->use_tc ? p->tc_n : 0, bg = 1;
     std::sscanf(env, "c64=%d,c32=%d,bi=%d,bg=%d", &c64, &c32, &bi, &bg);
-    p->halo64 = p->use_halo ? std::max(0, std::min(2, c64)) : 0;
-    p->halo32 = p->use_halo ? std::max(0, std::min(2, c32)) : 0;
+    const int kmax = p->sep_ok ? 3 : 2;
+    p->halo64 = p->use_halo ? std::max(0, std::min(kmax, c64)) : 0;
+    p->halo32 = p->use_halo ? std::max(0, std::min(kmax, c32)) : 0;
     if (p->use_tc) {
         if (bi == 0) {
             p->use_tc = false;
@@ -1081,7 +1141,7 @@ msc_status autotune(msc_plan *p)
 {
     if (tune_from_env(p)) return MSC_OK;
     const TuneKey key{p->n, p->R, p->K, p->nkx, p->nky, p->B, p->mixed ? 1 : 0, p->halo_hx,
-                      p->halo_hy, p->use_tc ? p->tc_n : 0, p->desc.flags};
+                      p->halo_hy, p->use_tc ? p->tc_n : 0, p->desc.flags, p->sep_ok ? 1 : 0};
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(key);
@@ -1108,11 +1168,12 @@ msc_status autotune_measure(msc_plan *p)
     const size_t vs = (size_t)p->R * p->n;
     MSC_CUDA(cudaMemsetAsync(p->X.p, 0, vs * sizeof(double2), p->stream));
     MSC_CUDA(cudaMemsetAsync(p->TMP.p, 0, vs * sizeof(double2), p->stream));
-    const char *kind_name[3] = {"neighbour", "halo_y8", "halo_y4"};
+    const char *kind_name[4] = {"neighbour", "halo_y8", "halo_y4", "separable"};
+    const int nkinds = p->sep_ok ? 4 : 3;
     if (p->use_halo) {
         float best = 0.f;
         int best_k = 0;
-        for (int k = 0; k < 3; ++k) {
+        for (int k = 0; k < nkinds; ++k) {
             p->halo64 = k;
             const float t = time_launch(p, [&](cudaStream_t st) {
                 launch_coupling_t<double>(p, nullptr, p->X.p, p->TMP.p, -1.0, p->TMP.p, st);
@@ -1132,7 +1193,7 @@ msc_status autotune_measure(msc_plan *p)
         if (p->use_halo) {
             float best = 0.f;
             int best_k = 0;
-            for (int k = 0; k < 3; ++k) {
+            for (int k = 0; k < nkinds; ++k) {
                 p->halo32 = k;
                 const float t = time_launch(p, [&](cudaStream_t st) {
                     launch_coupling_t<float>(p, nullptr, a, c, 1.0f, b, st);
@@ -1208,6 +1269,98 @@ struct SetupTimer {
 };
 
 msc_status ensure_gs_levels(msc_plan *p);
+
+// Separable coupling: for every z, the tap window W[sdx][sdy] (signed
+// offsets, zero where there is no tap, the centre free) is tested for the
+// form p_sdx q_sdy.  The pivot is the largest entry off the centre row and
+// column; p is its column, q its row divided by it, and every tap must
+// match p q to 1e-13 of the potential's scale at that z, max(|W|, |V_00|):
+// the rounding the potential's own 2-D FFT leaves in its small components
+// (~1e-15 of that scale for the square-lattice Morse potentials) passes,
+// anything structural fails.  A window of zeros gives p = q = 0.  Any z that
+// fails (a hexagonal lattice's coupling, taps only on the centre cross)
+// leaves the plan on the direct kernels.
+void separable_factors(msc_plan *p, const std::vector<int> &win)
+{
+    p->sep_ok = false;
+    const int n = p->n, hx = p->halo_hx, hy = p->halo_hy;
+    const int wx = 2 * hx + 1, wy = 2 * hy + 1;
+    std::vector<double2> P((size_t)wx * n), Q((size_t)wy * n), Kc(n);
+    std::vector<double2> W((size_t)wx * wy);
+    for (int z = 0; z < n; ++z) {
+        double wmax = 0.0;
+        for (int c = 0; c < wx * wy; ++c) {
+            const int t = win[c];
+            W[c] = t >= 0 ? p->Vt_host[(size_t)t * n + z] : double2{0.0, 0.0};
+            wmax = std::max(wmax, std::sqrt(msc::cabs2(W[c])));
+        }
+        int pa = -1, pb = -1;
+        double best = 0.0;
+        for (int a = 0; a < wx; ++a)
+            for (int b = 0; b < wy; ++b) {
+                if (a == hx || b == hy) continue;
+                const double m = msc::cabs2(W[(size_t)a * wy + b]);
+                if (m > best) {
+                    best = m;
+                    pa = a;
+                    pb = b;
+                }
+            }
+        if (pa < 0) {
+            if (wmax > 0.0) return;          // taps on the centre cross only: not a product
+            for (int a = 0; a < wx; ++a) P[(size_t)a * n + z] = double2{0.0, 0.0};
+            for (int b = 0; b < wy; ++b) Q[(size_t)b * n + z] = double2{0.0, 0.0};
+            Kc[z] = double2{0.0, 0.0};
+            continue;
+        }
+        const double2 piv = W[(size_t)pa * wy + pb];
+        for (int a = 0; a < wx; ++a) P[(size_t)a * n + z] = W[(size_t)a * wy + pb];
+        for (int b = 0; b < wy; ++b) Q[(size_t)b * n + z] = msc::cdiv(W[(size_t)pa * wy + b], piv);
+        for (int a = 0; a < wx; ++a)
+            for (int b = 0; b < wy; ++b) {
+                if (a == hx && b == hy) continue;
+                const double2 pq = msc::cmul(P[(size_t)a * n + z], Q[(size_t)b * n + z]);
+                const double2 d = msc::csub(W[(size_t)a * wy + b], pq);
+                if (std::sqrt(msc::cabs2(d)) > 1e-13 * std::max(wmax, std::fabs(p->v00_host[z])))
+                    return;
+            }
+        Kc[z] = msc::cmul(P[(size_t)hx * n + z], Q[(size_t)hy * n + z]);
+    }
+    p->sep_p_h.swap(P);
+    p->sep_q_h.swap(Q);
+    p->sep_k_h.swap(Kc);
+    p->sep_ok = true;
+}
+
+// Upload p | q | kappa of the operator in use (A: as found; A^H, whose tap
+// at d is conj(V_{-d}): p_sdx -> conj(p_{-sdx}), q likewise, kappa -> conj).
+msc_status upload_separable(msc_plan *p)
+{
+    const int n = p->n, wx = 2 * p->halo_hx + 1, wy = 2 * p->halo_hy + 1;
+    std::vector<double2> all;
+    all.reserve((size_t)(wx + wy + 1) * n);
+    for (int a = 0; a < wx; ++a)
+        for (int z = 0; z < n; ++z) {
+            const double2 v = p->sep_p_h[(size_t)(p->adjoint ? wx - 1 - a : a) * n + z];
+            all.push_back(p->adjoint ? msc::cconj(v) : v);
+        }
+    for (int b = 0; b < wy; ++b)
+        for (int z = 0; z < n; ++z) {
+            const double2 v = p->sep_q_h[(size_t)(p->adjoint ? wy - 1 - b : b) * n + z];
+            all.push_back(p->adjoint ? msc::cconj(v) : v);
+        }
+    for (int z = 0; z < n; ++z) all.push_back(p->adjoint ? msc::cconj(p->sep_k_h[z]) : p->sep_k_h[z]);
+    std::vector<float2> all32(all.size());
+    for (size_t i = 0; i < all.size(); ++i) all32[i] = make_float2((float)all[i].x, (float)all[i].y);
+    if (p->sep64.count == all.size()) {
+        MSC_CUDA(refill(p->sep64, all));
+        MSC_CUDA(refill(p->sep32, all32));
+    } else {
+        MSC_CUDA(upload(p->sep64, all));
+        MSC_CUDA(upload(p->sep32, all32));
+    }
+    return MSC_OK;
+}
 
 msc_status finalize(msc_plan *p)
 {
@@ -1338,6 +1491,11 @@ msc_status finalize(msc_plan *p)
             p->nwork = (int)(wl.size() / 3);
             MSC_CUDA(upload(p->tap_window, win));
             MSC_CUDA(upload(p->work, wl));
+            separable_factors(p, win);
+            if (p->sep_ok) {
+                msc_status sst = upload_separable(p);
+                if (sst != MSC_OK) return sst;
+            }
         }
     }
     tm.mark("halo tables");
@@ -2189,7 +2347,7 @@ const char *msc_plan_tuning_report(msc_plan *p)
         r += "\"" + p->tune_log[i].first + "\": " + std::to_string(p->tune_log[i].second);
     }
     if (!r.empty() && r.size() > 1) r += ", ";
-    const char *kn[3] = {"neighbour", "halo_y8", "halo_y4"};
+    const char *kn[4] = {"neighbour", "halo_y8", "halo_y4", "separable"};
     r += "\"chosen\": \"coupling64=" + std::string(p->use_halo ? kn[p->halo64] : kn[0]) +
          ",coupling32=" + std::string(p->use_halo ? kn[p->halo32] : kn[0]) +
          ",block_inverse32=" + (p->use_tc ? std::string(p->tc_groups == 2 ? "tc2_N" : "tc_N") + std::to_string(p->tc_n) : std::string("simt")) +
@@ -2266,6 +2424,11 @@ msc_status msc_plan_set_adjoint(msc_plan *p, int32_t adjoint)
         for (double2 &c : rc) c = msc::cconj(c);
     if (p->K > 0) MSC_CUDA(refill(p->Vt, vt));
     MSC_CUDA(refill(p->row_c, rc));
+    p->adjoint = want;
+    if (p->sep_ok) {
+        msc_status sst = upload_separable(p);
+        if (sst != MSC_OK) return sst;
+    }
     if (p->mixed) {
         if (p->K > 0) {
             std::vector<float2> vt32(vt.size());

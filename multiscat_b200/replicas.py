@@ -48,3 +48,21 @@ def gather_to_rank0(local: list, world: int) -> list | None:
     if out is None:
         return None
     return [x for part in out for x in part]
+
+
+def sharded_sweep(conditions: list, config, *, solve=None) -> list | None:
+    """A sweep of many beams over one potential split across the ranks of the
+    process group: rank r solves its contiguous slice of ``conditions`` on its
+    own GPU (``get_scattering_matrices``, one batched plan) and rank 0 gets
+    every beam's |S|^2 grid back in the order of ``conditions``; other ranks
+    get None.  Without a process group it is ``get_scattering_matrices``.
+    ``solve(conditions, config) -> list`` replaces the per-rank solve (the
+    host-side tests run the sharding and the gather without a GPU)."""
+    if solve is None:
+        from .api import get_scattering_matrices as solve
+    if not (dist.is_available() and dist.is_initialized()):
+        return list(solve(conditions, config))
+    world, rank = dist.get_world_size(), dist.get_rank()
+    mine = shard(list(conditions), rank, world)
+    local = list(solve(mine, config)) if mine else []
+    return gather_to_rank0(local, world)

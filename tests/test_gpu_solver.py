@@ -402,7 +402,7 @@ def test_cfg4_batch_mixed_matches_fp64():
 # FP64 operators against the neighbour-table kernel, and mixed solves of a
 # small uneven batch against the FP64 solve.
 # ---------------------------------------------------------------------------
-COUPLING_KINDS = {0: "neighbour", 1: "halo_y8", 2: "halo_y4"}
+COUPLING_KINDS = {0: "neighbour", 1: "halo_y8", 2: "halo_y4", 3: "separable"}
 
 
 @pytest.mark.parametrize("kind", sorted(COUPLING_KINDS))
@@ -429,9 +429,40 @@ def test_every_coupling_kernel_agrees(kind, monkeypatch):
     monkeypatch.setenv("MSC_TUNE", "c64=0,c32=0,bi=0")
     p0 = ScatteringPlan(c0.v, c0.t, [c0.system()])
     y0 = p0.apply_coupling(x)
-    assert float((yk - y0).abs().max()) <= 1e-13 * float(y0.abs().max())
+    # (the separable form sums in another order: 1e-12)
+    assert float((yk - y0).abs().max()) <= (1e-12 if kind == 3 else 1e-13) * float(y0.abs().max())
     pk.close()
     p0.close()
+
+
+def test_separable_coupling_is_found_only_where_the_taps_factorise(monkeypatch):
+    """The square-lattice Morse potentials (cfg0/cfg2/cfg4) factorise, the
+    hexagonal one (cfg1) and the He-LiF cross of four taps do not; a
+    factorised plan is exact in both operators it solves with (A and A^H)."""
+    monkeypatch.setenv("MSC_TUNE", "c64=3,c32=3,bi=0")
+    c0 = cfg0_case(nz=40)
+    pk = ScatteringPlan(c0.v, c0.t, [c0.system()])
+    x = torch.randn(c0.pkd.size, 40, dtype=torch.complex128, device="cuda")
+    yk = pk.apply_coupling(x)
+    assert "coupling64=separable" in pk.tuning_report()["chosen"]
+    pk.set_adjoint(True)
+    ya = pk.apply_coupling(x)
+    pk.close()
+    monkeypatch.setenv("MSC_TUNE", "c64=0,c32=0,bi=0")
+    p0 = ScatteringPlan(c0.v, c0.t, [c0.system()])
+    y0 = p0.apply_coupling(x)
+    p0.set_adjoint(True)
+    y0a = p0.apply_coupling(x)
+    p0.close()
+    assert float((yk - y0).abs().max()) <= 1e-12 * float(y0.abs().max())
+    assert float((ya - y0a).abs().max()) <= 1e-12 * float(y0a.abs().max())
+    monkeypatch.setenv("MSC_TUNE", "c64=3,c32=3,bi=0")
+    for case in (cfg1_case(nz=30, nk=11), wolken_case(nz=40)):
+        p1 = ScatteringPlan(case.v, case.t, [case.system()])
+        p1.apply_coupling(torch.zeros(case.pkd.size, case.v.shape[2], dtype=torch.complex128,
+                                      device="cuda"))
+        assert "separable" not in p1.tuning_report()["chosen"]
+        p1.close()
 
 
 # ---------------------------------------------------------------------------

@@ -11,7 +11,8 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from multiscat_b200.replicas import gather_to_rank0, max_over_ranks, shard, shard_bounds
+from multiscat_b200.replicas import (gather_to_rank0, max_over_ranks, shard, shard_bounds,
+                                     sharded_sweep)
 
 
 def test_shard_bounds_cover_every_item_once():
@@ -66,3 +67,41 @@ def test_single_process_helpers_without_group():
     assert max_over_ranks(3.0) == 3.0
     assert gather_to_rank0([1, 2], 1) == [1, 2]
     assert torch.tensor([1.0]).item() == 1.0
+
+
+def _fake_solve(conditions, config):
+    """Stands in for the per-rank GPU solve: one result per condition."""
+    return [(c.incident_energy, config.precision, os.getpid()) for c in conditions]
+
+
+def _sweep_worker(rank: int, world: int, port: int, out):
+    import math
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        from multiscat_b200 import OptimizationConfig
+        from tests.test_api_host import _sweep_conditions
+        conds = _sweep_conditions(7)
+        res = sharded_sweep(conds, OptimizationConfig(precision=1e-6), solve=_fake_solve)
+        out[rank] = None if res is None else [(r[0], r[1], r[2]) for r in res]
+        out[f"e{rank}"] = [c.incident_energy for c in conds]
+        assert math.isfinite(conds[0].incident_energy)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_sweep_splits_beams_and_gathers_in_order():
+    world = 2
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_sweep_worker, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    assert res[1] is None
+    got = res[0]
+    assert [r[0] for r in got] == res["e0"]                   # every beam once, in order
+    assert all(r[1] == 1e-6 for r in got)
+    pids = [r[2] for r in got]
+    assert len(set(pids[:4])) == 1 and len(set(pids[4:])) == 1 and pids[0] != pids[4]
