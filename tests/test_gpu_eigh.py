@@ -76,7 +76,7 @@ def test_preconditioner_hamiltonians(which):
         case = cfg0_case()
         t, v00 = case.t, case.v[0, 0].real
     elif which == "cfg1":
-        case = cfg1_case(nk=5)
+        case = cfg1_case(nk=9)
         t, v00 = case.t, case.v[0, 0].real
     else:
         nodes, w = sa.lobatto_rule(-2.0, 14.0, 300)

@@ -109,7 +109,7 @@ def test_reference_state_is_lower_block_times_psi():
     s_ref = get_scattering_matrix_from_state(ref_state, cond)
     np.testing.assert_allclose(s_ref.real, golden, rtol=0, atol=1e-5)
     np.testing.assert_allclose(s_ref.real, get_scattering_matrix(cond, cfg).real, rtol=0,
-                               atol=1e-10)
+                               atol=1e-9)
 
 
 @pytest.mark.parametrize("order", [0, 1])

@@ -402,7 +402,7 @@ def test_cfg4_batch_mixed_matches_fp64():
 # FP64 operators against the neighbour-table kernel, and mixed solves of a
 # small uneven batch against the FP64 solve.
 # ---------------------------------------------------------------------------
-COUPLING_KINDS = {0: "neighbour", 1: "halo_y8", 2: "halo_y4", 3: "separable"}
+COUPLING_KINDS = {0: "neighbour", 1: "halo_y8", 2: "halo_y4", 3: "separable", 4: "separable_z2"}
 
 
 @pytest.mark.parametrize("kind", sorted(COUPLING_KINDS))
@@ -430,7 +430,7 @@ def test_every_coupling_kernel_agrees(kind, monkeypatch):
     p0 = ScatteringPlan(c0.v, c0.t, [c0.system()])
     y0 = p0.apply_coupling(x)
     # (the separable form sums in another order: 1e-12)
-    assert float((yk - y0).abs().max()) <= (1e-12 if kind == 3 else 1e-13) * float(y0.abs().max())
+    assert float((yk - y0).abs().max()) <= (1e-12 if kind >= 3 else 1e-13) * float(y0.abs().max())
     pk.close()
     p0.close()
 
@@ -550,6 +550,20 @@ def test_no_kernel_reads_unwritten_memory():
 # Full-state API and warm start (the reference's get_scattering_state /
 # get_scattering_matrix_from_state, _multiscat.py:63-99, 227-246, and x0).
 # ---------------------------------------------------------------------------
+def ref_of(psi, cond):
+    """L psi of a psi-convention state, through the library's lower block."""
+    from multiscat_b200.api import _reference_order_system, natural_arrays
+    from multiscat_b200 import ScatteringPlan
+    arr = natural_arrays(cond)
+    sp = _reference_order_system(arr, None)
+    plan = ScatteringPlan(arr.potential_values, arr.kinetic, [sp], restart=1)
+    rows = torch.as_tensor(np.ascontiguousarray(psi[sp.channel_ix, sp.channel_iy]), device="cuda")
+    out = psi.copy()
+    out[sp.channel_ix, sp.channel_iy] = plan.apply_lower_block(rows).cpu().numpy()
+    plan.close()
+    return out
+
+
 def test_state_api_round_trip_matches_scattering_matrix():
     from multiscat_b200 import get_scattering_matrix_from_state, get_scattering_state
     cond = _wolken_condition(0.0)
@@ -558,7 +572,9 @@ def test_state_api_round_trip_matches_scattering_matrix():
     assert state.shape == (10, 10, 550) and state.dtype == np.complex128
     s_state = get_scattering_matrix_from_state(state, cond)
     s_direct = get_scattering_matrix(cond, cfg)
-    np.testing.assert_allclose(s_state.real, s_direct.real, rtol=0.0, atol=1e-12)
+    # two separate solves (the reference-convention state orders the channels
+    # by pkd), each converged to a relative residual of 1e-10
+    np.testing.assert_allclose(s_state.real, s_direct.real, rtol=0.0, atol=1e-9)
     np.testing.assert_allclose(s_state.real, _read_wolken_golden(), rtol=0.0, atol=1e-5)
     # warm start from the converged state: already below the tolerance
     again = get_scattering_state(cond, cfg, initial_state=state)
@@ -567,6 +583,9 @@ def test_state_api_round_trip_matches_scattering_matrix():
     psi = get_scattering_state(cond, cfg, convention="psi")
     s_psi = get_scattering_matrix_from_state(psi, cond, convention="psi")
     np.testing.assert_allclose(s_psi.real, s_direct.real, rtol=0.0, atol=1e-12)
+    # the reference convention's L^-1 (L psi) returns psi itself
+    np.testing.assert_allclose(get_scattering_matrix_from_state(ref_of(psi, cond), cond).real,
+                               s_psi.real, rtol=0.0, atol=1e-11)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

@@ -53,7 +53,7 @@ def _worker(rank: int, world: int, port: int, out):
 def test_two_rank_replicas_gloo():
     world = 2
     port = _free_port()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
@@ -95,7 +95,7 @@ def _sweep_worker(rank: int, world: int, port: int, out):
 def test_sharded_sweep_splits_beams_and_gathers_in_order():
     world = 2
     port = _free_port()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_sweep_worker, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
