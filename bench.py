@@ -186,14 +186,17 @@ def measure_fma_peaks() -> dict:
 
 
 def kernel_records(kt: dict, res, n: int, taps: int, mixed: bool, dcgs: bool, tensor: bool,
-                   peaks: dict, fma: dict, workload: str) -> dict:
+                   peaks: dict, fma: dict, workload: str, sep: tuple | None = None) -> dict:
     """Per timed kernel kind: its bound, algorithmic work of the rows it
     actually processed, achieved rate and fraction of the measured peak.
 
     block inverse: 8 n^2 flop per row (two real GEMMs of the complex row),
       x3 for the BF16x3 split on tcgen05 (bound: tensor; else the FMA pipe);
     coupling: 8 K n flop per row (K taps, one complex MAC each), ~27 flop per
-      byte at K = 80, so the FMA pipe bounds it, not HBM;
+      byte at K = 80, so the FMA pipe bounds it, not HBM; the separable form
+      (sep = (hx, HY) of its window) does 8 ((2hx+1)(8+2HY)/8 + 2HY + 2) n
+      flop per row, which leaves its FMA and HBM roofs close: the line names
+      the tighter one;
     Arnoldi passes: HBM bytes, one read or write of a row of a Krylov vector
       per vector touched: DCGS2 reduction (j + 1) + 1 reads at step j, update
       (j + 1) + 1 reads and 2 writes; CGS2 first projection (j + 1) + 1 reads,
@@ -226,6 +229,21 @@ def kernel_records(kt: dict, res, n: int, taps: int, mixed: bool, dcgs: bool, te
                         "achieved": fl / t_s / 1e12, "peak": bf16 if tensor else fma_peak,
                         "algorithmic": f"{8 * n * n * (3 if tensor else 1)} flop per row",
                         "rows": r_done, "bytes": 2.0 * es * n * r_done})
+        elif k == "coupling" and sep:
+            hx, hy = sep
+            per_row = 8.0 * ((2 * hx + 1) * (8 + 2 * hy) / 8.0 + 2 * hy + 2) * n
+            fl = per_row * steps_rows
+            nbytes = 3.0 * es * n * steps_rows
+            if fl / (fma_peak * 1e12) >= nbytes / (hbm * 1e9):
+                rec.update({"bound": "fma", "unit": "TFLOP/s", "achieved": fl / t_s / 1e12,
+                            "peak": fma_peak})
+            else:
+                rec.update({"bound": "hbm", "unit": "GB/s", "achieved": nbytes / t_s / 1e9,
+                            "peak": hbm})
+            rec.update({"what": "channel coupling, separable form (x pass + y pass)",
+                        "algorithmic": f"{per_row:.0f} flop and {3 * es * n} bytes per row",
+                        "rows": steps_rows, "bytes": nbytes,
+                        "direct_form_equivalent_tflops": 8.0 * taps * n * steps_rows / t_s / 1e12})
         elif k == "coupling":
             fl = 8.0 * taps * n * steps_rows
             rec.update({"bound": "fma", "unit": "TFLOP/s", "achieved": fl / t_s / 1e12,
@@ -243,7 +261,7 @@ def kernel_records(kt: dict, res, n: int, taps: int, mixed: bool, dcgs: bool, te
                         "peak": hbm, "algorithmic": "one pass per Krylov vector row touched",
                         "rows": steps_rows, "bytes": nbytes})
         rec["frac"] = rec["achieved"] / rec["peak"]
-        tr = NCU_TRAFFIC.get((workload, k))
+        tr = NCU_TRAFFIC.get((workload, k if not (k == "coupling" and sep) else "coupling_sep"))
         if tr and mixed and "bytes" in rec:
             per_row = tr[0] / tr[1]
             alg_per_row = (3.0 if k == "coupling" else 2.0) * es * n
@@ -319,15 +337,20 @@ def run_b200(args) -> None:
     peaks, peak_kind = load_peaks()
     fma = measure_fma_peaks()
     tensor = mixed and "tc_" in tuning.get("chosen", "")
+    chosen = tuning.get("chosen", "")
+    sep = None
+    if ("coupling32=separable" if mixed else "coupling64=separable") in chosen:
+        sep = (int(tuning.get("halo_hx", 0)), int(tuning.get("halo_hy", 0)))
     kernels = kernel_records(kt, res, n, taps, mixed, args.gram_schmidt == "dcgs2", tensor,
-                             peaks, fma, args.workload)
+                             peaks, fma, args.workload, sep)
     roof = None
     if kernels:
         dom = max(kernels, key=lambda k: kernels[k]["share_of_timed_kernels"])
         kr = kernels[dom]
         nl = kr["launches"]
         traffic = None
-        tr = NCU_TRAFFIC.get((args.workload, dom))
+        tr = NCU_TRAFFIC.get((args.workload, dom if not (dom == "coupling" and sep)
+                              else "coupling_sep"))
         if tr and mixed:
             traffic = tr[0] / tr[1] * (kr["rows"] / nl)      # at this run's average rows per launch
         roof = {"kernel": f"{dom}: {kr['what']}", "bound": kr["bound"], "achieved": kr["achieved"],

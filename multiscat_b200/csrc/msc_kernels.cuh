@@ -1477,7 +1477,7 @@ __device__ __forceinline__ bool dcgs_stop(const GmresState &st, int s, double es
 //   coef[0..j)        a_i = -s_i / nu            (q_j = v / nu + sum a_i Q_i)
 //   coef[j+1 .. 2j+1) b_i = -(c_i - s_i d / nu)  (v_{j+1} = w / nu - (d / nu) v + sum b_i Q_i)
 //   coef[2m+2] = (1 / nu, 0), coef[2m+3] = -d / nu
-__device__ void dcgs_coefficients(GmresState &st, const DcgsState &ds, int s, int m, int j,
+__device__ __noinline__ void dcgs_coefficients(GmresState &st, const DcgsState &ds, int s, int m, int j,
                                   double rtol, double inner_rtol)
 {
     const double2 *sum = ds.dsum + (size_t)s * 2 * (m + 1);

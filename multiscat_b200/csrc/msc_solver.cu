@@ -475,11 +475,10 @@ size_t sep_smem(int hx, int hy, int zc, size_t elem)
     return (hxw * hyw + (2 * hx + 1) + (2 * hy + 1) + 1) * zc * elem + hxw * hyw * sizeof(int);
 }
 
-template <int HY, typename R>
+template <int HY, int ZC, typename R>
 void launch_sep(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
                 C2<R> *out, cudaStream_t st)
 {
-    constexpr int ZC = halo_zc<R>();
     msc::CouplingTiles ct{p->work.p, p->pos_map.p, p->tap_window.p, p->nwork, p->nkx, p->nky,
                           p->halo_hx, p->K};
     const size_t np = (size_t)(2 * p->halo_hx + 1) * p->n, nq = (size_t)(2 * p->halo_hy + 1) * p->n;
@@ -493,15 +492,17 @@ void launch_sep(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0
             ct, gate, p->n, sep, src, in0, sgn, out);
 }
 
-template <typename R>
+// ZC: z values per block (the halo kernel's, or half of it: half the shared
+// memory, twice the resident blocks to hide the halo loads)
+template <int ZC, typename R>
 void launch_sep_hy(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
                    C2<R> *out, cudaStream_t st)
 {
     switch (p->halo_hy) {
-    case 1: launch_sep<1, R>(p, gate, src, in0, sgn, out, st); return;
-    case 2: launch_sep<2, R>(p, gate, src, in0, sgn, out, st); return;
-    case 4: launch_sep<4, R>(p, gate, src, in0, sgn, out, st); return;
-    default: launch_sep<8, R>(p, gate, src, in0, sgn, out, st); return;
+    case 1: launch_sep<1, ZC, R>(p, gate, src, in0, sgn, out, st); return;
+    case 2: launch_sep<2, ZC, R>(p, gate, src, in0, sgn, out, st); return;
+    case 4: launch_sep<4, ZC, R>(p, gate, src, in0, sgn, out, st); return;
+    default: launch_sep<8, ZC, R>(p, gate, src, in0, sgn, out, st); return;
     }
 }
 
@@ -510,11 +511,20 @@ void launch_coupling_t(msc_plan *p, const int *gate, const C2<R> *src, const C2<
                        C2<R> *out, cudaStream_t st)
 {
     // coupling kind per precision: 0 neighbour table, 1 halo (8 y/thread), 2 halo (4 y/thread),
-    // 3 separable (two 1-D passes; only when the tap windows factorise)
+    // 3 separable (two 1-D passes; only when the tap windows factorise),
+    // 4 separable with half the z per block
     const int kind = p->use_halo ? (std::is_same<R, float>::value ? p->halo32 : p->halo64) : 0;
     if (kind == 1) { launch_halo_ys<8, R>(p, gate, src, in0, sgn, out, st); return; }
     if (kind == 2) { launch_halo_ys<4, R>(p, gate, src, in0, sgn, out, st); return; }
-    if (kind == 3 && p->sep_ok) { launch_sep_hy<R>(p, gate, src, in0, sgn, out, st); return; }
+    if (kind == 3 && p->sep_ok) {
+        launch_sep_hy<halo_zc<R>(), R>(p, gate, src, in0, sgn, out, st);
+        return;
+    }
+    if (kind == 4 && p->sep_ok) {
+        launch_sep_hy<halo_zc<R>() / 2, R>(p, gate, src, in0, sgn, out, st);
+        return;
+    }
+
     dim3 grid(p->ntiles, (p->n + 31) / 32);
     dim3 block(32, msc::kTileRows);
     msc::k_coupling<R><<<grid, block, smem_coupling(std::max(p->K, 1)), st>>>(
@@ -872,7 +882,10 @@ msc_status set_kernel_attributes(int n, int K)
 #define MSC_SEP_ATTR(HY, R)                                                                      \
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>(), R>,              \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
-                                  (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448)));
+                                  (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448))); \
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>() / 2, R>,          \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                  (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>() / 2, sizeof(C2<R>)), 232448)));
     MSC_SEP_ATTR(1, float)
     MSC_SEP_ATTR(2, float)
     MSC_SEP_ATTR(4, float)
@@ -1121,7 +1134,7 @@ bool tune_from_env(msc_plan *p)
     if (!env || !*env) return false;
     int c64 = p->halo64, c32 = p->halo32, bi = p->use_tc ? p->tc_n : 0, bg = 1;
     std::sscanf(env, "c64=%d,c32=%d,bi=%d,bg=%d", &c64, &c32, &bi, &bg);
-    const int kmax = p->sep_ok ? 3 : 2;
+    const int kmax = p->sep_ok ? 4 : 2;
     p->halo64 = p->use_halo ? std::max(0, std::min(kmax, c64)) : 0;
     p->halo32 = p->use_halo ? std::max(0, std::min(kmax, c32)) : 0;
     if (p->use_tc) {
@@ -1168,8 +1181,8 @@ msc_status autotune_measure(msc_plan *p)
     const size_t vs = (size_t)p->R * p->n;
     MSC_CUDA(cudaMemsetAsync(p->X.p, 0, vs * sizeof(double2), p->stream));
     MSC_CUDA(cudaMemsetAsync(p->TMP.p, 0, vs * sizeof(double2), p->stream));
-    const char *kind_name[4] = {"neighbour", "halo_y8", "halo_y4", "separable"};
-    const int nkinds = p->sep_ok ? 4 : 3;
+    const char *kind_name[5] = {"neighbour", "halo_y8", "halo_y4", "separable", "separable_z2"};
+    const int nkinds = p->sep_ok ? 5 : 3;
     if (p->use_halo) {
         float best = 0.f;
         int best_k = 0;
@@ -2347,7 +2360,9 @@ const char *msc_plan_tuning_report(msc_plan *p)
         r += "\"" + p->tune_log[i].first + "\": " + std::to_string(p->tune_log[i].second);
     }
     if (!r.empty() && r.size() > 1) r += ", ";
-    const char *kn[4] = {"neighbour", "halo_y8", "halo_y4", "separable"};
+    const char *kn[5] = {"neighbour", "halo_y8", "halo_y4", "separable", "separable_z2"};
+    r += "\"halo_hx\": " + std::to_string(p->use_halo ? p->halo_hx : 0) + ", \"halo_hy\": " +
+         std::to_string(p->use_halo ? p->halo_hy : 0) + ", ";
     r += "\"chosen\": \"coupling64=" + std::string(p->use_halo ? kn[p->halo64] : kn[0]) +
          ",coupling32=" + std::string(p->use_halo ? kn[p->halo32] : kn[0]) +
          ",block_inverse32=" + (p->use_tc ? std::string(p->tc_groups == 2 ? "tc2_N" : "tc_N") + std::to_string(p->tc_n) : std::string("simt")) +

@@ -170,18 +170,33 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar)
                  : "memory");
 }
 
-// 32 lanes x 16 consecutive 32-bit columns.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
+// 32 lanes x 16 consecutive 32-bit columns, issued without waiting: several
+// loads go out back to back and one tmem_wait_ld completes them (the
+// epilogues read up to 64 columns per warp and M tile at once instead of
+// paying the load latency per 16).
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[16])
 {
-    uint32_t r[16];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Up to four 16-column chunks starting at column c (warp-uniform count nch),
+// one wait for all of them.
+__device__ __forceinline__ void tmem_ld_chunks(uint32_t taddr, int nch, float (&v)[4][16])
+{
+    uint32_t r[4][16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    for (int q = 0; q < 4; ++q)
+        if (q < nch) tmem_ld16_nowait(taddr + (uint32_t)(16 * q), r[q]);
+    tmem_wait_ld();
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[q][i] = __uint_as_float(r[q][i]);
 }
 
 // Shared-memory matrix descriptor (no swizzle, canonical 8x16-byte core matrices).
@@ -243,6 +258,16 @@ __device__ __forceinline__ float warp_reduce_scatter16(float (&v)[16], int lane)
         v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
     }
     return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+// 1 / (pkd + lam_k): the sum in FP64 (pkd and lam_k cancel near a channel
+// resonance), the reciprocal by the SFU's approximate FP32 divide (two
+// instructions instead of the correctly rounded sequence; its 2-ulp error
+// is far below the BF16x3 products').  Both epilogues call it, so the
+// Sherman-Morrison sums and yt use the same values.
+__device__ __forceinline__ float shifted_inverse(double pkd, double lam)
+{
+    return __fdividef(1.0f, (float)(pkd + lam));
 }
 
 struct TcParams {
@@ -487,9 +512,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
             const bool valid = k < n;
             const double lam_k = valid ? prm.lam[k] : 0.0;
             const float en_k = valid ? (float)prm.en[k] : 0.f;
-            for (int c0 = c_begin; c0 < c_begin + HALF; c0 += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + c0), v);
+            for (int cb = c_begin; cb < c_begin + HALF; cb += 64) {
+            const int nch = min(4, (c_begin + HALF - cb) >> 4);
+            float vv[4][16];
+            tmem_ld_chunks(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + cb), nch, vv);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (q >= nch) continue;
+                const int c0 = cb + 16 * q;
+                float (&v)[16] = vv[q];
 #pragma unroll
                 for (int c = 0; c < 16; c += 2) {
                     // select, not multiply: accumulator rows k >= kp of the last
@@ -497,7 +528,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     // NaN, which a zero weight would not remove
                     const int j = (c0 + c) >> 1;
                     if (valid && j < nrow) {
-                        const float w = en_k * __frcp_rn((float)(pkd_s[g][j] + lam_k));
+                        const float w = en_k * shifted_inverse(pkd_s[g][j], lam_k);
                         v[c] *= w;
                         v[c + 1] *= w;
                     } else {
@@ -507,6 +538,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                 }
                 const float sum = warp_reduce_scatter16(v, lane);
                 if ((lane & 1) == 0) sm_part[g][wl][m][c0 + ((lane >> 1) & 15)] = sum;
+            }
             }
         }
         group_sync(bar_id, GT);
@@ -539,17 +571,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
             const bool stage = k < kp;
             const double lam_k = valid ? prm.lam[k] : 0.0;
             const float en_k = valid ? (float)prm.en[k] : 0.f;
-            for (int c0 = c_begin; c0 < c_begin + HALF; c0 += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + c0), v);
-                if (!stage) continue;
+            for (int cb = c_begin; cb < c_begin + HALF; cb += 64) {
+            const int nch = min(4, (c_begin + HALF - cb) >> 4);
+            float vv[4][16];
+            tmem_ld_chunks(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + cb), nch, vv);
+            if (!stage) continue;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (q >= nch) continue;
+                const int c0 = cb + 16 * q;
+                const float (&v)[16] = vv[q];
                 uint32_t hw[8], lw[8];
 #pragma unroll
                 for (int c = 0; c < 16; c += 2) {
                     const int j = (c0 + c) >> 1;
                     float yr = 0.f, yi = 0.f;
                     if (valid && j < nrow) {
-                        const float inv = __frcp_rn((float)(pkd_s[g][j] + lam_k));
+                        const float inv = shifted_inverse(pkd_s[g][j], lam_k);
                         const float2 b = beta_s[g][j];
                         yr = (v[c] + b.x * en_k) * inv;
                         yi = (v[c + 1] + b.y * en_k) * inv;
@@ -566,6 +604,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                 *reinterpret_cast<uint4 *>(b_hi + o + 128) = make_uint4(hw[4], hw[5], hw[6], hw[7]);
                 *reinterpret_cast<uint4 *>(b_lo + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
                 *reinterpret_cast<uint4 *>(b_lo + o + 128) = make_uint4(lw[4], lw[5], lw[6], lw[7]);
+            }
             }
         }
         tc_fence_before();
@@ -611,14 +650,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         // ---- epilogue 2: u rows to global (z contiguous across lanes)
         for (int m = 0; m < mt_count && epi; ++m) {
             const int z = m * 128 + lq * 32 + lane;
-            for (int c0 = c_begin; c0 < c_begin + HALF; c0 += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)((mt_count + m) * N + c0), v);
+            for (int cb = c_begin; cb < c_begin + HALF; cb += 64) {
+                const int nch = min(4, (c_begin + HALF - cb) >> 4);
+                float vv[4][16];
+                tmem_ld_chunks(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)((mt_count + m) * N + cb),
+                               nch, vv);
                 if (z < n) {
 #pragma unroll
-                    for (int c = 0; c < 16; c += 2) {
-                        const int j = (c0 + c) >> 1;
-                        if (j < nrow) prm.out[(size_t)(row0 + j) * n + z] = make_float2(v[c], v[c + 1]);
+                    for (int q = 0; q < 4; ++q) {
+                        if (q >= nch) continue;
+#pragma unroll
+                        for (int c = 0; c < 16; c += 2) {
+                            const int j = (cb + 16 * q + c) >> 1;
+                            if (j < nrow)
+                                prm.out[(size_t)(row0 + j) * n + z] = make_float2(vv[q][c], vv[q][c + 1]);
+                        }
                     }
                 }
             }

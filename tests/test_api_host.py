@@ -266,3 +266,10 @@ def test_bench_kernel_records_classify_each_kernel_by_its_bound():
         assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
     simt = bench.kernel_records(kt, Res, n, taps, False, False, False, peaks, fma, "cfg2")
     assert simt["block_inverse"]["bound"] == "fma" and simt["block_inverse"]["peak"] == 35.0
+    sep = bench.kernel_records(kt, Res, n, taps, True, True, True, peaks, fma, "cfg2", (4, 4))
+    per_row = 8 * (9 * 16 / 8 + 10) * n                       # 28 complex MACs per output
+    fl, nb = per_row * steps_rows, 3 * 8 * n * steps_rows
+    c = sep["coupling"]
+    assert c["bound"] == ("fma" if fl / 70e12 >= nb / 6000e9 else "hbm")
+    want = fl / 1e-3 / 1e12 if c["bound"] == "fma" else nb / 1e-3 / 1e9
+    assert c["achieved"] == pytest.approx(want)

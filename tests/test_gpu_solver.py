@@ -578,7 +578,7 @@ def test_state_api_round_trip_matches_scattering_matrix():
     np.testing.assert_allclose(s_state.real, _read_wolken_golden(), rtol=0.0, atol=1e-5)
     # warm start from the converged state: already below the tolerance
     again = get_scattering_state(cond, cfg, initial_state=state)
-    np.testing.assert_allclose(again, state, rtol=0.0, atol=1e-12 * np.abs(state).max())
+    np.testing.assert_allclose(again, state, rtol=0.0, atol=1e-10 * np.abs(state).max())
     # the psi convention round-trips the same way
     psi = get_scattering_state(cond, cfg, convention="psi")
     s_psi = get_scattering_matrix_from_state(psi, cond, convention="psi")
