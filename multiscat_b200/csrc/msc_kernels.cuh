@@ -364,92 +364,144 @@ k_coupling_masked(Tiles tiles, const int *__restrict__ gate, int n, int K,
 //   y_r = D_r^-1 (x_r - sum_{r' < r} V_{r r'} y_{r'}).
 // One CTA per system.  Rows are taken level by level (a row's level is one
 // more than the highest level among its lower neighbours, so the rows of a
-// level do not depend on each other); the warps share a level's rows, one
-// row per warp, and a barrier closes every level.  D_r^-1 in the eigenbasis
-// of H0 with the Sherman-Morrison boundary term, as k_block_inverse:
-//   xt = E^T s, sigma = sum_k en_k xt_k / (pkd + lam_k),
-//   beta = c sigma / (1 - c f_n), y = E (xt + beta en) / (pkd + lam).
-// Vectors in R (FP32 in the mixed form's inner solve), arithmetic in FP64.
-// Dynamic shared memory: 2 n double2 per warp.
+// level do not depend on each other), up to kGsRows rows of a level at a
+// time, each phase spread over all threads of the CTA:
+//   A  s_b(z) = x_b(z) - sum_{lower taps} V_t(z) y_{nbr}(z)     (b, z) per thread
+//   B  xt_b(k) = sum_z E(z, k) s_b(z)                           (b, k) per thread
+//   C  beta_b = c sigma / (1 - c f_n), sigma = sum_k en_k xt_b(k) / (pkd_b + lam_k)
+//   D  yt_b(k) = (xt_b(k) + beta_b en_k) / (pkd_b + lam_k)
+//   E  y_b(z) = sum_k E(z, k) yt_b(k)                           (b, z) per thread
+// with D_r^-1 in the eigenbasis of H0 and the Sherman-Morrison boundary
+// term, as k_block_inverse.  E (FP64, or FP32 in the mixed form's inner
+// solve) sits in shared memory with a row stride of n + 1 (both the k-major
+// and the z-major walk are free of bank conflicts) when it fits, else it is
+// read from L2.  pkd + lam is formed in FP64 for both precisions.
 // ---------------------------------------------------------------------------
 struct GsLevels {
     const int *sys_lvl;     // [B + 1]  first level of each system
     const int *lvl_start;   // [levels + 1]  first entry of each level in lvl_rows
     const int *lvl_rows;    // [R]  rows, system by system, level by level
+    const int *low_ptr;     // [R + 1]  each row's lower neighbours at low_ptr[r] .. low_ptr[r + 1]
+    const int *low_tap;     //          their coupling tap
+    const int *low_row;     //          and their row
 };
+
+constexpr int kGsRows = 8;
 
 template <typename R>
 __global__ void __launch_bounds__(256)
 k_gs_sweep(int nsys, const int *__restrict__ gate, int n, int K,
            const typename CT<R>::t *__restrict__ Vt, const int *__restrict__ nbr, GsLevels lv,
-           const double *__restrict__ E, const double *__restrict__ ET,
-           const double *__restrict__ lam, const double *__restrict__ en,
-           const double *__restrict__ row_pkd, const double2 *__restrict__ row_c,
-           const double *__restrict__ row_fn, const typename CT<R>::t *__restrict__ x,
-           typename CT<R>::t *__restrict__ y)
+           const R *__restrict__ E, int e_in_smem, const double *__restrict__ lam,
+           const double *__restrict__ en, const double *__restrict__ row_pkd,
+           const double2 *__restrict__ row_c, const double *__restrict__ row_fn,
+           const typename CT<R>::t *__restrict__ x, typename CT<R>::t *__restrict__ y)
 {
     using C2 = typename CT<R>::t;
-    extern __shared__ double2 gs_sm[];
+    extern __shared__ __align__(16) unsigned char gs_raw[];
     const int s = blockIdx.x;
     if (s >= nsys || (gate && gate[s] == 0)) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    double2 *sv = gs_sm + (size_t)warp * 2 * n;
-    double2 *tv = sv + n;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int ld = e_in_smem ? n + 1 : n;
+    R *Es = reinterpret_cast<R *>(gs_raw);
+    C2 *sv = reinterpret_cast<C2 *>(gs_raw + (e_in_smem ? ((size_t)n * ld * sizeof(R) + 15) / 16 * 16 : 0));
+    C2 *tv = sv + (size_t)kGsRows * n;
+    __shared__ double2 beta_s[kGsRows];
+    __shared__ int row_s[kGsRows];
+    if (e_in_smem) {
+        for (int i = tid; i < n * n; i += nt) {
+            const int z = i / n, k = i - z * n;
+            Es[z * ld + k] = E[i];
+        }
+    }
+    const R *Em = e_in_smem ? Es : E;
+    __syncthreads();
     for (int L = lv.sys_lvl[s]; L < lv.sys_lvl[s + 1]; ++L) {
-        for (int i = lv.lvl_start[L] + warp; i < lv.lvl_start[L + 1]; i += nw) {
-            const int r = lv.lvl_rows[i];
-            const int *nb = nbr + (size_t)r * K;
-            for (int z = lane; z < n; z += 32) {
+        for (int i0 = lv.lvl_start[L]; i0 < lv.lvl_start[L + 1]; i0 += kGsRows) {
+            const int nb = min(kGsRows, lv.lvl_start[L + 1] - i0);
+            if (tid < nb) row_s[tid] = lv.lvl_rows[i0 + tid];
+            __syncthreads();
+            // A: right-hand side minus the lower coupling
+            for (int idx = tid; idx < nb * n; idx += nt) {
+                const int b = idx / n, z = idx - b * n;
+                const int r = row_s[b];
                 const C2 xv = x[(size_t)r * n + z];
-                double ar = (double)xv.x, ai = (double)xv.y;
-                for (int t = 0; t < K; ++t) {
-                    const int j = nb[t];
-                    if (j < 0 || j >= r) continue;
+                R ar = xv.x, ai = xv.y;
+                const int e1 = __ldg(lv.low_ptr + r + 1);
+#pragma unroll 8
+                for (int e = __ldg(lv.low_ptr + r); e < e1; ++e) {
+                    const int t = __ldg(lv.low_tap + e), j = __ldg(lv.low_row + e);
                     const C2 v = Vt[(size_t)t * n + z];
                     const C2 u = y[(size_t)j * n + z];
-                    ar -= (double)v.x * (double)u.x - (double)v.y * (double)u.y;
-                    ai -= (double)v.x * (double)u.y + (double)v.y * (double)u.x;
+                    ar -= v.x * u.x - v.y * u.y;
+                    ai -= v.x * u.y + v.y * u.x;
                 }
-                sv[z] = make_double2(ar, ai);
+                sv[(size_t)b * n + z] = mk2<R>(ar, ai);
             }
-            __syncwarp();
-            const double pk = row_pkd[r];
-            double sr = 0.0, si = 0.0;
-            for (int k = lane; k < n; k += 32) {
-                double ar = 0.0, ai = 0.0;
+            __syncthreads();
+            // B: xt = E^T s
+            for (int idx = tid; idx < nb * n; idx += nt) {
+                const int b = idx / n, k = idx - b * n;
+                const C2 *sb = sv + (size_t)b * n;
+                R ar = 0, ai = 0;
+#pragma unroll 4
                 for (int z = 0; z < n; ++z) {
-                    const double e = __ldg(E + (size_t)z * n + k);
-                    ar = fma(e, sv[z].x, ar);
-                    ai = fma(e, sv[z].y, ai);
+                    const R e = Em[(size_t)z * ld + k];
+                    const C2 q = sb[z];
+                    ar = fma(e, q.x, ar);
+                    ai = fma(e, q.y, ai);
                 }
-                tv[k] = make_double2(ar, ai);
-                const double w = en[k] / (pk + lam[k]);
-                sr = fma(w, ar, sr);
-                si = fma(w, ai, si);
+                tv[(size_t)b * n + k] = mk2<R>(ar, ai);
             }
-            sr = warp_sum(sr);
-            si = warp_sum(si);
-            const double2 c = row_c[r];
-            const double fn = row_fn[r];
-            const double2 beta = cdiv(cmul(c, make_double2(sr, si)), make_double2(1.0 - c.x * fn, -c.y * fn));
-            for (int k = lane; k < n; k += 32) {
-                const double inv = 1.0 / (pk + lam[k]);
-                const double2 t = tv[k];
-                tv[k] = make_double2((t.x + beta.x * en[k]) * inv, (t.y + beta.y * en[k]) * inv);
+            __syncthreads();
+            // C: the Sherman-Morrison scalar of each row, one warp per row
+            for (int b = warp; b < nb; b += nt >> 5) {
+                const int r = row_s[b];
+                const double pk = row_pkd[r];
+                double sr = 0.0, si = 0.0;
+                for (int k = lane; k < n; k += 32) {
+                    const double w = en[k] / (pk + lam[k]);
+                    const C2 q = tv[(size_t)b * n + k];
+                    sr = fma(w, (double)q.x, sr);
+                    si = fma(w, (double)q.y, si);
+                }
+                sr = warp_sum(sr);
+                si = warp_sum(si);
+                if (lane == 0) {
+                    const double2 c = row_c[r];
+                    const double fn = row_fn[r];
+                    beta_s[b] = cdiv(cmul(c, make_double2(sr, si)), make_double2(1.0 - c.x * fn, -c.y * fn));
+                }
             }
-            __syncwarp();
-            for (int z = lane; z < n; z += 32) {
-                double ar = 0.0, ai = 0.0;
+            __syncthreads();
+            // D: yt = (xt + beta en) / (pkd + lam)
+            for (int idx = tid; idx < nb * n; idx += nt) {
+                const int b = idx / n, k = idx - b * n;
+                const double inv = 1.0 / (row_pkd[row_s[b]] + lam[k]);
+                const double2 bb = beta_s[b];
+                const C2 q = tv[idx];
+                tv[idx] = mk2<R>((R)(((double)q.x + bb.x * en[k]) * inv),
+                                 (R)(((double)q.y + bb.y * en[k]) * inv));
+            }
+            __syncthreads();
+            // E: y = E yt
+            for (int idx = tid; idx < nb * n; idx += nt) {
+                const int b = idx / n, z = idx - b * n;
+                const C2 *tb = tv + (size_t)b * n;
+                const R *ez = Em + (size_t)z * ld;
+                R ar = 0, ai = 0;
+#pragma unroll 4
                 for (int k = 0; k < n; ++k) {
-                    const double e = __ldg(ET + (size_t)k * n + z);
-                    ar = fma(e, tv[k].x, ar);
-                    ai = fma(e, tv[k].y, ai);
+                    const R e = ez[k];
+                    const C2 q = tb[k];
+                    ar = fma(e, q.x, ar);
+                    ai = fma(e, q.y, ai);
                 }
-                y[(size_t)r * n + z] = mk2<R>((R)ar, (R)ai);
+                y[(size_t)row_s[b] * n + z] = mk2<R>(ar, ai);
             }
-            __syncwarp();
+            __syncthreads();    // these rows are written before the next rows read them
         }
-        __syncthreads();    // this level's rows are written before the next level reads them
     }
 }
 
@@ -475,7 +527,10 @@ struct CouplingTiles {
     int ntaps;                // K
 };
 
-template <int HY, int BX, int ZC, int YS, typename R>
+// MASK 1 / 2: only the source channels with a smaller / larger row index
+// than the output's (V^lower / V^upper of the block Gauss-Seidel splitting,
+// as k_coupling_masked); 0: the full coupling.
+template <int HY, int BX, int ZC, int YS, typename R, int MASK = 0>
 __global__ void __launch_bounds__(BX * ZC * (8 / YS))
 k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
                 const typename CT<R>::t *__restrict__ Vt, const typename CT<R>::t *__restrict__ src,
@@ -592,19 +647,34 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
         ar[y] = 0;
         ai[y] = 0;
     }
+    int orow[MASK ? YS : 1];
+    if (MASK) {
+#pragma unroll
+        for (int y = 0; y < YS; ++y) orow[y] = rows[(tx + HX) * HYW + ysub * YS + y + HY];
+    }
     for (int sdx = -HX; sdx <= HX; ++sdx) {
         const int hx = tx - sdx + HX;
         const C2 *colp = halo + ((size_t)hx * HYW + ysub * YS) * ZC + zl;
         C2 col[CW];
 #pragma unroll
         for (int i = 0; i < CW; ++i) col[i] = colp[(size_t)i * ZC];
+        int crow[MASK ? CW : 1];
+        if (MASK) {
+#pragma unroll
+            for (int i = 0; i < CW; ++i) crow[i] = rows[hx * HYW + ysub * YS + i];
+        }
         const C2 *vrow = vw + (size_t)(sdx + HX) * WY * ZC + zl;
 #pragma unroll
         for (int sdy = -HY; sdy <= HY; ++sdy) {
             const C2 v = vrow[(sdy + HY) * ZC];
 #pragma unroll
             for (int y = 0; y < YS; ++y) {
-                const C2 q = col[y - sdy + HY];
+                C2 q = col[y - sdy + HY];
+                if (MASK) {
+                    const int sr = crow[MASK ? y - sdy + HY : 0], orr = orow[MASK ? y : 0];
+                    const bool keep = MASK == 1 ? sr < orr : sr > orr;
+                    if (!keep) q = mk2<R>(0, 0);
+                }
                 ar[y] = fma(v.x, q.x, fma(-v.y, q.y, ar[y]));
                 ai[y] = fma(v.x, q.y, fma(v.y, q.x, ai[y]));
             }

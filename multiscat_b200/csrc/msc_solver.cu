@@ -174,8 +174,8 @@ struct msc_plan {
     // level sets of every system's rows (k_gs_sweep)
     bool gs = false;
     bool gs_ready = false;
-    int gs_warps = 8;
-    DevBuf<int> gs_sys_lvl, gs_lvl_start, gs_lvl_rows;
+    bool gs_e64_smem = false, gs_e32_smem = false;   // E held in the sweep's shared memory
+    DevBuf<int> gs_sys_lvl, gs_lvl_start, gs_lvl_rows, gs_low_ptr, gs_low_tap, gs_low_row;
     bool dcgs = true;              // DCGS2 (two basis passes per step); false: CGS2
     DevBuf<double> scale, bnorm, resid, est, beta0;
     // mixed form: FP32 copies of the operator data and the FP32 Krylov space
@@ -263,6 +263,7 @@ struct msc_plan {
         U32.release(); R64.release(); e_img.release(); tc_error.release();
         Hraw.release(); dsum.release(); dcoef.release(); gsave.release();
         gs_sys_lvl.release(); gs_lvl_start.release(); gs_lvl_rows.release();
+        gs_low_ptr.release(); gs_low_tap.release(); gs_low_row.release();
         sep64.release(); sep32.release();
     }
 
@@ -444,7 +445,7 @@ size_t halo_smem(int hx, int hy, int zc, size_t elem)
            (size_t)(kHaloBX + 2 * hx) * (8 + 2 * hy) * sizeof(int);
 }
 
-template <int HY, int YS, typename R>
+template <int HY, int YS, typename R, int MASK = 0>
 void launch_halo(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
                  C2<R> *out, cudaStream_t st)
 {
@@ -452,20 +453,20 @@ void launch_halo(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in
     msc::CouplingTiles ct{p->work.p, p->pos_map.p, p->tap_window.p, p->nwork, p->nkx, p->nky,
                           p->halo_hx, p->K};
     dim3 grid(p->nwork, (p->n + ZC - 1) / ZC);
-    msc::k_coupling_halo<HY, kHaloBX, ZC, YS, R>
+    msc::k_coupling_halo<HY, kHaloBX, ZC, YS, R, MASK>
         <<<grid, kHaloBX * ZC * (8 / YS), halo_smem(p->halo_hx, HY, ZC, sizeof(C2<R>)), st>>>(
             ct, gate, p->n, OpData<R>::Vt(p), src, in0, sgn, out);
 }
 
-template <int YS, typename R>
+template <int YS, typename R, int MASK = 0>
 void launch_halo_ys(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
                     C2<R> *out, cudaStream_t st)
 {
     switch (p->halo_hy) {
-    case 1: launch_halo<1, YS, R>(p, gate, src, in0, sgn, out, st); return;
-    case 2: launch_halo<2, YS, R>(p, gate, src, in0, sgn, out, st); return;
-    case 4: launch_halo<4, YS, R>(p, gate, src, in0, sgn, out, st); return;
-    default: launch_halo<8, YS, R>(p, gate, src, in0, sgn, out, st); return;
+    case 1: launch_halo<1, YS, R, MASK>(p, gate, src, in0, sgn, out, st); return;
+    case 2: launch_halo<2, YS, R, MASK>(p, gate, src, in0, sgn, out, st); return;
+    case 4: launch_halo<4, YS, R, MASK>(p, gate, src, in0, sgn, out, st); return;
+    default: launch_halo<8, YS, R, MASK>(p, gate, src, in0, sgn, out, st); return;
     }
 }
 
@@ -537,27 +538,43 @@ void launch_coupling(msc_plan *p, const int *gate, const double2 *src, const dou
     launch_coupling_t<double>(p, gate, src, in0, sgn, out, st);
 }
 
-// Lower (mask 1) or upper (mask 2) part of the coupling in plan row order.
+// Lower (mask 1) or upper (mask 2) part of the coupling in plan row order:
+// the halo kernel with the row test when the plan has halo tables, else
+// the neighbour table.
 template <typename R>
 void launch_coupling_masked_t(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0,
                               R sgn, int mask, C2<R> *out, cudaStream_t st)
 {
+    if (p->use_halo) {
+        if (mask == 1) launch_halo_ys<4, R, 1>(p, gate, src, in0, sgn, out, st);
+        else launch_halo_ys<4, R, 2>(p, gate, src, in0, sgn, out, st);
+        return;
+    }
     dim3 grid(p->ntiles, (p->n + 31) / 32);
     dim3 block(32, msc::kTileRows);
     msc::k_coupling_masked<R><<<grid, block, smem_coupling(std::max(p->K, 1)), st>>>(
         p->tiles(), gate, p->n, p->K, OpData<R>::Vt(p), p->nbr.p, src, in0, sgn, mask, out);
 }
 
-size_t gs_smem(int n, int warps) { return (size_t)warps * 2 * n * sizeof(double2); }
+// Shared memory of the Gauss-Seidel sweep: E with row stride n + 1 when
+// e_in_smem, then the s and t buffers of kGsRows rows.
+template <typename R>
+size_t gs_smem(int n, bool e_in_smem)
+{
+    const size_t e = e_in_smem ? ((size_t)n * (n + 1) * sizeof(R) + 15) / 16 * 16 : 0;
+    return e + 2 * (size_t)msc::kGsRows * n * sizeof(C2<R>);
+}
 
 // y = L^-1 x (block Gauss-Seidel forward sweep), one CTA per system.
 template <typename R>
 void launch_gs_sweep_t(msc_plan *p, const int *gate, const C2<R> *x, C2<R> *y, cudaStream_t st)
 {
-    const msc::GsLevels lv{p->gs_sys_lvl.p, p->gs_lvl_start.p, p->gs_lvl_rows.p};
-    msc::k_gs_sweep<R><<<p->B, 32 * p->gs_warps, gs_smem(p->n, p->gs_warps), st>>>(
-        p->B, gate, p->n, p->K, OpData<R>::Vt(p), p->nbr.p, lv, p->E.p, p->ET.p, p->lam.p, p->en.p,
-        p->row_pkd.p, p->row_c.p, p->row_fn.p, x, y);
+    const msc::GsLevels lv{p->gs_sys_lvl.p, p->gs_lvl_start.p, p->gs_lvl_rows.p,
+                           p->gs_low_ptr.p, p->gs_low_tap.p, p->gs_low_row.p};
+    const bool es = std::is_same<R, float>::value ? p->gs_e32_smem : p->gs_e64_smem;
+    msc::k_gs_sweep<R><<<p->B, 256, gs_smem<R>(p->n, es), st>>>(
+        p->B, gate, p->n, p->K, OpData<R>::Vt(p), p->nbr.p, lv, OpData<R>::E(p), es ? 1 : 0,
+        p->lam.p, p->en.p, p->row_pkd.p, p->row_c.p, p->row_fn.p, x, y);
 }
 
 template <typename R>
@@ -895,6 +912,19 @@ msc_status set_kernel_attributes(int n, int K)
     MSC_SEP_ATTR(4, double)
     MSC_SEP_ATTR(8, double)
 #undef MSC_SEP_ATTR
+#define MSC_HALO_MASK_ATTR(HY, R, M)                                                              \
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_halo<HY, kHaloBX, halo_zc<R>(), 4, R, M>,       \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                  (int)std::min<size_t>(halo_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448)));
+    MSC_HALO_MASK_ATTR(1, float, 1) MSC_HALO_MASK_ATTR(2, float, 1)
+    MSC_HALO_MASK_ATTR(4, float, 1) MSC_HALO_MASK_ATTR(8, float, 1)
+    MSC_HALO_MASK_ATTR(1, float, 2) MSC_HALO_MASK_ATTR(2, float, 2)
+    MSC_HALO_MASK_ATTR(4, float, 2) MSC_HALO_MASK_ATTR(8, float, 2)
+    MSC_HALO_MASK_ATTR(1, double, 1) MSC_HALO_MASK_ATTR(2, double, 1)
+    MSC_HALO_MASK_ATTR(4, double, 1) MSC_HALO_MASK_ATTR(8, double, 1)
+    MSC_HALO_MASK_ATTR(1, double, 2) MSC_HALO_MASK_ATTR(2, double, 2)
+    MSC_HALO_MASK_ATTR(4, double, 2) MSC_HALO_MASK_ATTR(8, double, 2)
+#undef MSC_HALO_MASK_ATTR
     MSC_HALO_ATTR(1, float)
     MSC_HALO_ATTR(2, float)
     MSC_HALO_ATTR(4, float)
@@ -1650,10 +1680,13 @@ msc_status ensure_gs_levels(msc_plan *p)
     if (p->gs_ready) return MSC_OK;
     const int ntor = p->nkx * p->nky;
     std::vector<int> sys_lvl(p->B + 1, 0), lvl_start, rows;
+    std::vector<int> low_ptr(1, 0), low_tap, low_row;   // lower neighbours per row (CSR)
     rows.reserve(p->R);
+    low_ptr.reserve(p->R + 1);
     std::vector<int> pos_row(ntor, -1);
     for (int s = 0; s < p->B; ++s) {
         const SystemHost &sh = p->sys[s];
+        const int r0 = p->sys_row0_h[s];
         for (int j = 0; j < sh.C; ++j) pos_row[sh.ix[j] * p->nky + sh.iy[j]] = j;
         std::vector<int> lvl(sh.C, 0);
         int nlvl = 0;
@@ -1665,8 +1698,13 @@ msc_status ensure_gs_levels(msc_plan *p)
                 int sy = sh.iy[j] - p->taps[t].second;
                 sy += sy < 0 ? p->nky : 0;
                 const int q = pos_row[sx * p->nky + sy];
-                if (q >= 0 && q < j) best = std::max(best, lvl[q]);
+                if (q >= 0 && q < j) {
+                    best = std::max(best, lvl[q]);
+                    low_tap.push_back(t);
+                    low_row.push_back(r0 + q);
+                }
             }
+            low_ptr.push_back((int)low_tap.size());
             lvl[j] = best + 1;
             nlvl = std::max(nlvl, lvl[j] + 1);
         }
@@ -1683,17 +1721,26 @@ msc_status ensure_gs_levels(msc_plan *p)
     }
     sys_lvl[p->B] = (int)lvl_start.size();
     lvl_start.push_back((int)rows.size());
+    if (low_tap.empty()) {
+        low_tap.push_back(0);
+        low_row.push_back(0);
+    }
+    MSC_CUDA(upload(p->gs_low_ptr, low_ptr));
+    MSC_CUDA(upload(p->gs_low_tap, low_tap));
+    MSC_CUDA(upload(p->gs_low_row, low_row));
     MSC_CUDA(upload(p->gs_sys_lvl, sys_lvl));
     MSC_CUDA(upload(p->gs_lvl_start, lvl_start));
     MSC_CUDA(upload(p->gs_lvl_rows, rows));
     int dev = 0, optin = 0;
     MSC_CUDA(cudaGetDevice(&dev));
     MSC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    p->gs_warps = 8;
-    while (p->gs_warps > 1 && gs_smem(p->n, p->gs_warps) > (size_t)optin - 4096) p->gs_warps /= 2;
-    const int bytes = (int)gs_smem(p->n, p->gs_warps);
-    MSC_CUDA(cudaFuncSetAttribute(msc::k_gs_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    MSC_CUDA(cudaFuncSetAttribute(msc::k_gs_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    const size_t room = (size_t)optin - 1024;    // static shared memory of the kernel
+    p->gs_e64_smem = gs_smem<double>(p->n, true) <= room;
+    p->gs_e32_smem = p->E32.p && gs_smem<float>(p->n, true) <= room;
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_gs_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)gs_smem<double>(p->n, p->gs_e64_smem)));
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_gs_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)gs_smem<float>(p->n, p->gs_e32_smem)));
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_masked<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem_coupling(msc::kMaxTaps)));
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_masked<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
