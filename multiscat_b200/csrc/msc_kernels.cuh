@@ -1613,7 +1613,7 @@ template <> struct DcgsUnroll<double> { static constexpr int value = 4; };
 // a fixed order (deterministic).  The last block of a system reduces the
 // per-block partials and runs dcgs_coefficients.
 template <typename R>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 2)
 k_dcgs_reduce(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int j,
               const typename CT<R>::t *__restrict__ W, GmresState st, DcgsState ds, int m,
               double rtol, double inner_rtol)
@@ -1643,13 +1643,25 @@ k_dcgs_reduce(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int j,
             vv[u] = (e < ne) ? vp[e] : mk2<R>(0, 0);
             ww[u] = (e < ne) ? wp[e] : mk2<R>(0, 0);
         }
+        // q_i is loaded one vector ahead, so its loads are in flight while
+        // the previous vector's products and warp sums run
+        C2 qn[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = base + u * 32 + lane;
+            qn[u] = (e < ne) ? Q[e0 + e] : mk2<R>(0, 0);
+        }
         for (int i = 0; i < nv; ++i) {
-            const C2 *q = Q + (size_t)i * a.qstride + e0;
             C2 qv[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int e = base + u * 32 + lane;
-                qv[u] = (e < ne) ? q[e] : mk2<R>(0, 0);
+            for (int u = 0; u < U; ++u) qv[u] = qn[u];
+            if (i + 1 < nv) {
+                const C2 *q = Q + (size_t)(i + 1) * a.qstride + e0;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int e = base + u * 32 + lane;
+                    qn[u] = (e < ne) ? q[e] : mk2<R>(0, 0);
+                }
             }
             double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
 #pragma unroll
