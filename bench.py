@@ -162,6 +162,7 @@ def oracle_fixture_error(res, workload: str, beams: int, world: int) -> dict | N
 NCU_TRAFFIC = {
     # (workload, kind): (bytes, rows of the captured launch, profile)
     ("cfg2", "coupling"): (439.8e6 + 138.9e6, 119741, "k_coupling_halo_f32_cfg2.md"),
+    ("cfg2", "coupling_sep"): (79.125e6 + 14.128e6, 30011, "kernels_cfg2_128beams.md"),
     ("cfg2", "block_inverse"): (148.2e6 + 94.3e6, 119741, "k_block_inverse_tc_cfg2.md"),
 }
 
