@@ -62,7 +62,7 @@ typedef struct {
     double rtol;            /* stop when ||b - A psi|| <= rtol ||b|| (per system)*/
     int32_t precision;      /* msc_precision                                    */
     int32_t inner_restart;  /* mixed: inner FP32 restart (0 = min(restart, 20)) */
-    double inner_rtol;      /* mixed: inner relative tolerance (0 = 1e-5)       */
+    double inner_rtol;      /* mixed: inner relative tolerance (0 = 3e-6)       */
     int32_t max_refinements;/* mixed: outer FP64 refinement steps (0 = 30)      */
     int32_t flags;          /* bit 0: mixed form without the tcgen05 kernel;
                                bit 1: keep the tcgen05 kernel even when the
