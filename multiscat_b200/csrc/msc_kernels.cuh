@@ -680,19 +680,20 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
             }
         }
     }
-    const int gx = x0 + tx;
+    // output rows from the staged rows table; the in0 loads of all YS
+    // outputs go out before the stores
+    int rowv[YS];
+    C2 base[YS];
 #pragma unroll
-    for (int y = 0; y < YS; ++y) {
-        const int gy = y0 + ysub * YS + y;
-        if (gy < nky) {
-            const int row = pr[gx * nky + gy];
-            if (row >= 0) {
-                const size_t o = (size_t)row * n + z;
-                const C2 base = in0 ? in0[o] : mk2<R>(0, 0);
-                out[o] = mk2<R>(base.x + sgn * ar[y], base.y + sgn * ai[y]);
-            }
-        }
-    }
+    for (int y = 0; y < YS; ++y)
+        rowv[y] = (y0 + ysub * YS + y < nky) ? rows[(tx + HX) * HYW + ysub * YS + y + HY] : -1;
+#pragma unroll
+    for (int y = 0; y < YS; ++y)
+        base[y] = (in0 && rowv[y] >= 0) ? in0[(size_t)rowv[y] * n + z] : mk2<R>(0, 0);
+#pragma unroll
+    for (int y = 0; y < YS; ++y)
+        if (rowv[y] >= 0)
+            out[(size_t)rowv[y] * n + z] = mk2<R>(base[y].x + sgn * ar[y], base[y].y + sgn * ai[y]);
 }
 
 // ---------------------------------------------------------------------------
@@ -717,11 +718,18 @@ struct SepTaps {
     const void *kappa;   // [n] complex (R)
 };
 
-template <int HY, int BX, int ZC, typename R>
-__global__ void __launch_bounds__(BX * ZC)
+// BULK = 1 stages the halo with bulk copies instead of loads and stores
+// through registers: the z range [z0, z0 + ZC) of a halo position is one
+// contiguous run of the row-major source, so each position with a row is
+// one cp.async.bulk (ZC elements, 256 bytes), all completing on one
+// mbarrier; positions without a row and the z tail past n are zeroed by
+// plain stores.  Needs 16-byte aligned runs: n even for FP32.  A wait that
+// times out sets *err and the block returns without writing.
+template <int HY, int BX, int ZC, typename R, int BULK = 0>
+__global__ void __launch_bounds__(BX * ZC, HY <= 4 ? 3 : 1)
 k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps sep,
                const typename CT<R>::t *__restrict__ src, const typename CT<R>::t *__restrict__ in0,
-               R sgn, typename CT<R>::t *__restrict__ out)
+               R sgn, typename CT<R>::t *__restrict__ out, int *err = nullptr)
 {
     using C2 = typename CT<R>::t;
     constexpr int BY = 8;
@@ -773,8 +781,44 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
         colany[threadIdx.x] = any;
     }
     __syncthreads();
-    constexpr int kU = 8;
     const int total = npos * ZC;
+    if constexpr (BULK != 0) {
+        __shared__ __align__(8) uint64_t bar;
+        __shared__ int nvalid;
+        const int cnt = min(ZC, n - z0);
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_fence_init();
+            nvalid = 0;
+        }
+        __syncthreads();
+        int mine = 0;
+        for (int pidx = threadIdx.x; pidx < npos; pidx += NT) mine += rows[pidx] >= 0;
+        if (mine) atomicAdd(&nvalid, mine);
+        for (int idx = threadIdx.x; idx < total; idx += NT) {
+            const int pidx = idx / ZC, zl = idx - pidx * ZC;
+            if (rows[pidx] < 0 || zl >= cnt) halo[idx] = mk2<R>(0, 0);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) mbar_expect_tx(&bar, (uint32_t)nvalid * (uint32_t)cnt * (uint32_t)sizeof(C2));
+        __syncthreads();
+        for (int pidx = threadIdx.x; pidx < npos; pidx += NT) {
+            const int row = rows[pidx];
+            if (row >= 0)
+                bulk_g2s(halo + (size_t)pidx * ZC, src + (size_t)row * n + z0,
+                         (uint32_t)cnt * (uint32_t)sizeof(C2), &bar);
+        }
+        const bool got = mbar_wait(&bar, 0);
+        if (!__syncthreads_and(got)) {
+            if (threadIdx.x == 0) {
+                if (err) atomicExch(err, 1);
+                (void)mbar_wait(&bar, 0);        // copies still in flight land before the exit
+            }
+            __syncthreads();
+            return;
+        }
+    } else {
+    constexpr int kU = 8;
     if (std::is_same<R, float>::value && (n % 2) == 0) {
         const int total2 = total / 2;
         float4 *halo4 = reinterpret_cast<float4 *>(halo);
@@ -817,6 +861,7 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
             }
         }
     }
+    }
     __syncthreads();
 
     const int zl = threadIdx.x % ZC;
@@ -846,13 +891,20 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
     for (int i = 0; i < WY; ++i) qv[i] = qw[i * ZC + zl];
     const C2 kap = kw[zl];
     const C2 *own = halo + (size_t)(tx + HX) * HYW * ZC + zl;
-    const int gx = x0 + tx;
+    // the patch column's rows come from the staged rows table (its interior
+    // positions), and the in0 values of all BY outputs are loaded before the
+    // arithmetic: no global load waits on another inside the output loop
+    int rowv[BY];
+    C2 base[BY];
+#pragma unroll
+    for (int y = 0; y < BY; ++y)
+        rowv[y] = (y0 + y < nky) ? rows[(tx + HX) * HYW + y + HY] : -1;
+#pragma unroll
+    for (int y = 0; y < BY; ++y)
+        base[y] = (in0 && rowv[y] >= 0) ? in0[(size_t)rowv[y] * n + z] : mk2<R>(0, 0);
 #pragma unroll
     for (int y = 0; y < BY; ++y) {
-        const int gy = y0 + y;
-        if (gy >= nky) continue;
-        const int row = pr[gx * nky + gy];
-        if (row < 0) continue;
+        if (rowv[y] < 0) continue;
         const C2 c = own[(size_t)(y + HY) * ZC];
         R ar = -(kap.x * c.x - kap.y * c.y), ai = -(kap.x * c.y + kap.y * c.x);
 #pragma unroll
@@ -862,9 +914,7 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
             ar = fma(q.x, xr, fma(-q.y, xi, ar));
             ai = fma(q.x, xi, fma(q.y, xr, ai));
         }
-        const size_t o = (size_t)row * n + z;
-        const C2 base = in0 ? in0[o] : mk2<R>(0, 0);
-        out[o] = mk2<R>(base.x + sgn * ar, base.y + sgn * ai);
+        out[(size_t)rowv[y] * n + z] = mk2<R>(base[y].x + sgn * ar, base[y].y + sgn * ai);
     }
 }
 
@@ -1612,6 +1662,14 @@ template <> struct DcgsUnroll<double> { static constexpr int value = 4; };
 // vector (q_i^H v, q_i^H w), reduced across the warp per vector and added in
 // a fixed order (deterministic).  The last block of a system reduces the
 // per-block partials and runs dcgs_coefficients.
+// Precision: a lane's products and its partial sum of U terms are formed in
+// the vectors' own type (FP32 for the inner solve of the mixed form: FP64
+// products there made the FP64 pipe, not memory, the limit), the sums across
+// lanes, warps and blocks in FP64.  The FP32 partials err by ~U ulp of the
+// terms, the level of the FP32 basis itself; the quantities DCGS2 forms from
+// them do not cancel: s = Q^H v is the small second-pass correction of an
+// already projected v (nu^2 = ||v||^2 - ||s||^2 keeps ||v||^2), and the
+// first-pass error of t = Q^H w is what the next step's s removes.
 template <typename R>
 __global__ void __launch_bounds__(256, 2)
 k_dcgs_reduce(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int j,
@@ -1663,24 +1721,24 @@ k_dcgs_reduce(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int j,
                     qn[u] = (e < ne) ? q[e] : mk2<R>(0, 0);
                 }
             }
-            double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
+            // products and the lane's partial sum of U terms in the vectors'
+            // own precision, the sums across lanes, warps and blocks in FP64
+            R ar = 0, ai = 0, br = 0, bi = 0;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const double qx = (double)qv[u].x, qy = (double)qv[u].y;
-                ar = fma(qx, (double)vv[u].x, fma(qy, (double)vv[u].y, ar));
-                ai = fma(qx, (double)vv[u].y, fma(-qy, (double)vv[u].x, ai));
-                br = fma(qx, (double)ww[u].x, fma(qy, (double)ww[u].y, br));
-                bi = fma(qx, (double)ww[u].y, fma(-qy, (double)ww[u].x, bi));
+                const R qx = qv[u].x, qy = qv[u].y;
+                ar = fma(qx, vv[u].x, fma(qy, vv[u].y, ar));
+                ai = fma(qx, vv[u].y, fma(-qy, vv[u].x, ai));
+                br = fma(qx, ww[u].x, fma(qy, ww[u].y, br));
+                bi = fma(qx, ww[u].y, fma(-qy, ww[u].x, bi));
             }
-            ar = warp_sum(ar);
-            ai = warp_sum(ai);
-            br = warp_sum(br);
-            bi = warp_sum(bi);
+            const double sar = warp_sum((double)ar), sai = warp_sum((double)ai);
+            const double sbr = warp_sum((double)br), sbi = warp_sum((double)bi);
             if (lane == 0) {
                 double2 &x = red[i][warp];
                 double2 &y = red[nv + i][warp];
-                x.x += ar; x.y += ai;
-                y.x += br; y.y += bi;
+                x.x += sar; x.y += sai;
+                y.x += sbr; y.y += sbi;
             }
         }
     }
@@ -1693,6 +1751,145 @@ k_dcgs_reduce(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int j,
             acc.y += red[i][w].y;
         }
         out[i] = acc;
+    }
+    if (last_block_reduce(a, s, 2 * nv, ds.dsum + (size_t)s * 2 * (m + 1))) {
+        if (threadIdx.x == 0) dcgs_coefficients(st, ds, s, m, j, rtol, inner_rtol);
+    }
+}
+
+// Reduction pass of step j with the basis streamed through shared memory
+// (FP32 Krylov vectors).  The block's chunk of each basis vector is one
+// contiguous range, so it arrives by a single cp.async.bulk into a ring of
+// kBulkStages stages, each completing on its own mbarrier: up to
+// kBulkStages vectors are in flight while one is reduced (the register form
+// above keeps one).  Two blocks per SM (3 stages of 32 KB each and 128
+// registers); one block with 6 stages was slower (239 against 186 us per
+// launch on the 512-beam cfg2 batch: 8 warps cannot keep up the FP32 work).  v and w stay in registers (thread t holds element
+// pairs t, t + 256, ...), and slot j (v itself) is reduced from them, so v
+// is read once.  Sums, their fixed order across warps and the last block's
+// work are those of k_dcgs_reduce.  Needs chunks of at most kBulkChunk
+// elements, an even count, starting on an even element (16-byte aligned
+// copies).  A wait that times out sets *err; the block then stops reducing,
+// waits (bounded) for its copies in flight and still takes part in the
+// per-system arrival count.
+constexpr int kBulkChunk = 4096;
+constexpr int kBulkStages = 3;
+
+__host__ __device__ constexpr size_t dcgs_bulk_smem() { return (size_t)kBulkStages * kBulkChunk * 8; }
+
+__global__ void __launch_bounds__(256, 2)
+k_dcgs_reduce_bulk(ArnoldiArgs a, const float2 *__restrict__ Q, int j, const float2 *__restrict__ W,
+                   GmresState st, DcgsState ds, int m, double rtol, double inner_rtol, int *err)
+{
+    constexpr int NW = 8, NT = 256;
+    constexpr int UP = kBulkChunk / (2 * NT);          // element pairs per thread
+    constexpr int SP = kBulkChunk / 2;                 // float4 per stage
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4 *ring = reinterpret_cast<float4 *>(smem_raw);
+    __shared__ __align__(8) uint64_t full[kBulkStages];
+    __shared__ double2 red[2 * (kMaxRestart + 1)][NW];
+    const int blk = blockIdx.x;
+    const int s = a.tiles.sys[blk];
+    if (a.gate && a.gate[s] == 0) return;
+    size_t e0;
+    int ne;
+    elem_range<float>(a, blk, 0, e0, ne);
+    const int np = ne >> 1;
+    const uint32_t bytes = (uint32_t)ne * 8u;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nv = j + 1;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < kBulkStages; ++q) mbar_init(&full[q], 1);
+        mbar_fence_init();
+    }
+    for (int i = threadIdx.x; i < 2 * nv * NW; i += NT) red[i / NW][i % NW] = make_double2(0.0, 0.0);
+    __syncthreads();
+    int issued = 0;                                    // thread 0: vectors whose copy was issued
+    if (threadIdx.x == 0) {
+        for (; issued < min(kBulkStages, j); ++issued) {
+            mbar_expect_tx(&full[issued], bytes);
+            bulk_g2s(ring + (size_t)issued * SP, Q + (size_t)issued * a.qstride + e0, bytes,
+                     &full[issued]);
+        }
+    }
+    const float4 *vp = reinterpret_cast<const float4 *>(Q + (size_t)j * a.qstride + e0);
+    const float4 *wp = reinterpret_cast<const float4 *>(W + e0);
+    float4 vv[UP], ww[UP];
+#pragma unroll
+    for (int u = 0; u < UP; ++u) {
+        const int p = threadIdx.x + u * NT;
+        vv[u] = p < np ? vp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+        ww[u] = p < np ? wp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    // dots of one vector's pairs with v and w (FP32 products and lane
+    // partial sums, as k_dcgs_reduce<float>); pair u comes from load(u)
+    auto dots = [&](auto load, float &ar, float &ai, float &br, float &bi) {
+#pragma unroll
+        for (int u = 0; u < UP; ++u) {
+            const float4 qu = load(u);
+            const float qe[4] = {qu.x, qu.y, qu.z, qu.w};
+            const float ve[4] = {vv[u].x, vv[u].y, vv[u].z, vv[u].w};
+            const float we[4] = {ww[u].x, ww[u].y, ww[u].z, ww[u].w};
+#pragma unroll
+            for (int h = 0; h < 4; h += 2) {
+                const float qx = qe[h], qy = qe[h + 1];
+                ar = fmaf(qx, ve[h], fmaf(qy, ve[h + 1], ar));
+                ai = fmaf(qx, ve[h + 1], fmaf(-qy, ve[h], ai));
+                br = fmaf(qx, we[h], fmaf(qy, we[h + 1], br));
+                bi = fmaf(qx, we[h + 1], fmaf(-qy, we[h], bi));
+            }
+        }
+    };
+    auto add_sums = [&](int i, float ar, float ai, float br, float bi) {
+        const double sar = warp_sum((double)ar), sai = warp_sum((double)ai);
+        const double sbr = warp_sum((double)br), sbi = warp_sum((double)bi);
+        if (lane == 0) {
+            red[i][warp] = make_double2(sar, sai);
+            red[nv + i][warp] = make_double2(sbr, sbi);
+        }
+    };
+    bool ok = true;
+    int i = 0;
+    for (; i < j; ++i) {
+        const int stg = i % kBulkStages;
+        const bool got = mbar_wait(&full[stg], (uint32_t)(i / kBulkStages) & 1u);
+        const float4 *qs = ring + (size_t)stg * SP;
+        float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
+        dots([&](int u) {
+            const int p = threadIdx.x + u * NT;
+            return (got && p < np) ? qs[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }, ar, ai, br, bi);
+        add_sums(i, ar, ai, br, bi);
+        // every thread is done with this stage before it is refilled
+        if (!__syncthreads_and(got)) {
+            ok = false;
+            break;
+        }
+        if (threadIdx.x == 0 && issued < j) {
+            fence_proxy_async();
+            mbar_expect_tx(&full[stg], bytes);
+            bulk_g2s(ring + (size_t)stg * SP, Q + (size_t)issued * a.qstride + e0, bytes, &full[stg]);
+            ++issued;
+        }
+    }
+    if (ok) {
+        float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;   // slot j: v^H v and v^H w
+        dots([&](int u) { return vv[u]; }, ar, ai, br, bi);
+        add_sums(j, ar, ai, br, bi);
+    } else if (threadIdx.x == 0) {
+        if (err) atomicExch(err, 1);
+        for (int q = i; q < issued; ++q)
+            (void)mbar_wait(&full[q % kBulkStages], (uint32_t)(q / kBulkStages) & 1u);
+    }
+    __syncthreads();
+    double2 *out = a.partial + (size_t)blk * a.pstride;
+    for (int k = threadIdx.x; k < 2 * nv; k += NT) {
+        double2 acc = red[k][0];
+        for (int w = 1; w < NW; ++w) {
+            acc.x += red[k][w].x;
+            acc.y += red[k][w].y;
+        }
+        out[k] = acc;
     }
     if (last_block_reduce(a, s, 2 * nv, ds.dsum + (size_t)s * 2 * (m + 1))) {
         if (threadIdx.x == 0) dcgs_coefficients(st, ds, s, m, j, rtol, inner_rtol);

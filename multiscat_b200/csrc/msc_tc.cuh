@@ -19,10 +19,11 @@
 // CTA.  The B operands (x, then yt) are staged per tile of channels by the
 // threads themselves (FP32 -> BF16 hi/lo, re/im de-interleaved).
 //
-// Execution.  Persistent CTAs (one per SM, 256 threads = 8 warps).  Per tile:
-// stage x as B with 16-byte stores; one thread issues the MMAs and commits to
-// an mbarrier; all warps read the accumulator with tcgen05.ld (warp w owns
-// TMEM lanes 32 (w % 4)..32 (w % 4) + 31 and the column half w / 4), reduce
+// Execution.  Persistent CTAs (one per SM, 512 threads = 16 warps).  Per
+// tile: stage x as B with 16-byte stores; one thread issues the MMAs and
+// commits to an mbarrier; all warps read the accumulator with tcgen05.ld
+// (warp w owns TMEM lanes 32 (w % 4)..32 (w % 4) + 31 and the columns of
+// its column group w / 4: a quarter of N with one group), reduce
 // the Sherman-Morrison sums over k with a reduce-scatter butterfly, form
 // yt (pkd + lam in FP64) and stage it as the MN-major B operand of the second
 // GEMM with 16-byte stores, store u.  beta is formed from the accumulator
@@ -32,8 +33,13 @@
 // on time-out the kernel records an error code, stops issuing work and still
 // releases its TMEM.
 //
-// Warp groups.  With G = 2 the 8 warps form two groups of 4 (each group's
-// warps cover the four TMEM lane quarters and all N columns); each group has
+// The epilogues are chains of short dependent steps (TMEM load, FP64 sum
+// and SFU reciprocal, shuffles); 16 warps keep four per scheduler to hide
+// them, with at most 128 registers per thread (the accumulator is read 32
+// columns at a time).
+//
+// Warp groups.  With G = 2 the 16 warps form two groups of 8 (each group's
+// warps cover the four TMEM lane quarters and two column halves); each group has
 // its own B buffer, TMEM columns, mbarrier and named barrier and runs its own
 // tile loop (tiles 2 b + g, stride 2 gridDim), so one group's staging and
 // epilogues can overlap the other's MMAs.  G is autotuned with N.
@@ -46,72 +52,7 @@
 namespace msc {
 namespace tc {
 
-constexpr int kThreads = 256;   // 8 warps: warp w reads TMEM lanes 32 (w % 4)..; G = 1: columns half w / 4
-constexpr long long kSpinLimit = 1ll << 26;   // polls before a wait is declared hung
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_fence_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait: true when the phase completed, false after kSpinLimit polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
-{
-    for (long long i = 0; i < kSpinLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(smem_dst)),
-        "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void cp_async_16(void *smem_dst, const void *gsrc)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-__device__ __forceinline__ void fence_proxy_async()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
+constexpr int kThreads = 512;   // 16 warps: warp w reads TMEM lanes 32 (w % 4).. of its column group
 
 // Named barrier `id` over `count` threads (a warp group's tile loop; barrier
 // 0 stays the CTA-wide __syncthreads).
@@ -184,17 +125,18 @@ __device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[1
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// Up to four 16-column chunks starting at column c (warp-uniform count nch),
-// one wait for all of them.
-__device__ __forceinline__ void tmem_ld_chunks(uint32_t taddr, int nch, float (&v)[4][16])
+// Up to kLdChunks 16-column chunks starting at column c (warp-uniform count
+// nch), one wait for all of them.
+constexpr int kLdChunks = 2;
+__device__ __forceinline__ void tmem_ld_chunks(uint32_t taddr, int nch, float (&v)[kLdChunks][16])
 {
-    uint32_t r[4][16];
+    uint32_t r[kLdChunks][16];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < kLdChunks; ++q)
         if (q < nch) tmem_ld16_nowait(taddr + (uint32_t)(16 * q), r[q]);
     tmem_wait_ld();
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < kLdChunks; ++q)
 #pragma unroll
         for (int i = 0; i < 16; ++i) v[q][i] = __uint_as_float(r[q][i]);
 }
@@ -293,8 +235,8 @@ __device__ __forceinline__ uint32_t kmaj_off(int c, int k, int rows)
     return (uint32_t)(((k >> 3) * (rows >> 3) + (c >> 3)) * 128 + (c & 7) * 16 + (k & 7) * 2);
 }
 
-// G = 1: the CTA's 8 warps work on one tile at a time.  G = 2: two groups
-// of 4 warps (warps 0-3, 4-7), each with its own B buffer, TMEM columns,
+// G = 1: the CTA's 16 warps work on one tile at a time.  G = 2: two groups
+// of 8 warps (warps 0-7, 8-15), each with its own B buffer, TMEM columns,
 // mbarrier and named barrier, run independent tile loops over the shared E
 // image, so that one group's staging and epilogues overlap the other's MMAs.
 template <int N, int G>
@@ -308,20 +250,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     constexpr int TR = N / 2;                 // channels per tile
     constexpr int P = GT / TR;                // staging threads per channel
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bar_e, bar_mma[G];
+    __shared__ __align__(8) uint64_t bar_e, bar_mma[G], bar_pf[G];
     __shared__ uint32_t tmem_base_s;
-    __shared__ float sm_part[G][NW][2][N];    // Sherman-Morrison partial sums [group][warp][M tile][col]
+    __shared__ float sm_part[G][4][2][N];     // Sherman-Morrison partial sums [group][lane quarter][M tile][col]
     __shared__ float2 beta_s[G][TR];
     __shared__ double pkd_s[G][TR];
+    __shared__ double lam_s[256];             // eigenvalues of H0 (k < n <= 256), 0 past n
+    __shared__ float en_s[256];               // last components E[n-1, k] (FP32), 0 past n
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = (G == 1) ? 0 : warp / NW;               // group of this thread
     const int gtid = tid - g * GT, wl = warp - g * NW;    // thread / warp index within the group
     const int bar_id = 1 + g;                             // the group's named barrier
     const int lq = warp & 3;                              // TMEM lane quarter of this warp
-    constexpr int HALF = (G == 1 && N >= 32) ? N / 2 : N; // columns per warp
-    const int c_begin = (G == 1 && N >= 32) ? (wl >> 2) * HALF : 0;
-    const bool epi = (G == 2) || (N >= 32) || wl < 4;     // G = 1, N = 16: warps 4-7 sit out the epilogues
+    constexpr int NCG = NW / 4;                           // column groups (warps per lane quarter)
+    constexpr int CW = (N / NCG >= 16) ? N / NCG : 16;    // columns per warp
+    const int c_begin = (wl >> 2) * CW;
+    const bool epi = c_begin < N;                         // narrow tiles: surplus column groups sit out
     const int n = prm.n, kp = prm.kp, mt_count = prm.mt;
     const int kb = kp >> 3;                               // 8-blocks along z and k
     const uint32_t part_bytes = (uint32_t)kp * kp * 2u;   // one of E_hi / E_lo
@@ -336,9 +281,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     while (ncols < (uint32_t)(2 * mt_count * N)) ncols <<= 1;
 
     if (warp == 0) tmem_alloc(&tmem_base_s, G * ncols);
+    for (int k = tid; k < 256; k += kThreads) {
+        lam_s[k] = k < n ? prm.lam[k] : 0.0;
+        en_s[k] = k < n ? (float)prm.en[k] : 0.f;
+    }
     if (tid == 0) {
         mbar_init(&bar_e, 1);
         for (int q = 0; q < G; ++q) mbar_init(&bar_mma[q], 1);
+        for (int q = 0; q < G; ++q) mbar_init(&bar_pf[q], 1);
         mbar_fence_init();
     }
     tc_fence_before();
@@ -388,21 +338,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     };
     // Prefetch: once the second GEMM has consumed the B buffer, the next
     // tile's raw x rows ([TR][n] complex FP32 = 8 TR n bytes, within the B
-    // buffer's 4 N kp = 8 TR kp bytes) are copied into it with cp.async while
-    // the current tile is stored; the next staging converts them from shared
-    // memory.  Needs 16-byte aligned rows (n even) and at most kMaxPf units
-    // per thread held in registers (raw and converted data share the buffer).
-    constexpr int kMaxPf = 5;
+    // buffer's 4 N kp = 8 TR kp bytes; one contiguous range of x) arrive in
+    // it by one bulk copy on the group's mbarrier while the current tile is
+    // stored; the next staging converts them from shared memory.  Needs a
+    // 16-byte aligned range (n even, x 16-byte aligned) and at most kMaxPf
+    // units per thread held in registers (raw and converted data share the
+    // buffer).
+    constexpr int kMaxPf = 4;
     const int upt = (kb + P - 1) / P;
-    const bool use_pf = (n % 2 == 0) && upt <= kMaxPf;
+    const bool use_pf = (n % 2 == 0) && upt <= kMaxPf &&
+                        (reinterpret_cast<uintptr_t>(prm.x) & 15u) == 0;
     float2 *raw = reinterpret_cast<float2 *>(b_hi);
+    uint32_t pf_phase = 0;
+    bool pf_pending = false;
     auto prefetch = [&](int t) {
-        const int r0 = t * TR, nr = min(TR, prm.rows - r0), half = n >> 1;
-        for (int idx = gtid; idx < nr * half; idx += GT) {
-            const int j = idx / half, q = idx - j * half;
-            cp_async_16(raw + (size_t)j * n + 2 * q, prm.x + (size_t)(r0 + j) * n + 2 * q);
+        if (gtid == 0) {
+            const int r0 = t * TR, nr = min(TR, prm.rows - r0);
+            const uint32_t bytes = (uint32_t)nr * (uint32_t)n * 8u;
+            mbar_expect_tx(&bar_pf[g], bytes);
+            bulk_g2s(raw, prm.x + (size_t)r0 * n, bytes, &bar_pf[g]);
         }
-        cp_async_commit_group();
+        pf_pending = true;
     };
     // first active tile of this group at or after t (stride G gridDim.x); the
     // group's thread 0
@@ -420,6 +376,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     if (gtid == 0) next_s[g] = find_active(G * blockIdx.x + g);
     __syncthreads();
     int tile = next_s[g];
+    __syncthreads();            // every thread has read next_s before the loop rewrites it
     if (use_pf && tile < prm.ntiles) prefetch(tile);
 
     while (tile < prm.ntiles && ok) {
@@ -432,17 +389,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         {
             const bool jok = sj < nrow;
             if (use_pf) {
-                cp_async_wait_all();
-                group_sync(bar_id, GT);                // the raw tile is complete
+                const bool got = mbar_wait(&bar_pf[g], pf_phase);
+                if (!group_and(bar_id, GT, got)) { ok = false; break; }   // the raw tile is complete
+                pf_phase ^= 1u;
+                pf_pending = false;
+                // two z per 16-byte load: the rows' 8 n-byte stride then
+                // spreads a warp's 32 channels over all banks
                 float2 v[kMaxPf][8];
+                const float4 *raw4 = reinterpret_cast<const float4 *>(raw);
 #pragma unroll
                 for (int u = 0; u < kMaxPf; ++u) {
                     const int zb = sp + u * P;
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
+                    for (int e = 0; e < 8; e += 2) {
                         const int z = zb * 8 + e;
-                        v[u][e] = (u < upt && zb < kb && jok && z < n) ? raw[(size_t)sj * n + z]
-                                                                        : make_float2(0.f, 0.f);
+                        float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (u < upt && zb < kb && jok && z < n) t = raw4[((size_t)sj * n + z) >> 1];
+                        v[u][e] = make_float2(t.x, t.y);
+                        v[u][e + 1] = make_float2(t.z, t.w);
                     }
                 }
                 group_sync(bar_id, GT);                // raw reads done before B is overwritten
@@ -491,6 +455,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                 }
             }
             mma_commit(&bar_mma[g]);
+            // the next active tile (its search reads gate and row_sys from
+            // global memory) is found while the MMAs run; every thread of
+            // the group read next_s before the previous tile's last barrier
+            next_s[g] = find_active(tile + G * gridDim.x);
         }
         mma_pending = true;
         if (mbar_wait(&bar_mma[g], mma_phase)) {
@@ -510,14 +478,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         for (int m = 0; m < mt_count && epi; ++m) {
             const int k = m * 128 + lq * 32 + lane;
             const bool valid = k < n;
-            const double lam_k = valid ? prm.lam[k] : 0.0;
-            const float en_k = valid ? (float)prm.en[k] : 0.f;
-            for (int cb = c_begin; cb < c_begin + HALF; cb += 64) {
-            const int nch = min(4, (c_begin + HALF - cb) >> 4);
-            float vv[4][16];
+            const double lam_k = lam_s[k];
+            const float en_k = en_s[k];
+            for (int cb = c_begin; cb < c_begin + CW; cb += 16 * kLdChunks) {
+            const int nch = min(kLdChunks, (c_begin + CW - cb) >> 4);
+            float vv[kLdChunks][16];
             tmem_ld_chunks(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + cb), nch, vv);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kLdChunks; ++q) {
                 if (q >= nch) continue;
                 const int c0 = cb + 16 * q;
                 float (&v)[16] = vv[q];
@@ -537,7 +505,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     }
                 }
                 const float sum = warp_reduce_scatter16(v, lane);
-                if ((lane & 1) == 0) sm_part[g][wl][m][c0 + ((lane >> 1) & 15)] = sum;
+                if ((lane & 1) == 0) sm_part[g][lq][m][c0 + ((lane >> 1) & 15)] = sum;
             }
             }
         }
@@ -547,9 +515,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
             if (j < nrow) {
                 double sr = 0.0, si = 0.0;   // fixed summation order: deterministic
                 // the 4 warps (one per lane quarter) that own column 2j
-                const int wg = (G == 1 && N >= 32) ? ((2 * j) / HALF) * 4 : 0;
                 for (int m = 0; m < mt_count; ++m)
-                    for (int w = wg; w < wg + 4; ++w) {
+                    for (int w = 0; w < 4; ++w) {
                         sr += sm_part[g][w][m][2 * j];
                         si += sm_part[g][w][m][2 * j + 1];
                     }
@@ -569,15 +536,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
             const int k = m * 128 + lq * 32 + lane;
             const bool valid = k < n;
             const bool stage = k < kp;
-            const double lam_k = valid ? prm.lam[k] : 0.0;
-            const float en_k = valid ? (float)prm.en[k] : 0.f;
-            for (int cb = c_begin; cb < c_begin + HALF; cb += 64) {
-            const int nch = min(4, (c_begin + HALF - cb) >> 4);
-            float vv[4][16];
+            const double lam_k = lam_s[k];
+            const float en_k = en_s[k];
+            for (int cb = c_begin; cb < c_begin + CW; cb += 16 * kLdChunks) {
+            const int nch = min(kLdChunks, (c_begin + CW - cb) >> 4);
+            float vv[kLdChunks][16];
             tmem_ld_chunks(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(m * N + cb), nch, vv);
             if (!stage) continue;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kLdChunks; ++q) {
                 if (q >= nch) continue;
                 const int c0 = cb + 16 * q;
                 const float (&v)[16] = vv[q];
@@ -641,23 +608,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         }
         tc_fence_after();
         if (!group_and(bar_id, GT, ok)) { ok = false; break; }
-        // the B buffer is free: find the next active tile and start its copy
-        if (gtid == 0) next_s[g] = find_active(tile + G * gridDim.x);
-        group_sync(bar_id, GT);
+        // the B buffer is free: start the next tile's copy
         const int next = next_s[g];
         if (use_pf && next < prm.ntiles) prefetch(next);
 
         // ---- epilogue 2: u rows to global (z contiguous across lanes)
         for (int m = 0; m < mt_count && epi; ++m) {
             const int z = m * 128 + lq * 32 + lane;
-            for (int cb = c_begin; cb < c_begin + HALF; cb += 64) {
-                const int nch = min(4, (c_begin + HALF - cb) >> 4);
-                float vv[4][16];
+            for (int cb = c_begin; cb < c_begin + CW; cb += 16 * kLdChunks) {
+                const int nch = min(kLdChunks, (c_begin + CW - cb) >> 4);
+                float vv[kLdChunks][16];
                 tmem_ld_chunks(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)((mt_count + m) * N + cb),
                                nch, vv);
                 if (z < n) {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
+                    for (int q = 0; q < kLdChunks; ++q) {
                         if (q >= nch) continue;
 #pragma unroll
                         for (int c = 0; c < 16; c += 2) {
@@ -675,7 +640,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     }
 
     if (!ok && gtid == 0 && prm.error) atomicExch(prm.error, 1);
-    cp_async_wait_all();   // no copy may land after the kernel leaves
+    // no copy may land after the kernel leaves
+    if (gtid == 0 && pf_pending) (void)mbar_wait(&bar_pf[g], pf_phase);
     // Drain on a time-out: give the copy or MMAs still in flight a bounded
     // chance to finish before the accumulator columns are released.
     if (gtid == 0 && !e_ok) (void)mbar_wait(&bar_e, 0);   // copy issued but not yet seen complete

@@ -402,7 +402,8 @@ def test_cfg4_batch_mixed_matches_fp64():
 # FP64 operators against the neighbour-table kernel, and mixed solves of a
 # small uneven batch against the FP64 solve.
 # ---------------------------------------------------------------------------
-COUPLING_KINDS = {0: "neighbour", 1: "halo_y8", 2: "halo_y4", 3: "separable", 4: "separable_z2"}
+COUPLING_KINDS = {0: "neighbour", 1: "halo_y8", 2: "halo_y4", 3: "separable", 4: "separable_z2",
+                  5: "separable_bulk", 6: "separable_bulk_z2"}
 
 
 @pytest.mark.parametrize("kind", sorted(COUPLING_KINDS))
@@ -652,3 +653,28 @@ def test_dcgs2_and_cgs2_arnoldi_agree(precision):
     assert d.max() <= (1e-9 if precision == "fp64" else 1e-8)
     it_d, it_c = out["dcgs2"].iterations, out["cgs2"].iterations
     assert np.abs(it_d - it_c).max() <= 2 + 0.1 * it_c.max(), (it_d, it_c)
+
+
+def test_streamed_arnoldi_reduction_agrees_with_register_form(monkeypatch):
+    """The FP32 DCGS2 reduction that streams the basis through shared memory
+    by bulk copies (the default where chunks allow it) and the
+    register-streamed form compute the same sums in another grouping: the
+    same converged intensities and about the same iteration counts."""
+    case, systems = cfg2_batch(n_solves=24, seed=3)
+    out = {}
+    for mode, name in (("registers", "registers"), (None, "bulk")):
+        if mode is None:
+            monkeypatch.delenv("MSC_ARNOLDI_REDUCE", raising=False)
+        else:
+            monkeypatch.setenv("MSC_ARNOLDI_REDUCE", mode)
+        plan = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed")
+        res = plan.solve()
+        assert plan.tuning_report()["arnoldi_reduce"] == name
+        plan.close()
+        assert (res.status == 0).all() and (res.residual <= 1e-10).all()
+        out[name] = res
+    ref = out["registers"]
+    for name in ("bulk",):
+        d = np.abs(out[name].intensities.cpu().numpy() - ref.intensities.cpu().numpy())
+        assert d.max() <= 1e-8, (name, d.max())
+        assert np.abs(out[name].iterations - ref.iterations).max() <= 2 + 0.1 * ref.iterations.max()
