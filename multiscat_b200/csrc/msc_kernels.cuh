@@ -718,18 +718,13 @@ struct SepTaps {
     const void *kappa;   // [n] complex (R)
 };
 
-// BULK = 1 stages the halo with bulk copies instead of loads and stores
-// through registers: the z range [z0, z0 + ZC) of a halo position is one
-// contiguous run of the row-major source, so each position with a row is
-// one cp.async.bulk (ZC elements, 256 bytes), all completing on one
-// mbarrier; positions without a row and the z tail past n are zeroed by
-// plain stores.  Needs 16-byte aligned runs: n even for FP32.  A wait that
-// times out sets *err and the block returns without writing.
-template <int HY, int BX, int ZC, typename R, int BULK = 0>
+// (Staging the halo by one bulk copy per halo position instead, on an
+// mbarrier, measured the same: 283 against 280 us on the 512-beam batch.)
+template <int HY, int BX, int ZC, typename R>
 __global__ void __launch_bounds__(BX * ZC, HY <= 4 ? 3 : 1)
 k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps sep,
                const typename CT<R>::t *__restrict__ src, const typename CT<R>::t *__restrict__ in0,
-               R sgn, typename CT<R>::t *__restrict__ out, int *err = nullptr)
+               R sgn, typename CT<R>::t *__restrict__ out)
 {
     using C2 = typename CT<R>::t;
     constexpr int BY = 8;
@@ -782,42 +777,6 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
     }
     __syncthreads();
     const int total = npos * ZC;
-    if constexpr (BULK != 0) {
-        __shared__ __align__(8) uint64_t bar;
-        __shared__ int nvalid;
-        const int cnt = min(ZC, n - z0);
-        if (threadIdx.x == 0) {
-            mbar_init(&bar, 1);
-            mbar_fence_init();
-            nvalid = 0;
-        }
-        __syncthreads();
-        int mine = 0;
-        for (int pidx = threadIdx.x; pidx < npos; pidx += NT) mine += rows[pidx] >= 0;
-        if (mine) atomicAdd(&nvalid, mine);
-        for (int idx = threadIdx.x; idx < total; idx += NT) {
-            const int pidx = idx / ZC, zl = idx - pidx * ZC;
-            if (rows[pidx] < 0 || zl >= cnt) halo[idx] = mk2<R>(0, 0);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) mbar_expect_tx(&bar, (uint32_t)nvalid * (uint32_t)cnt * (uint32_t)sizeof(C2));
-        __syncthreads();
-        for (int pidx = threadIdx.x; pidx < npos; pidx += NT) {
-            const int row = rows[pidx];
-            if (row >= 0)
-                bulk_g2s(halo + (size_t)pidx * ZC, src + (size_t)row * n + z0,
-                         (uint32_t)cnt * (uint32_t)sizeof(C2), &bar);
-        }
-        const bool got = mbar_wait(&bar, 0);
-        if (!__syncthreads_and(got)) {
-            if (threadIdx.x == 0) {
-                if (err) atomicExch(err, 1);
-                (void)mbar_wait(&bar, 0);        // copies still in flight land before the exit
-            }
-            __syncthreads();
-            return;
-        }
-    } else {
     constexpr int kU = 8;
     if (std::is_same<R, float>::value && (n % 2) == 0) {
         const int total2 = total / 2;
@@ -860,7 +819,6 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
                 if (idx < total) halo[idx] = v[u];
             }
         }
-    }
     }
     __syncthreads();
 
@@ -906,6 +864,203 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
     for (int y = 0; y < BY; ++y) {
         if (rowv[y] < 0) continue;
         const C2 c = own[(size_t)(y + HY) * ZC];
+        R ar = -(kap.x * c.x - kap.y * c.y), ai = -(kap.x * c.y + kap.y * c.x);
+#pragma unroll
+        for (int sdy = -HY; sdy <= HY; ++sdy) {
+            const C2 q = qv[sdy + HY];
+            const R xr = tr[y - sdy + HY], xi = ti[y - sdy + HY];
+            ar = fma(q.x, xr, fma(-q.y, xi, ar));
+            ai = fma(q.x, xi, fma(q.y, xr, ai));
+        }
+        out[(size_t)rowv[y] * n + z] = mk2<R>(base[y].x + sgn * ar, base[y].y + sgn * ai);
+    }
+}
+
+// The separable coupling with the x pass run along the halo rows: one
+// thread per (halo row, z) holds the row's BX + 2 HX values in registers
+// and writes the BX values of t over the row's middle columns; the y pass
+// then runs per (x, z) column as in k_coupling_sep.  Each halo value is read
+// from shared memory once by the x pass instead of by up to 2 HX + 1
+// threads: about half the shared-memory operations of k_coupling_sep, whose
+// x pass is bound by them.  With 2 HX >= BX the row's t values go to its
+// 2 HX outer columns (already read), so the patch's own values stay for
+// the kappa term; narrower windows write t over the patch columns and keep
+// the own values in registers.  The x reach HXT is a template parameter
+// (the row lives in registers); the plan runs this form only for windows
+// with hx = HXT.
+template <int HY, int BX, int ZC, typename R, int HXT>
+__global__ void __launch_bounds__(BX * ZC, HY <= 4 ? 3 : 1)
+k_coupling_sep_rows(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps sep,
+                    const typename CT<R>::t *__restrict__ src,
+                    const typename CT<R>::t *__restrict__ in0, R sgn,
+                    typename CT<R>::t *__restrict__ out)
+{
+    using C2 = typename CT<R>::t;
+    constexpr int BY = 8;
+    constexpr int HYW = BY + 2 * HY;
+    constexpr int WY = 2 * HY + 1;
+    constexpr int NT = BX * ZC;
+    constexpr int HX = HXT;
+    constexpr int HXW = BX + 2 * HX;
+    constexpr int WX = 2 * HX + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C2 *halo = reinterpret_cast<C2 *>(smem_raw);                       // [HXW][HYW][ZC]
+    C2 *pw = halo + (size_t)HXW * HYW * ZC;                            // [WX][ZC]
+    C2 *qw = pw + (size_t)WX * ZC;                                     // [WY][ZC]
+    C2 *kw = qw + (size_t)WY * ZC;                                     // [ZC]
+    int *rows = reinterpret_cast<int *>(kw + ZC);                      // [HXW][HYW]
+    __shared__ int colany[BX];
+
+    const int w = blockIdx.x;
+    const int s = ct.work[3 * w];
+    if (gate && gate[s] == 0) return;
+    const int x0 = ct.work[3 * w + 1], y0 = ct.work[3 * w + 2];
+    const int z0 = blockIdx.y * ZC;
+    const int nkx = ct.nkx, nky = ct.nky;
+    const int *pr = ct.pos_row + (size_t)s * nkx * nky;
+    const C2 *P = reinterpret_cast<const C2 *>(sep.p);
+    const C2 *Qv = reinterpret_cast<const C2 *>(sep.q);
+    const C2 *Kp = reinterpret_cast<const C2 *>(sep.kappa);
+    for (int i = threadIdx.x; i < (WX + WY + 1) * ZC; i += NT) {
+        const int row = i / ZC, z = z0 + (i % ZC);
+        C2 v = mk2<R>(0, 0);
+        if (z < n) v = row < WX ? P[(size_t)row * n + z]
+                     : row < WX + WY ? Qv[(size_t)(row - WX) * n + z] : Kp[z];
+        pw[i] = v;          // pw, qw and kw are consecutive
+    }
+    constexpr int npos = HXW * HYW;
+    for (int pidx = threadIdx.x; pidx < npos; pidx += NT) {
+        const int hy = pidx % HYW, hx = pidx / HYW;
+        int gx = (x0 + hx - HX) % nkx;
+        if (gx < 0) gx += nkx;
+        int gy = (y0 + hy - HY) % nky;
+        if (gy < 0) gy += nky;
+        rows[pidx] = pr[gx * nky + gy];
+    }
+    if (threadIdx.x < BX) {
+        const int gx = x0 + threadIdx.x;
+        int any = 0;
+        if (gx < nkx)
+            for (int y = 0; y < BY && !any; ++y) any = (y0 + y < nky) && pr[gx * nky + y0 + y] >= 0;
+        colany[threadIdx.x] = any;
+    }
+    __syncthreads();
+    constexpr int kU = 8;
+    constexpr int total = npos * ZC;
+    if (std::is_same<R, float>::value && (n % 2) == 0) {
+        constexpr int total2 = total / 2;
+        float4 *halo4 = reinterpret_cast<float4 *>(halo);
+        for (int base = threadIdx.x; base < total2; base += NT * kU) {
+            float4 v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (idx < total2) {
+                    const int row = rows[(2 * idx) / ZC];
+                    const int z = z0 + ((2 * idx) % ZC);
+                    if (row >= 0 && z < n)
+                        v[u] = *reinterpret_cast<const float4 *>(src + (size_t)row * n + z);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                if (idx < total2) halo4[idx] = v[u];
+            }
+        }
+    } else {
+        for (int base = threadIdx.x; base < total; base += NT * kU) {
+            C2 v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                v[u] = mk2<R>(0, 0);
+                if (idx < total) {
+                    const int row = rows[idx / ZC];
+                    const int z = z0 + (idx % ZC);
+                    if (row >= 0 && z < n) v[u] = src[(size_t)row * n + z];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int idx = base + u * NT;
+                if (idx < total) halo[idx] = v[u];
+            }
+        }
+    }
+    __syncthreads();
+
+    // t(x) goes to column tcol(x): the outer columns x < HX and
+    // HX + BX .. HX + BX + (BX - HX) - 1 when they are enough, else over
+    // the patch columns HX + x
+    constexpr bool kOuter = 2 * HX >= BX;
+    auto tcol = [](int x) { return kOuter ? (x < HX ? x : x + BX) : x + HX; };
+    const int zl = threadIdx.x % ZC;
+    const int tx = threadIdx.x / ZC;
+    const C2 *own = halo + (size_t)(tx + HX) * HYW * ZC + zl;
+    C2 cen[kOuter ? 1 : BY];
+    if constexpr (!kOuter) {
+        // the column's own values (kappa term), before the x pass overwrites them
+#pragma unroll
+        for (int y = 0; y < BY; ++y) cen[y] = own[(size_t)(y + HY) * ZC];
+        __syncthreads();
+    }
+
+    // x pass, one thread per halo row (hy, z): t(x, hy) = sum_sdx p_sdx
+    // src(x - sdx, hy) for the patch's BX columns, written to columns
+    // tcol(x) of the same row (no other thread touches that row)
+    for (int item = threadIdx.x; item < HYW * ZC; item += NT) {
+        const int hy = item / ZC, zr = item - hy * ZC;
+        C2 *rowp = halo + (size_t)hy * ZC + zr;          // element hx at rowp[hx * HYW * ZC]
+        C2 pv[WX], rv[HXW];
+#pragma unroll
+        for (int i = 0; i < WX; ++i) pv[i] = pw[i * ZC + zr];
+#pragma unroll
+        for (int i = 0; i < HXW; ++i) rv[i] = rowp[(size_t)i * HYW * ZC];
+#pragma unroll
+        for (int x = 0; x < BX; ++x) {
+            R ar = 0, ai = 0;
+#pragma unroll
+            for (int sdx = -HX; sdx <= HX; ++sdx) {
+                const C2 v = rv[x - sdx + HX];
+                const C2 q = pv[sdx + HX];
+                ar = fma(q.x, v.x, fma(-q.y, v.y, ar));
+                ai = fma(q.x, v.y, fma(q.y, v.x, ai));
+            }
+            rowp[(size_t)tcol(x) * HYW * ZC] = mk2<R>(ar, ai);
+        }
+    }
+    __syncthreads();
+
+    // y pass, one thread per patch column (x, z): out(y) = in0 + sgn
+    // [sum_sdy q_sdy t(x, y - sdy) - kappa src(x, y)]
+    const int z = z0 + zl;
+    if (x0 + tx >= nkx || z >= n || !colany[tx]) return;
+    const C2 *tcolp = halo + (size_t)tcol(tx) * HYW * ZC + zl;
+    R tr[HYW], ti[HYW];
+#pragma unroll
+    for (int i = 0; i < HYW; ++i) {
+        const C2 v = tcolp[(size_t)i * ZC];
+        tr[i] = v.x;
+        ti[i] = v.y;
+    }
+    C2 qv[WY];
+#pragma unroll
+    for (int i = 0; i < WY; ++i) qv[i] = qw[i * ZC + zl];
+    const C2 kap = kw[zl];
+    int rowv[BY];
+    C2 base[BY];
+#pragma unroll
+    for (int y = 0; y < BY; ++y)
+        rowv[y] = (y0 + y < nky) ? rows[(tx + HX) * HYW + y + HY] : -1;
+#pragma unroll
+    for (int y = 0; y < BY; ++y)
+        base[y] = (in0 && rowv[y] >= 0) ? in0[(size_t)rowv[y] * n + z] : mk2<R>(0, 0);
+#pragma unroll
+    for (int y = 0; y < BY; ++y) {
+        if (rowv[y] < 0) continue;
+        const C2 c = kOuter ? own[(size_t)(y + HY) * ZC] : cen[kOuter ? 0 : y];
         R ar = -(kap.x * c.x - kap.y * c.y), ai = -(kap.x * c.y + kap.y * c.x);
 #pragma unroll
         for (int sdy = -HY; sdy <= HY; ++sdy) {
@@ -1896,6 +2051,29 @@ k_dcgs_reduce_bulk(ArnoldiArgs a, const float2 *__restrict__ Q, int j, const flo
     }
 }
 
+// Per-system scalar work at the end of the update (one thread): the
+// provisional column j from ||v_{j+1}||, its rotation, the iteration count
+// and the stop rules.
+__device__ __noinline__ void dcgs_update_finish(GmresState &st, const DcgsState &ds, int s, int m, int j,
+                                                double rtol, int max_iter, double inner_rtol)
+{
+    const double vn2 = st.h2[(size_t)s * (m + 2)].x;
+    const double beta = sqrt(fmax(vn2, 0.0));
+    double2 *col = ds.Hraw + (size_t)s * (m + 1) * m + (size_t)j * (m + 1);
+    col[j + 1] = make_double2(beta, 0.0);
+    ds.gsave[s] = st.g[(size_t)s * (m + 1) + j];
+    const double est = dcgs_rotate_column(st, ds, s, m, j);
+    st.est[s] = est;
+    st.kcyc[s] = j + 1;
+    st.iters[s] += 1;
+    st.projv[s] += j + 1;
+    bool stop = dcgs_stop(st, s, est, rtol, inner_rtol) || !isfinite(beta);
+    if (j + 1 >= m) stop = true;
+    if (st.iters[s] >= max_iter) stop = true;
+    if (beta <= 1e-300) stop = true;
+    if (stop) st.active[s] = 0;
+}
+
 // Update pass of step j over row chunks: slot j <- q_j, slot j + 1 <- v_{j+1}
 // (one read of q_0 .. q_{j-1}, v, w; two writes), ||v_{j+1}||^2 reduced per
 // system; the last block forms the provisional column j and its rotation,
@@ -1992,23 +2170,137 @@ k_dcgs_update(ArnoldiArgs a, typename CT<R>::t *__restrict__ Q, int j,
         a.partial[(size_t)blk * a.pstride] = make_double2(t, 0.0);
     }
     if (last_block_reduce(a, s, 1, st.h2 + (size_t)s * (m + 2))) {
-        if (threadIdx.x == 0) {
-            const double vn2 = st.h2[(size_t)s * (m + 2)].x;
-            const double beta = sqrt(fmax(vn2, 0.0));
-            double2 *col = ds.Hraw + (size_t)s * (m + 1) * m + (size_t)j * (m + 1);
-            col[j + 1] = make_double2(beta, 0.0);
-            ds.gsave[s] = st.g[(size_t)s * (m + 1) + j];
-            const double est = dcgs_rotate_column(st, ds, s, m, j);
-            st.est[s] = est;
-            st.kcyc[s] = j + 1;
-            st.iters[s] += 1;
-            st.projv[s] += j + 1;
-            bool stop = dcgs_stop(st, s, est, rtol, inner_rtol) || !isfinite(beta);
-            if (j + 1 >= m) stop = true;
-            if (st.iters[s] >= max_iter) stop = true;
-            if (beta <= 1e-300) stop = true;
-            if (stop) st.active[s] = 0;
+        if (threadIdx.x == 0) dcgs_update_finish(st, ds, s, m, j, rtol, max_iter, inner_rtol);
+    }
+}
+
+// Update pass of step j with the basis streamed through shared memory
+// (FP32 Krylov vectors; the chunks and stages of k_dcgs_reduce_bulk).
+// Thread t forms q_j and v_{j+1} of its element pairs t, t + 256, ... in
+// registers from v and w, then adds a_i q_i and b_i q_i as q_0 .. q_{j-1}
+// arrive; the arithmetic, ||v_{j+1}||^2 and the last block's work are those
+// of k_dcgs_update.  A wait that times out sets *err; the block then writes
+// nothing, waits (bounded) for its copies in flight and still takes part
+// in the per-system arrival count.
+__global__ void __launch_bounds__(256, 2)
+k_dcgs_update_bulk(ArnoldiArgs a, float2 *__restrict__ Q, int j, const float2 *__restrict__ W,
+                   GmresState st, DcgsState ds, int m, double rtol, int max_iter,
+                   double inner_rtol, int *err)
+{
+    constexpr int NT = 256;
+    constexpr int UP = kBulkChunk / (2 * NT);
+    constexpr int SP = kBulkChunk / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4 *ring = reinterpret_cast<float4 *>(smem_raw);
+    __shared__ __align__(8) uint64_t full[kBulkStages];
+    __shared__ float2 ca[kMaxRestart], cb[kMaxRestart];
+    __shared__ double wsum[NT / 32];
+    const int blk = blockIdx.x;
+    const int s = a.tiles.sys[blk];
+    if (a.gate && a.gate[s] == 0) return;
+    const double2 *cf = ds.coef + (size_t)s * ds.cstride;
+    for (int i = threadIdx.x; i < j; i += NT) {
+        ca[i] = make_float2((float)cf[i].x, (float)cf[i].y);
+        cb[i] = make_float2((float)cf[j + 1 + i].x, (float)cf[j + 1 + i].y);
+    }
+    const float inu = (float)cf[2 * m + 2].x;
+    const float2 dv = make_float2((float)cf[2 * m + 3].x, (float)cf[2 * m + 3].y);
+    size_t e0;
+    int ne;
+    elem_range<float>(a, blk, 0, e0, ne);
+    const int np = ne >> 1;
+    const uint32_t bytes = (uint32_t)ne * 8u;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < kBulkStages; ++q) mbar_init(&full[q], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int issued = 0;
+    if (threadIdx.x == 0) {
+        for (; issued < min(kBulkStages, j); ++issued) {
+            mbar_expect_tx(&full[issued], bytes);
+            bulk_g2s(ring + (size_t)issued * SP, Q + (size_t)issued * a.qstride + e0, bytes,
+                     &full[issued]);
         }
+    }
+    float4 *vq = reinterpret_cast<float4 *>(Q + (size_t)j * a.qstride + e0);        // v in, q_j out
+    float4 *vn = reinterpret_cast<float4 *>(Q + (size_t)(j + 1) * a.qstride + e0);  // v_{j+1} out
+    const float4 *wp = reinterpret_cast<const float4 *>(W + e0);
+    // q = v / nu ; n = w / nu + dv v   (two elements per float4)
+    float4 qa[UP], na[UP];
+#pragma unroll
+    for (int u = 0; u < UP; ++u) {
+        const int p = threadIdx.x + u * NT;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f), w = v;
+        if (p < np) {
+            v = vq[p];
+            w = wp[p];
+        }
+        qa[u] = make_float4(v.x * inu, v.y * inu, v.z * inu, v.w * inu);
+        na[u] = make_float4(w.x * inu + (dv.x * v.x - dv.y * v.y), w.y * inu + (dv.x * v.y + dv.y * v.x),
+                            w.z * inu + (dv.x * v.z - dv.y * v.w), w.w * inu + (dv.x * v.w + dv.y * v.z));
+    }
+    bool ok = true;
+    int i = 0;
+    for (; i < j; ++i) {
+        const int stg = i % kBulkStages;
+        const bool got = mbar_wait(&full[stg], (uint32_t)(i / kBulkStages) & 1u);
+        const float4 *qs = ring + (size_t)stg * SP;
+        const float2 x = ca[i], y = cb[i];
+#pragma unroll
+        for (int u = 0; u < UP; ++u) {
+            const int p = threadIdx.x + u * NT;
+            const float4 b = (got && p < np) ? qs[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 &q = qa[u];
+            float4 &nn = na[u];
+            q.x = fmaf(b.x, x.x, fmaf(-b.y, x.y, q.x));
+            q.y = fmaf(b.x, x.y, fmaf(b.y, x.x, q.y));
+            q.z = fmaf(b.z, x.x, fmaf(-b.w, x.y, q.z));
+            q.w = fmaf(b.z, x.y, fmaf(b.w, x.x, q.w));
+            nn.x = fmaf(b.x, y.x, fmaf(-b.y, y.y, nn.x));
+            nn.y = fmaf(b.x, y.y, fmaf(b.y, y.x, nn.y));
+            nn.z = fmaf(b.z, y.x, fmaf(-b.w, y.y, nn.z));
+            nn.w = fmaf(b.z, y.y, fmaf(b.w, y.x, nn.w));
+        }
+        if (!__syncthreads_and(got)) {
+            ok = false;
+            break;
+        }
+        if (threadIdx.x == 0 && issued < j) {
+            fence_proxy_async();
+            mbar_expect_tx(&full[stg], bytes);
+            bulk_g2s(ring + (size_t)stg * SP, Q + (size_t)issued * a.qstride + e0, bytes, &full[stg]);
+            ++issued;
+        }
+    }
+    double nrm = 0.0;
+    if (ok) {
+#pragma unroll
+        for (int u = 0; u < UP; ++u) {
+            const int p = threadIdx.x + u * NT;
+            if (p < np) {
+                vq[p] = qa[u];
+                vn[p] = na[u];
+                const float4 nn = na[u];
+                nrm += (double)nn.x * nn.x + (double)nn.y * nn.y + (double)nn.z * nn.z +
+                       (double)nn.w * nn.w;
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        if (err) atomicExch(err, 1);
+        for (int q = i; q < issued; ++q)
+            (void)mbar_wait(&full[q % kBulkStages], (uint32_t)(q / kBulkStages) & 1u);
+    }
+    nrm = warp_sum(nrm);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = nrm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < NT / 32; ++w) t += wsum[w];
+        a.partial[(size_t)blk * a.pstride] = make_double2(t, 0.0);
+    }
+    if (last_block_reduce(a, s, 1, st.h2 + (size_t)s * (m + 2))) {
+        if (threadIdx.x == 0) dcgs_update_finish(st, ds, s, m, j, rtol, max_iter, inner_rtol);
     }
 }
 

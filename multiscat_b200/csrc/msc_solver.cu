@@ -177,7 +177,9 @@ struct msc_plan {
     bool gs_e64_smem = false, gs_e32_smem = false;   // E held in the sweep's shared memory
     DevBuf<int> gs_sys_lvl, gs_lvl_start, gs_lvl_rows, gs_low_ptr, gs_low_tap, gs_low_row;
     bool dcgs = true;              // DCGS2 (two basis passes per step); false: CGS2
-    bool bulk_reduce = false;      // FP32 DCGS2 reduction streams the basis by bulk copies
+    // FP32 DCGS2 passes streaming the basis by bulk copies: 2 reduction and
+    // update, 1 reduction only, 0 neither
+    int bulk_arnoldi = 0;
     DevBuf<int> wait_error;        // set by a kernel whose bounded wait timed out
     DevBuf<double> scale, bnorm, resid, est, beta0;
     // mixed form: FP32 copies of the operator data and the FP32 Krylov space
@@ -480,7 +482,7 @@ size_t sep_smem(int hx, int hy, int zc, size_t elem)
 
 template <int HY, int ZC, typename R>
 void launch_sep(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
-                C2<R> *out, cudaStream_t st, bool bulk = false)
+                C2<R> *out, cudaStream_t st)
 {
     msc::CouplingTiles ct{p->work.p, p->pos_map.p, p->tap_window.p, p->nwork, p->nkx, p->nky,
                           p->halo_hx, p->K};
@@ -491,33 +493,59 @@ void launch_sep(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0
     const msc::SepTaps sep{base, base + np, base + np + nq};
     dim3 grid(p->nwork, (p->n + ZC - 1) / ZC);
     const size_t sm = sep_smem(p->halo_hx, HY, ZC, sizeof(C2<R>));
-    if (bulk)
-        msc::k_coupling_sep<HY, kHaloBX, ZC, R, 1><<<grid, kHaloBX * ZC, sm, st>>>(
-            ct, gate, p->n, sep, src, in0, sgn, out, p->wait_error.p);
-    else
-        msc::k_coupling_sep<HY, kHaloBX, ZC, R><<<grid, kHaloBX * ZC, sm, st>>>(
-            ct, gate, p->n, sep, src, in0, sgn, out);
+    msc::k_coupling_sep<HY, kHaloBX, ZC, R><<<grid, kHaloBX * ZC, sm, st>>>(
+        ct, gate, p->n, sep, src, in0, sgn, out);
 }
 
-// The bulk-copy halo staging takes 16-byte aligned runs of ZC elements.
-template <typename R>
-bool sep_bulk_ok(const msc_plan *p, const void *src)
+// The row-wise separable kernel: square windows (hx = hy), x reach as a
+// template parameter.
+bool sep_rows_ok(const msc_plan *p)
 {
-    return p->sep_ok && (sizeof(C2<R>) == 16 || p->n % 2 == 0) &&
-           reinterpret_cast<uintptr_t>(src) % 16 == 0;
+    return p->sep_ok && p->halo_hx == p->halo_hy &&
+           (p->halo_hx == 1 || p->halo_hx == 2 || p->halo_hx == 4 || p->halo_hx == 8);
+}
+
+template <int H, typename R>
+void launch_sep_rows_h(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
+                       C2<R> *out, cudaStream_t st)
+{
+    constexpr int ZC = halo_zc<R>();
+    msc::CouplingTiles ct{p->work.p, p->pos_map.p, p->tap_window.p, p->nwork, p->nkx, p->nky,
+                          p->halo_hx, p->K};
+    const size_t np = (size_t)(2 * H + 1) * p->n, nq = (size_t)(2 * H + 1) * p->n;
+    const C2<R> *base = std::is_same<R, float>::value
+                            ? reinterpret_cast<const C2<R> *>(p->sep32.p)
+                            : reinterpret_cast<const C2<R> *>(p->sep64.p);
+    const msc::SepTaps sep{base, base + np, base + np + nq};
+    dim3 grid(p->nwork, (p->n + ZC - 1) / ZC);
+    msc::k_coupling_sep_rows<H, kHaloBX, ZC, R, H>
+        <<<grid, kHaloBX * ZC, sep_smem(H, H, ZC, sizeof(C2<R>)), st>>>(ct, gate, p->n, sep, src,
+                                                                        in0, sgn, out);
+}
+
+template <typename R>
+void launch_sep_rows(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
+                     C2<R> *out, cudaStream_t st)
+{
+    switch (p->halo_hx) {
+    case 1: launch_sep_rows_h<1, R>(p, gate, src, in0, sgn, out, st); return;
+    case 2: launch_sep_rows_h<2, R>(p, gate, src, in0, sgn, out, st); return;
+    case 4: launch_sep_rows_h<4, R>(p, gate, src, in0, sgn, out, st); return;
+    default: launch_sep_rows_h<8, R>(p, gate, src, in0, sgn, out, st); return;
+    }
 }
 
 // ZC: z values per block (the halo kernel's, or half of it: half the shared
 // memory, twice the resident blocks to hide the halo loads)
 template <int ZC, typename R>
 void launch_sep_hy(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0, R sgn,
-                   C2<R> *out, cudaStream_t st, bool bulk = false)
+                   C2<R> *out, cudaStream_t st)
 {
     switch (p->halo_hy) {
-    case 1: launch_sep<1, ZC, R>(p, gate, src, in0, sgn, out, st, bulk); return;
-    case 2: launch_sep<2, ZC, R>(p, gate, src, in0, sgn, out, st, bulk); return;
-    case 4: launch_sep<4, ZC, R>(p, gate, src, in0, sgn, out, st, bulk); return;
-    default: launch_sep<8, ZC, R>(p, gate, src, in0, sgn, out, st, bulk); return;
+    case 1: launch_sep<1, ZC, R>(p, gate, src, in0, sgn, out, st); return;
+    case 2: launch_sep<2, ZC, R>(p, gate, src, in0, sgn, out, st); return;
+    case 4: launch_sep<4, ZC, R>(p, gate, src, in0, sgn, out, st); return;
+    default: launch_sep<8, ZC, R>(p, gate, src, in0, sgn, out, st); return;
     }
 }
 
@@ -527,13 +555,12 @@ void launch_coupling_t(msc_plan *p, const int *gate, const C2<R> *src, const C2<
 {
     // coupling kind per precision: 0 neighbour table, 1 halo (8 y/thread), 2 halo (4 y/thread),
     // 3 separable (two 1-D passes; only when the tap windows factorise),
-    // 4 separable with half the z per block, 5 and 6 the same with the halo
-    // staged by bulk copies (where the source runs are 16-byte aligned)
+    // 4 separable with half the z per block, 5 separable with the x pass
+    // along the halo rows (square windows; otherwise the column form)
     const int kind = p->use_halo ? (std::is_same<R, float>::value ? p->halo32 : p->halo64) : 0;
-    if ((kind == 5 || kind == 6) && p->sep_ok) {
-        const bool bulk = sep_bulk_ok<R>(p, src);
-        if (kind == 5) launch_sep_hy<halo_zc<R>(), R>(p, gate, src, in0, sgn, out, st, bulk);
-        else launch_sep_hy<halo_zc<R>() / 2, R>(p, gate, src, in0, sgn, out, st, bulk);
+    if (kind == 5 && p->sep_ok) {
+        if (sep_rows_ok(p)) launch_sep_rows<R>(p, gate, src, in0, sgn, out, st);
+        else launch_sep_hy<halo_zc<R>(), R>(p, gate, src, in0, sgn, out, st);
         return;
     }
     if (kind == 1) { launch_halo_ys<8, R>(p, gate, src, in0, sgn, out, st); return; }
@@ -775,7 +802,7 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
             // candidate into slots j and j + 1 and runs the stop test.
             if (tm) mark(p, 2, j, 0, st);
             if constexpr (std::is_same<R, float>::value) {
-                if (p->bulk_reduce)
+                if (p->bulk_arnoldi > 0)
                     msc::k_dcgs_reduce_bulk<<<nblk1, 256, msc::dcgs_bulk_smem(), st>>>(
                         a1, Q, j, W, p->state(), p->dstate(), p->m, p->desc.rtol, inner,
                         p->wait_error.p);
@@ -789,9 +816,19 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
             }
             if (tm) mark(p, 2, j, 1, st);
             if (tm) mark(p, 3, j, 0, st);
-            msc::k_dcgs_update<R><<<nblk1, 256, 0, st>>>(a1, Q, j, W, p->state(), p->dstate(),
-                                                         p->m, p->desc.rtol,
-                                                         p->desc.max_iterations, inner);
+            bool updated = false;
+            if constexpr (std::is_same<R, float>::value) {
+                if (p->bulk_arnoldi > 1) {
+                    msc::k_dcgs_update_bulk<<<nblk1, 256, msc::dcgs_bulk_smem(), st>>>(
+                        a1, Q, j, W, p->state(), p->dstate(), p->m, p->desc.rtol,
+                        p->desc.max_iterations, inner, p->wait_error.p);
+                    updated = true;
+                }
+            }
+            if (!updated)
+                msc::k_dcgs_update<R><<<nblk1, 256, 0, st>>>(a1, Q, j, W, p->state(), p->dstate(),
+                                                             p->m, p->desc.rtol,
+                                                             p->desc.max_iterations, inner);
             if (tm) mark(p, 3, j, 1, st);
             continue;
         }
@@ -934,13 +971,16 @@ msc_status set_kernel_attributes(int n, int K)
                                   (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448))); \
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>() / 2, R>,          \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
-                                  (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>() / 2, sizeof(C2<R>)), 232448))); \
-    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>(), R, 1>,           \
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
-                                  (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448))); \
-    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>() / 2, R, 1>,       \
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
                                   (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>() / 2, sizeof(C2<R>)), 232448)));
+#define MSC_SEP_ROWS_ATTR(H, R)                                                                  \
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep_rows<H, kHaloBX, halo_zc<R>(), R, H>,      \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                  (int)std::min<size_t>(sep_smem(H, H, halo_zc<R>(), sizeof(C2<R>)), 232448)));
+    MSC_SEP_ROWS_ATTR(1, float) MSC_SEP_ROWS_ATTR(2, float)
+    MSC_SEP_ROWS_ATTR(4, float) MSC_SEP_ROWS_ATTR(8, float)
+    MSC_SEP_ROWS_ATTR(1, double) MSC_SEP_ROWS_ATTR(2, double)
+    MSC_SEP_ROWS_ATTR(4, double) MSC_SEP_ROWS_ATTR(8, double)
+#undef MSC_SEP_ROWS_ATTR
     MSC_SEP_ATTR(1, float)
     MSC_SEP_ATTR(2, float)
     MSC_SEP_ATTR(4, float)
@@ -1202,7 +1242,7 @@ bool tune_from_env(msc_plan *p)
     if (!env || !*env) return false;
     int c64 = p->halo64, c32 = p->halo32, bi = p->use_tc ? p->tc_n : 0, bg = 1;
     std::sscanf(env, "c64=%d,c32=%d,bi=%d,bg=%d", &c64, &c32, &bi, &bg);
-    const int kmax = p->sep_ok ? 6 : 2;
+    const int kmax = p->sep_ok ? 5 : 2;
     p->halo64 = p->use_halo ? std::max(0, std::min(kmax, c64)) : 0;
     p->halo32 = p->use_halo ? std::max(0, std::min(kmax, c32)) : 0;
     if (p->use_tc) {
@@ -1249,9 +1289,9 @@ msc_status autotune_measure(msc_plan *p)
     const size_t vs = (size_t)p->R * p->n;
     MSC_CUDA(cudaMemsetAsync(p->X.p, 0, vs * sizeof(double2), p->stream));
     MSC_CUDA(cudaMemsetAsync(p->TMP.p, 0, vs * sizeof(double2), p->stream));
-    const char *kind_name[7] = {"neighbour", "halo_y8", "halo_y4", "separable", "separable_z2",
-                                "separable_bulk", "separable_bulk_z2"};
-    const int nkinds = p->sep_ok ? 7 : 3;
+    const char *kind_name[6] = {"neighbour", "halo_y8", "halo_y4", "separable", "separable_z2",
+                                "separable_rows"};
+    const int nkinds = sep_rows_ok(p) ? 6 : p->sep_ok ? 5 : 3;
     if (p->use_halo) {
         float best = 0.f;
         int best_k = 0;
@@ -1638,14 +1678,21 @@ msc_status finalize(msc_plan *p)
         // the streamed reduction takes chunks of at most kBulkChunk elements
         // on 16-byte boundaries (n even: every chunk starts on an even element)
         const int max_rows = cn.empty() ? 0 : *std::max_element(cn.begin(), cn.end());
-        const char *rmode = std::getenv("MSC_ARNOLDI_REDUCE");
+        const char *rmode = std::getenv("MSC_ARNOLDI_STREAM");
         const bool bulk_ok = p->mixed && n % 2 == 0 && (long long)max_rows * n <= msc::kBulkChunk;
-        // (MSC_ARNOLDI_REDUCE=registers selects the register-streamed form)
-        p->bulk_reduce = bulk_ok && !(rmode && std::strcmp(rmode, "registers") == 0);
+        // (MSC_ARNOLDI_STREAM=registers selects the register-streamed passes,
+        // =reduce the streamed reduction with the register-streamed update)
+        p->bulk_arnoldi = bulk_ok ? 2 : 0;
+        if (bulk_ok && rmode && std::strcmp(rmode, "registers") == 0) p->bulk_arnoldi = 0;
+        if (bulk_ok && rmode && std::strcmp(rmode, "reduce") == 0) p->bulk_arnoldi = 1;
         MSC_CUDA(p->wait_error.alloc(1));
         MSC_CUDA(cudaMemset(p->wait_error.p, 0, sizeof(int)));
-        if (p->bulk_reduce)
+        if (p->bulk_arnoldi > 0)
             MSC_CUDA(cudaFuncSetAttribute(msc::k_dcgs_reduce_bulk,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)msc::dcgs_bulk_smem()));
+        if (p->bulk_arnoldi > 1)
+            MSC_CUDA(cudaFuncSetAttribute(msc::k_dcgs_update_bulk,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)msc::dcgs_bulk_smem()));
         MSC_CUDA(upload(p->chunk_row0, c0));
@@ -2274,7 +2321,7 @@ msc_status msc_solve(msc_plan *p, double *psi_out, double *intensities_out, msc_
     {
         int w_err = 0;
         MSC_CUDA(cudaMemcpy(&w_err, p->wait_error.p, sizeof(int), cudaMemcpyDeviceToHost));
-        if (w_err) return fail(MSC_ERR_CUDA, "a bulk-copy wait (Arnoldi reduction or coupling halo) timed out");
+        if (w_err) return fail(MSC_ERR_CUDA, "a bulk-copy wait of the streamed Arnoldi passes timed out");
     }
     std::vector<int> iters(p->B), cycles(p->B), status(p->B), unfinished(p->B), fallback(p->B, 0);
     std::vector<int> projv(p->B);
@@ -2466,14 +2513,14 @@ const char *msc_plan_tuning_report(msc_plan *p)
         r += "\"" + p->tune_log[i].first + "\": " + std::to_string(p->tune_log[i].second);
     }
     if (!r.empty() && r.size() > 1) r += ", ";
-    const char *kn[7] = {"neighbour", "halo_y8", "halo_y4", "separable", "separable_z2",
-                         "separable_bulk", "separable_bulk_z2"};
+    const char *kn[6] = {"neighbour", "halo_y8", "halo_y4", "separable", "separable_z2",
+                         "separable_rows"};
     r += "\"halo_hx\": " + std::to_string(p->use_halo ? p->halo_hx : 0) + ", \"halo_hy\": " +
          std::to_string(p->use_halo ? p->halo_hy : 0) + ", ";
     r += "\"chosen\": \"coupling64=" + std::string(p->use_halo ? kn[p->halo64] : kn[0]) +
          ",coupling32=" + std::string(p->use_halo ? kn[p->halo32] : kn[0]) +
          ",block_inverse32=" + (p->use_tc ? std::string(p->tc_groups == 2 ? "tc2_N" : "tc_N") + std::to_string(p->tc_n) : std::string("simt")) +
-         "\", \"arnoldi_reduce\": \"" + (p->mixed && p->dcgs ? (p->bulk_reduce ? "bulk" : "registers") : "registers") +
+         "\", \"arnoldi_stream\": \"" + (p->mixed && p->dcgs && p->bulk_arnoldi > 0 ? (p->bulk_arnoldi > 1 ? "bulk" : "bulk_reduce") : "registers") +
          "\"}";
     p->tune_report = r;
     return p->tune_report.c_str();

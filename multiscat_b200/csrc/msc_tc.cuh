@@ -255,6 +255,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     __shared__ float sm_part[G][4][2][N];     // Sherman-Morrison partial sums [group][lane quarter][M tile][col]
     __shared__ float2 beta_s[G][TR];
     __shared__ double pkd_s[G][TR];
+    __shared__ double2 rc_s[G][TR];            // the tile's boundary constants c_j and fn_j,
+    __shared__ double fn_s[G][TR];             // loaded with pkd while the tile is staged
     __shared__ double lam_s[256];             // eigenvalues of H0 (k < n <= 256), 0 past n
     __shared__ float en_s[256];               // last components E[n-1, k] (FP32), 0 past n
 
@@ -382,7 +384,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     while (tile < prm.ntiles && ok) {
         const int row0 = tile * TR;
         const int nrow = min(TR, prm.rows - row0);
-        for (int j = gtid; j < TR; j += GT) pkd_s[g][j] = (j < nrow) ? prm.row_pkd[row0 + j] : 0.0;
+        for (int j = gtid; j < TR; j += GT) {
+            const bool in = j < nrow;
+            pkd_s[g][j] = in ? prm.row_pkd[row0 + j] : 0.0;
+            rc_s[g][j] = in ? prm.row_c[row0 + j] : make_double2(0.0, 0.0);
+            fn_s[g][j] = in ? prm.row_fn[row0 + j] : 0.0;
+        }
 
         // ---- stage x as the B operand of GEMM 1 (K-major: rows = 2 TR re/im
         // columns, K = z)
@@ -520,8 +527,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                         sr += sm_part[g][w][m][2 * j];
                         si += sm_part[g][w][m][2 * j + 1];
                     }
-                const double2 c = prm.row_c[row0 + j];
-                const double fn = prm.row_fn[row0 + j];
+                const double2 c = rc_s[g][j];
+                const double fn = fn_s[g][j];
                 b = cdiv(cmul(c, make_double2(sr, si)), make_double2(1.0 - c.x * fn, -c.y * fn));
             }
             beta_s[g][j] = make_float2((float)b.x, (float)b.y);

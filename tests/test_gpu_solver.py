@@ -403,7 +403,7 @@ def test_cfg4_batch_mixed_matches_fp64():
 # small uneven batch against the FP64 solve.
 # ---------------------------------------------------------------------------
 COUPLING_KINDS = {0: "neighbour", 1: "halo_y8", 2: "halo_y4", 3: "separable", 4: "separable_z2",
-                  5: "separable_bulk", 6: "separable_bulk_z2"}
+                  5: "separable_rows"}
 
 
 @pytest.mark.parametrize("kind", sorted(COUPLING_KINDS))
@@ -655,26 +655,27 @@ def test_dcgs2_and_cgs2_arnoldi_agree(precision):
     assert np.abs(it_d - it_c).max() <= 2 + 0.1 * it_c.max(), (it_d, it_c)
 
 
-def test_streamed_arnoldi_reduction_agrees_with_register_form(monkeypatch):
-    """The FP32 DCGS2 reduction that streams the basis through shared memory
-    by bulk copies (the default where chunks allow it) and the
-    register-streamed form compute the same sums in another grouping: the
-    same converged intensities and about the same iteration counts."""
+def test_streamed_arnoldi_passes_agree_with_register_form(monkeypatch):
+    """The FP32 DCGS2 reduction and update that stream the basis through
+    shared memory by bulk copies (the default where chunks allow it; the
+    reduction alone, or both) and the register-streamed passes compute the
+    same sums in another grouping: the same converged intensities and about
+    the same iteration counts."""
     case, systems = cfg2_batch(n_solves=24, seed=3)
     out = {}
-    for mode, name in (("registers", "registers"), (None, "bulk")):
+    for mode, name in (("registers", "registers"), ("reduce", "bulk_reduce"), (None, "bulk")):
         if mode is None:
-            monkeypatch.delenv("MSC_ARNOLDI_REDUCE", raising=False)
+            monkeypatch.delenv("MSC_ARNOLDI_STREAM", raising=False)
         else:
-            monkeypatch.setenv("MSC_ARNOLDI_REDUCE", mode)
+            monkeypatch.setenv("MSC_ARNOLDI_STREAM", mode)
         plan = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed")
         res = plan.solve()
-        assert plan.tuning_report()["arnoldi_reduce"] == name
+        assert plan.tuning_report()["arnoldi_stream"] == name
         plan.close()
         assert (res.status == 0).all() and (res.residual <= 1e-10).all()
         out[name] = res
     ref = out["registers"]
-    for name in ("bulk",):
+    for name in ("bulk_reduce", "bulk"):
         d = np.abs(out[name].intensities.cpu().numpy() - ref.intensities.cpu().numpy())
         assert d.max() <= 1e-8, (name, d.max())
         assert np.abs(out[name].iterations - ref.iterations).max() <= 2 + 0.1 * ref.iterations.max()
