@@ -550,11 +550,9 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
     C2 *halo = reinterpret_cast<C2 *>(smem_raw);                              // [HXW][HYW][ZC]
     C2 *vw = halo + (size_t)HXW * HYW * ZC;                                   // [window cell][ZC]
     int *rows = reinterpret_cast<int *>(vw + (size_t)nwin * ZC);              // [HXW][HYW]
-    // segany[seg][x]: does y segment seg (YS positions) of patch column x hold
-    // a channel?  Threads of empty segments skip the tap loop (truncated
-    // channel sets leave many near the edge of the channel disk).
-    constexpr int NSEG = BY / YS;
-    __shared__ int segany[NSEG * BX];
+    // Threads whose y segment (YS positions) of their patch column holds no
+    // channel skip the tap loop (truncated channel sets leave many near the
+    // edge of the channel disk); the test reads the staged rows table.
 
     const int w = blockIdx.x;
     const int s = ct.work[3 * w];
@@ -578,15 +576,6 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
         int gy = (y0 + hy - HY) % nky;
         if (gy < 0) gy += nky;
         rows[pidx] = pr[gx * nky + gy];
-    }
-    if (threadIdx.x < NSEG * BX) {
-        const int cx = threadIdx.x % BX, seg = threadIdx.x / BX;
-        const int gx = x0 + cx;
-        int any = 0;
-        if (gx < nkx)
-            for (int y = seg * YS; y < (seg + 1) * YS && !any; ++y)
-                any = (y0 + y < nky) && pr[gx * nky + y0 + y] >= 0;
-        segany[threadIdx.x] = any;
     }
     __syncthreads();
     constexpr int kU = 8;
@@ -640,7 +629,11 @@ k_coupling_halo(CouplingTiles ct, const int *__restrict__ gate, int n,
     const int tx = (threadIdx.x / ZC) % BX;
     const int ysub = threadIdx.x / (ZC * BX);      // which YS-slice of the 8 y outputs
     const int z = z0 + zl;
-    if (x0 + tx >= nkx || z >= n || !segany[ysub * BX + tx]) return;
+    bool any = false;
+#pragma unroll
+    for (int y = ysub * YS; y < (ysub + 1) * YS; ++y)
+        any |= (y0 + y < nky) && rows[(tx + HX) * HYW + y + HY] >= 0;
+    if (x0 + tx >= nkx || z >= n || !any) return;
     R ar[YS], ai[YS];
 #pragma unroll
     for (int y = 0; y < YS; ++y) {
@@ -740,7 +733,6 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
     C2 *qw = pw + (size_t)WX * ZC;                                     // [WY][ZC]
     C2 *kw = qw + (size_t)WY * ZC;                                     // [ZC]
     int *rows = reinterpret_cast<int *>(kw + ZC);                      // [HXW][HYW]
-    __shared__ int colany[BX];
 
     const int w = blockIdx.x;
     const int s = ct.work[3 * w];
@@ -767,13 +759,6 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
         int gy = (y0 + hy - HY) % nky;
         if (gy < 0) gy += nky;
         rows[pidx] = pr[gx * nky + gy];
-    }
-    if (threadIdx.x < BX) {
-        const int gx = x0 + threadIdx.x;
-        int any = 0;
-        if (gx < nkx)
-            for (int y = 0; y < BY && !any; ++y) any = (y0 + y < nky) && pr[gx * nky + y0 + y] >= 0;
-        colany[threadIdx.x] = any;
     }
     __syncthreads();
     const int total = npos * ZC;
@@ -825,7 +810,10 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
     const int zl = threadIdx.x % ZC;
     const int tx = threadIdx.x / ZC;
     const int z = z0 + zl;
-    if (x0 + tx >= nkx || z >= n || !colany[tx]) return;
+    bool any = false;       // a channel in this patch column (staged rows table)
+#pragma unroll
+    for (int y = 0; y < BY; ++y) any |= (y0 + y < nky) && rows[(tx + HX) * HYW + y + HY] >= 0;
+    if (x0 + tx >= nkx || z >= n || !any) return;
     // pass 1: t(hy) = sum_sdx p_sdx halo(tx - sdx + HX, hy) over the halo column
     R tr[HYW], ti[HYW];
 #pragma unroll
@@ -909,7 +897,6 @@ k_coupling_sep_rows(CouplingTiles ct, const int *__restrict__ gate, int n, SepTa
     C2 *qw = pw + (size_t)WX * ZC;                                     // [WY][ZC]
     C2 *kw = qw + (size_t)WY * ZC;                                     // [ZC]
     int *rows = reinterpret_cast<int *>(kw + ZC);                      // [HXW][HYW]
-    __shared__ int colany[BX];
 
     const int w = blockIdx.x;
     const int s = ct.work[3 * w];
@@ -936,13 +923,6 @@ k_coupling_sep_rows(CouplingTiles ct, const int *__restrict__ gate, int n, SepTa
         int gy = (y0 + hy - HY) % nky;
         if (gy < 0) gy += nky;
         rows[pidx] = pr[gx * nky + gy];
-    }
-    if (threadIdx.x < BX) {
-        const int gx = x0 + threadIdx.x;
-        int any = 0;
-        if (gx < nkx)
-            for (int y = 0; y < BY && !any; ++y) any = (y0 + y < nky) && pr[gx * nky + y0 + y] >= 0;
-        colany[threadIdx.x] = any;
     }
     __syncthreads();
     constexpr int kU = 8;
@@ -1036,7 +1016,10 @@ k_coupling_sep_rows(CouplingTiles ct, const int *__restrict__ gate, int n, SepTa
     // y pass, one thread per patch column (x, z): out(y) = in0 + sgn
     // [sum_sdy q_sdy t(x, y - sdy) - kappa src(x, y)]
     const int z = z0 + zl;
-    if (x0 + tx >= nkx || z >= n || !colany[tx]) return;
+    bool any = false;       // a channel in this patch column (staged rows table)
+#pragma unroll
+    for (int y = 0; y < BY; ++y) any |= (y0 + y < nky) && rows[(tx + HX) * HYW + y + HY] >= 0;
+    if (x0 + tx >= nkx || z >= n || !any) return;
     const C2 *tcolp = halo + (size_t)tcol(tx) * HYW * ZC + zl;
     R tr[HYW], ti[HYW];
 #pragma unroll

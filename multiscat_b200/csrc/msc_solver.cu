@@ -37,6 +37,7 @@
 #include "msc_eigh_gpu.cuh"
 #include "msc_kernels.cuh"
 #include "msc_tc.cuh"
+#include "msc_tcc.cuh"
 
 namespace {
 
@@ -196,9 +197,12 @@ struct msc_plan {
     // tcgen05 block inverse (mixed form)
     bool use_tc = false;
     int tc_n = 0, tc_tile_rows = 0, tc_ntiles = 0, tc_grid = 0;
-    int tc_groups = 1;          // warp groups with their own tile loop (1 or 2)
+    int tc_groups = 1;          // warp groups with their own tile loop (1 or 2), or
+                                // kTcChannelMajor: k_block_inverse_tcc
     int tc2_max = 0;            // widest N the two-group kernel may take (0: none)
     size_t tc_smem = 0, tc2_smem = 0;
+    bool tcc_ok = false;        // the channel-major kernel fits (E and one A buffer)
+    size_t tcc_smem = 0;
     DevBuf<__nv_bfloat16> e_img;
     DevBuf<int> tc_error;
     DevBuf<int> active, kcyc, iters, projv, cycles, unfinished, status, counter;
@@ -361,6 +365,9 @@ using C2 = typename msc::CT<R>::t;
 template <typename R>
 size_t smem_block_inverse_t(int n) { return (size_t)2 * n * 2 * block_inverse_rows(n) * sizeof(R); }
 
+// tc_groups code of the channel-major tcgen05 kernel (k_block_inverse_tcc)
+constexpr int kTcChannelMajor = 3;
+
 void launch_block_inverse_tc(msc_plan *p, const int *gate, const float2 *x, float2 *out,
                              cudaStream_t st)
 {
@@ -384,6 +391,10 @@ void launch_block_inverse_tc(msc_plan *p, const int *gate, const float2 *x, floa
     prm.error = p->tc_error.p;
     using msc::tc::k_block_inverse_tc;
     constexpr int T = msc::tc::kThreads;
+    if (p->tc_groups == kTcChannelMajor) {
+        msc::tc::k_block_inverse_tcc<<<p->tc_grid, T, p->tcc_smem, st>>>(prm);
+        return;
+    }
     if (p->tc_groups == 2) {
         const size_t sm = p->tc2_smem;
         switch (p->tc_n) {
@@ -1157,6 +1168,21 @@ msc_status setup_tensor_core(msc_plan *p)
             if (e != cudaSuccess) return fail(MSC_ERR_CUDA, std::string("tc smem attribute: ") + cudaGetErrorString(e));
         }
     }
+    // channel-major kernel: E_hi, E_lo and one A buffer of 128 rows x kp
+    {
+        const size_t kpc = (size_t)(n + 15) / 16 * 16;
+        cudaFuncAttributes fa{};
+        p->tcc_smem = 4 * kpc * kpc + 512 * kpc + 1024;
+        p->tcc_ok = kpc <= 256 &&
+                    cudaFuncGetAttributes(&fa, msc::tc::k_block_inverse_tcc) == cudaSuccess &&
+                    p->tcc_smem + fa.sharedSizeBytes <= (size_t)optin;
+        if (p->tcc_ok) {
+            cudaError_t e = cudaFuncSetAttribute(msc::tc::k_block_inverse_tcc,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)p->tcc_smem);
+            if (e != cudaSuccess) return fail(MSC_ERR_CUDA, std::string("tcc smem attribute: ") + cudaGetErrorString(e));
+        }
+    }
     // E image: [hi|lo][z/8][k/8][z%8][k%8], zero padded to kp x kp
     const int kp = (n + 15) / 16 * 16, kb = kp / 8;
     std::vector<__nv_bfloat16> img((size_t)2 * kp * kp, __float2bfloat16(0.f));
@@ -1221,6 +1247,18 @@ void apply_tc_width(msc_plan *p, int N, int G = 1)
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (G == kTcChannelMajor) {
+        if (p->tcc_ok) {
+            p->tc_n = 128;                 // M rows: 64 channels
+            p->tc_groups = G;
+            p->tc_tile_rows = 64;
+            p->tc_ntiles = (p->R + 63) / 64;
+            p->tc_grid = std::min(p->tc_ntiles, sms);
+            return;
+        }
+        G = 1;
+        N = std::min(N, 128);
+    }
     if (G == 2 && N > p->tc2_max) G = 1;
     p->tc_n = N;
     p->tc_groups = G;
@@ -1251,7 +1289,7 @@ bool tune_from_env(msc_plan *p)
         } else {
             int N = 16;
             while (N < bi && N < p->tc_n) N *= 2;
-            apply_tc_width(p, N, bg == 2 ? 2 : 1);
+            apply_tc_width(p, N, (bg == 2 || bg == kTcChannelMajor) ? bg : 1);
         }
     }
     p->tune_log.push_back({"from_MSC_TUNE", 1.f});
@@ -1338,6 +1376,9 @@ msc_status autotune_measure(msc_plan *p)
             });
             p->tune_log.push_back({"block_inverse32_simt_us", t_simt});
             p->use_tc = true;
+            // (the channel-major form, MSC_TUNE bg=3, is left out: 243 against
+            // 250 us per full-batch launch on the 512-beam cfg2 batch, but the
+            // batch was not faster end to end with it)
             for (int G = 1; G <= 2; ++G)
                 for (int N = 16; N <= (G == 1 ? best_n0 : p->tc2_max); N *= 2) {
                     apply_tc_width(p, N, G);
@@ -2519,7 +2560,9 @@ const char *msc_plan_tuning_report(msc_plan *p)
          std::to_string(p->use_halo ? p->halo_hy : 0) + ", ";
     r += "\"chosen\": \"coupling64=" + std::string(p->use_halo ? kn[p->halo64] : kn[0]) +
          ",coupling32=" + std::string(p->use_halo ? kn[p->halo32] : kn[0]) +
-         ",block_inverse32=" + (p->use_tc ? std::string(p->tc_groups == 2 ? "tc2_N" : "tc_N") + std::to_string(p->tc_n) : std::string("simt")) +
+         ",block_inverse32=" + (!p->use_tc ? std::string("simt")
+                                : p->tc_groups == kTcChannelMajor ? std::string("tcc")
+                                : std::string(p->tc_groups == 2 ? "tc2_N" : "tc_N") + std::to_string(p->tc_n)) +
          "\", \"arnoldi_stream\": \"" + (p->mixed && p->dcgs && p->bulk_arnoldi > 0 ? (p->bulk_arnoldi > 1 ? "bulk" : "bulk_reduce") : "registers") +
          "\"}";
     p->tune_report = r;

@@ -343,11 +343,12 @@ def test_mixed_odd_node_count_matches_fp64():
 
 
 @pytest.mark.parametrize("groups,width", [(1, 16), (1, 32), (1, 64), (1, 128),
-                                          (2, 16), (2, 32), (2, 64)])
+                                          (2, 16), (2, 32), (2, 64), (3, 128)])
 def test_tensor_core_width_and_warp_groups_match_simt(groups, width, monkeypatch):
     """Every tcgen05 variant the autotuner can pick (tile width N; one tile
-    loop per CTA or two warp groups with their own), forced through MSC_TUNE,
-    on a 24-beam batch with enough rows for every width."""
+    loop per CTA, two warp groups with their own, or the channel-major
+    kernel, bg=3), forced through MSC_TUNE, on a 24-beam batch with enough
+    rows for every width."""
     case, systems = cfg2_batch(n_solves=24, seed=3)
     rng = np.random.default_rng(19)
     # a plan reads MSC_TUNE when its first call sets it up
@@ -361,7 +362,7 @@ def test_tensor_core_width_and_warp_groups_match_simt(groups, width, monkeypatch
     simt = ScatteringPlan(case.v, case.t, systems, precision="mixed", tensor_cores=False)
     y_simt = simt.apply_block_inverse_f32(x32).cpu().numpy()
     assert mixed.tensor_core_tile == width
-    tag = ("tc2_N" if groups == 2 else "tc_N") + str(width)
+    tag = "tcc" if groups == 3 else ("tc2_N" if groups == 2 else "tc_N") + str(width)
     assert f"block_inverse32={tag}" in mixed.tuning_report()["chosen"]
     scale = np.abs(y_simt).max()
     np.testing.assert_allclose(y_tc, y_simt, rtol=0, atol=TC_TOL * scale)
@@ -522,7 +523,7 @@ for tc in (True, False):
         assert (r.status == 0).all(), (tc, order, r.status)
         worst = max(worst, float((r.intensities - ref).abs().max()))
 import os
-for bg in (1, 2):          # both tcgen05 kernel forms, forced
+for bg in (1, 2, 3):       # every tcgen05 kernel form, forced
     os.environ["MSC_TUNE"] = f"c64=2,c32=2,bi=16,bg={bg}"
     r = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed",
                        tensor_cores=True).solve()
@@ -679,3 +680,32 @@ def test_streamed_arnoldi_passes_agree_with_register_form(monkeypatch):
         d = np.abs(out[name].intensities.cpu().numpy() - ref.intensities.cpu().numpy())
         assert d.max() <= 1e-8, (name, d.max())
         assert np.abs(out[name].iterations - ref.iterations).max() <= 2 + 0.1 * ref.iterations.max()
+
+
+@pytest.mark.parametrize("nz", [41, 150])
+def test_channel_major_tensor_core_kernel_matches_simt(nz, monkeypatch):
+    """The channel-major tcgen05 block inverse (bg=3) on odd and even node
+    counts (odd: no bulk prefetch, 8-byte stores) and a row total that leaves
+    a partial last tile, against the SIMT FP32 kernel and a mixed solve
+    against FP64."""
+    case, systems = cfg2_batch(n_solves=7, seed=5, nz=nz)
+    monkeypatch.setenv("MSC_TUNE", "c64=2,c32=2,bi=128,bg=3")
+    mixed = ScatteringPlan(case.v, case.t, systems, precision="mixed", tensor_cores=True)
+    rows = mixed.total_rows
+    rng = np.random.default_rng(nz)
+    x = rng.standard_normal((rows, nz)) + 1j * rng.standard_normal((rows, nz))
+    x32 = torch.as_tensor(x.astype(np.complex64), device="cuda")
+    y_tc = mixed.apply_block_inverse_f32(x32).cpu().numpy()
+    # (the plan read MSC_TUNE at its first call)
+    assert "block_inverse32=tcc" in mixed.tuning_report()["chosen"]
+    monkeypatch.setenv("MSC_TUNE", "c64=2,c32=2,bi=0")
+    simt = ScatteringPlan(case.v, case.t, systems, precision="mixed", tensor_cores=False)
+    y_simt = simt.apply_block_inverse_f32(x32).cpu().numpy()
+    scale = np.abs(y_simt).max()
+    np.testing.assert_allclose(y_tc, y_simt, rtol=0, atol=TC_TOL * scale)
+    ref = ScatteringPlan(case.v, case.t, systems).solve().intensities
+    res = mixed.solve()
+    assert (res.status == 0).all()
+    assert float((res.intensities - ref).abs().max()) <= MIXED_TOL
+    mixed.close()
+    simt.close()
