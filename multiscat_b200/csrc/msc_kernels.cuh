@@ -2037,7 +2037,7 @@ k_dcgs_reduce_bulk(ArnoldiArgs a, const float2 *__restrict__ Q, int j, const flo
 // Per-system scalar work at the end of the update (one thread): the
 // provisional column j from ||v_{j+1}||, its rotation, the iteration count
 // and the stop rules.
-__device__ __noinline__ void dcgs_update_finish(GmresState &st, const DcgsState &ds, int s, int m, int j,
+__device__ __forceinline__ void dcgs_update_finish(GmresState &st, const DcgsState &ds, int s, int m, int j,
                                                 double rtol, int max_iter, double inner_rtol)
 {
     const double vn2 = st.h2[(size_t)s * (m + 2)].x;

@@ -1721,9 +1721,16 @@ msc_status finalize(msc_plan *p)
         const int max_rows = cn.empty() ? 0 : *std::max_element(cn.begin(), cn.end());
         const char *rmode = std::getenv("MSC_ARNOLDI_STREAM");
         const bool bulk_ok = p->mixed && n % 2 == 0 && (long long)max_rows * n <= msc::kBulkChunk;
+        // Small chunks (a few rows: small batches, single systems) leave most
+        // of a streamed block's threads idle; the register-streamed passes
+        // split them across warps instead (cfg1, one 1681-row system in
+        // 400-element chunks: 52 + 24 against 73 + 40 us per step).
+        const bool bulk_big = (long long)max_rows * n >= msc::kBulkChunk / 2;
         // (MSC_ARNOLDI_STREAM=registers selects the register-streamed passes,
-        // =reduce the streamed reduction with the register-streamed update)
-        p->bulk_arnoldi = bulk_ok ? 2 : 0;
+        // =reduce the streamed reduction with the register-streamed update,
+        // =bulk both streamed wherever the chunks allow it)
+        p->bulk_arnoldi = (bulk_ok && bulk_big) ? 2 : 0;
+        if (bulk_ok && rmode && std::strcmp(rmode, "bulk") == 0) p->bulk_arnoldi = 2;
         if (bulk_ok && rmode && std::strcmp(rmode, "registers") == 0) p->bulk_arnoldi = 0;
         if (bulk_ok && rmode && std::strcmp(rmode, "reduce") == 0) p->bulk_arnoldi = 1;
         MSC_CUDA(p->wait_error.alloc(1));

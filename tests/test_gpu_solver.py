@@ -658,17 +658,16 @@ def test_dcgs2_and_cgs2_arnoldi_agree(precision):
 
 def test_streamed_arnoldi_passes_agree_with_register_form(monkeypatch):
     """The FP32 DCGS2 reduction and update that stream the basis through
-    shared memory by bulk copies (the default where chunks allow it; the
-    reduction alone, or both) and the register-streamed passes compute the
+    shared memory by bulk copies (the default for chunks of 2048-4096
+    elements; the reduction alone, or both) and the register-streamed passes compute the
     same sums in another grouping: the same converged intensities and about
     the same iteration counts."""
     case, systems = cfg2_batch(n_solves=24, seed=3)
     out = {}
-    for mode, name in (("registers", "registers"), ("reduce", "bulk_reduce"), (None, "bulk")):
-        if mode is None:
-            monkeypatch.delenv("MSC_ARNOLDI_STREAM", raising=False)
-        else:
-            monkeypatch.setenv("MSC_ARNOLDI_STREAM", mode)
+    # (24 beams make chunks of ~1300 elements, below the default threshold of
+    # the streamed passes: "bulk" forces them)
+    for mode, name in (("registers", "registers"), ("reduce", "bulk_reduce"), ("bulk", "bulk")):
+        monkeypatch.setenv("MSC_ARNOLDI_STREAM", mode)
         plan = ScatteringPlan(case.v, case.t, systems, rtol=1e-10, precision="mixed")
         res = plan.solve()
         assert plan.tuning_report()["arnoldi_stream"] == name
