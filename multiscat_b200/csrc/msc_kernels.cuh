@@ -1942,23 +1942,21 @@ k_dcgs_reduce_bulk(ArnoldiArgs a, const float2 *__restrict__ Q, int j, const flo
     }
     for (int i = threadIdx.x; i < 2 * nv * NW; i += NT) red[i / NW][i % NW] = make_double2(0.0, 0.0);
     __syncthreads();
-    int issued = 0;                                    // thread 0: vectors whose copy was issued
+    // the stream: item 0 = v (slot j), item 1 = w, item 2 + i = q_i; v and
+    // w come through the ring too, so no thread waits on a global load
+    const int NI = j + 2;
+    auto src_of = [&](int it) {
+        return it == 0 ? Q + (size_t)j * a.qstride + e0
+             : it == 1 ? W + e0 : Q + (size_t)(it - 2) * a.qstride + e0;
+    };
+    int issued = 0;                                    // thread 0: items whose copy was issued
     if (threadIdx.x == 0) {
-        for (; issued < min(kBulkStages, j); ++issued) {
+        for (; issued < min(kBulkStages, NI); ++issued) {
             mbar_expect_tx(&full[issued], bytes);
-            bulk_g2s(ring + (size_t)issued * SP, Q + (size_t)issued * a.qstride + e0, bytes,
-                     &full[issued]);
+            bulk_g2s(ring + (size_t)issued * SP, src_of(issued), bytes, &full[issued]);
         }
     }
-    const float4 *vp = reinterpret_cast<const float4 *>(Q + (size_t)j * a.qstride + e0);
-    const float4 *wp = reinterpret_cast<const float4 *>(W + e0);
     float4 vv[UP], ww[UP];
-#pragma unroll
-    for (int u = 0; u < UP; ++u) {
-        const int p = threadIdx.x + u * NT;
-        vv[u] = p < np ? vp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
-        ww[u] = p < np ? wp[p] : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
     // dots of one vector's pairs with v and w (FP32 products and lane
     // partial sums, as k_dcgs_reduce<float>); pair u comes from load(u)
     auto dots = [&](auto load, float &ar, float &ai, float &br, float &bi) {
@@ -1988,25 +1986,34 @@ k_dcgs_reduce_bulk(ArnoldiArgs a, const float2 *__restrict__ Q, int j, const flo
     };
     bool ok = true;
     int i = 0;
-    for (; i < j; ++i) {
+    for (; i < NI; ++i) {
         const int stg = i % kBulkStages;
         const bool got = mbar_wait(&full[stg], (uint32_t)(i / kBulkStages) & 1u);
         const float4 *qs = ring + (size_t)stg * SP;
-        float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
-        dots([&](int u) {
+        auto ld = [&](int u) {
             const int p = threadIdx.x + u * NT;
             return (got && p < np) ? qs[p] : make_float4(0.f, 0.f, 0.f, 0.f);
-        }, ar, ai, br, bi);
-        add_sums(i, ar, ai, br, bi);
+        };
+        if (i == 0) {
+#pragma unroll
+            for (int u = 0; u < UP; ++u) vv[u] = ld(u);
+        } else if (i == 1) {
+#pragma unroll
+            for (int u = 0; u < UP; ++u) ww[u] = ld(u);
+        } else {
+            float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
+            dots(ld, ar, ai, br, bi);
+            add_sums(i - 2, ar, ai, br, bi);
+        }
         // every thread is done with this stage before it is refilled
         if (!__syncthreads_and(got)) {
             ok = false;
             break;
         }
-        if (threadIdx.x == 0 && issued < j) {
+        if (threadIdx.x == 0 && issued < NI) {
             fence_proxy_async();
             mbar_expect_tx(&full[stg], bytes);
-            bulk_g2s(ring + (size_t)stg * SP, Q + (size_t)issued * a.qstride + e0, bytes, &full[stg]);
+            bulk_g2s(ring + (size_t)stg * SP, src_of(issued), bytes, &full[stg]);
             ++issued;
         }
     }
@@ -2198,38 +2205,47 @@ k_dcgs_update_bulk(ArnoldiArgs a, float2 *__restrict__ Q, int j, const float2 *_
         mbar_fence_init();
     }
     __syncthreads();
+    // the stream: item 0 = v (slot j), item 1 = w, item 2 + i = q_i
+    const int NI = j + 2;
+    auto src_of = [&](int it) {
+        return it == 0 ? Q + (size_t)j * a.qstride + e0
+             : it == 1 ? W + e0 : Q + (size_t)(it - 2) * a.qstride + e0;
+    };
     int issued = 0;
     if (threadIdx.x == 0) {
-        for (; issued < min(kBulkStages, j); ++issued) {
+        for (; issued < min(kBulkStages, NI); ++issued) {
             mbar_expect_tx(&full[issued], bytes);
-            bulk_g2s(ring + (size_t)issued * SP, Q + (size_t)issued * a.qstride + e0, bytes,
-                     &full[issued]);
+            bulk_g2s(ring + (size_t)issued * SP, src_of(issued), bytes, &full[issued]);
         }
     }
     float4 *vq = reinterpret_cast<float4 *>(Q + (size_t)j * a.qstride + e0);        // v in, q_j out
     float4 *vn = reinterpret_cast<float4 *>(Q + (size_t)(j + 1) * a.qstride + e0);  // v_{j+1} out
-    const float4 *wp = reinterpret_cast<const float4 *>(W + e0);
-    // q = v / nu ; n = w / nu + dv v   (two elements per float4)
     float4 qa[UP], na[UP];
-#pragma unroll
-    for (int u = 0; u < UP; ++u) {
-        const int p = threadIdx.x + u * NT;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f), w = v;
-        if (p < np) {
-            v = vq[p];
-            w = wp[p];
-        }
-        qa[u] = make_float4(v.x * inu, v.y * inu, v.z * inu, v.w * inu);
-        na[u] = make_float4(w.x * inu + (dv.x * v.x - dv.y * v.y), w.y * inu + (dv.x * v.y + dv.y * v.x),
-                            w.z * inu + (dv.x * v.z - dv.y * v.w), w.w * inu + (dv.x * v.w + dv.y * v.z));
-    }
     bool ok = true;
     int i = 0;
-    for (; i < j; ++i) {
+    for (; i < NI; ++i) {
         const int stg = i % kBulkStages;
         const bool got = mbar_wait(&full[stg], (uint32_t)(i / kBulkStages) & 1u);
         const float4 *qs = ring + (size_t)stg * SP;
-        const float2 x = ca[i], y = cb[i];
+        if (i < 2) {
+#pragma unroll
+            for (int u = 0; u < UP; ++u) {
+                const int p = threadIdx.x + u * NT;
+                const float4 t = (got && p < np) ? qs[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+                if (i == 0) {
+                    qa[u] = t;                          // v, until w arrives
+                } else {
+                    // q = v / nu ; n = w / nu + dv v   (two elements per float4)
+                    const float4 v = qa[u], w = t;
+                    qa[u] = make_float4(v.x * inu, v.y * inu, v.z * inu, v.w * inu);
+                    na[u] = make_float4(w.x * inu + (dv.x * v.x - dv.y * v.y),
+                                        w.y * inu + (dv.x * v.y + dv.y * v.x),
+                                        w.z * inu + (dv.x * v.z - dv.y * v.w),
+                                        w.w * inu + (dv.x * v.w + dv.y * v.z));
+                }
+            }
+        } else {
+        const float2 x = ca[i - 2], y = cb[i - 2];
 #pragma unroll
         for (int u = 0; u < UP; ++u) {
             const int p = threadIdx.x + u * NT;
@@ -2245,14 +2261,15 @@ k_dcgs_update_bulk(ArnoldiArgs a, float2 *__restrict__ Q, int j, const float2 *_
             nn.z = fmaf(b.z, y.x, fmaf(-b.w, y.y, nn.z));
             nn.w = fmaf(b.z, y.y, fmaf(b.w, y.x, nn.w));
         }
+        }
         if (!__syncthreads_and(got)) {
             ok = false;
             break;
         }
-        if (threadIdx.x == 0 && issued < j) {
+        if (threadIdx.x == 0 && issued < NI) {
             fence_proxy_async();
             mbar_expect_tx(&full[stg], bytes);
-            bulk_g2s(ring + (size_t)stg * SP, Q + (size_t)issued * a.qstride + e0, bytes, &full[stg]);
+            bulk_g2s(ring + (size_t)stg * SP, src_of(issued), bytes, &full[stg]);
             ++issued;
         }
     }
