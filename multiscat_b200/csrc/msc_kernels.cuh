@@ -1681,15 +1681,14 @@ struct DcgsState {
 };
 
 // Column j of H from its unrotated entries: apply rotations 0..j-1, make
-// rotation j from (H[j], H[j+1]) and update g (g[j] is taken from gsave,
-// g[j+1] starts at 0).  Returns the new residual estimate |g[j+1]|.
-__device__ double dcgs_rotate_column(GmresState &st, const DcgsState &ds, int s, int m, int j)
+// rotation j from (H[j], H[j+1]) and update g (g[j] is taken from gj, the
+// value saved before the provisional rotation j; g[j+1] starts at 0).
+// Returns the new residual estimate |g[j+1]|.  The arrays are one system's
+// (raw: its unrotated column j; H: its column j; cs, sn, g), in global or
+// shared memory.
+__device__ double dcgs_rotate_column_p(const double2 *raw, double2 *H, double2 *cs, double2 *sn,
+                                       double2 *g, double2 gj, int j)
 {
-    const double2 *raw = ds.Hraw + (size_t)s * (m + 1) * m + (size_t)j * (m + 1);
-    double2 *H = st.H + (size_t)s * (m + 1) * m + (size_t)j * (m + 1);
-    double2 *cs = st.cs + (size_t)s * m;
-    double2 *sn = st.sn + (size_t)s * m;
-    double2 *g = st.g + (size_t)s * (m + 1);
     for (int i = 0; i <= j + 1; ++i) H[i] = raw[i];
     for (int i = 0; i < j; ++i) {
         const double c = cs[i].x;
@@ -1718,10 +1717,17 @@ __device__ double dcgs_rotate_column(GmresState &st, const DcgsState &ds, int s,
     sn[j] = sv;
     H[j] = (aa == 0.0) ? make_double2(beta, 0.0) : cscale(a, r / aa);
     H[j + 1] = make_double2(0.0, 0.0);
-    const double2 gj = ds.gsave[s];
     g[j] = cscale(gj, c);
     g[j + 1] = make_double2(-(sv.x * gj.x + sv.y * gj.y), -(sv.x * gj.y - sv.y * gj.x));
     return sqrt(cabs2(g[j + 1]));
+}
+
+__device__ __forceinline__ double dcgs_rotate_column(GmresState &st, const DcgsState &ds, int s, int m, int j)
+{
+    return dcgs_rotate_column_p(ds.Hraw + (size_t)s * (m + 1) * m + (size_t)j * (m + 1),
+                                st.H + (size_t)s * (m + 1) * m + (size_t)j * (m + 1),
+                                st.cs + (size_t)s * m, st.sn + (size_t)s * m,
+                                st.g + (size_t)s * (m + 1), ds.gsave[s], j);
 }
 
 __device__ __forceinline__ bool dcgs_stop(const GmresState &st, int s, double est, double rtol,
@@ -1735,44 +1741,39 @@ __device__ __forceinline__ bool dcgs_stop(const GmresState &st, int s, double es
 //   coef[0..j)        a_i = -s_i / nu            (q_j = v / nu + sum a_i Q_i)
 //   coef[j+1 .. 2j+1) b_i = -(c_i - s_i d / nu)  (v_{j+1} = w / nu - (d / nu) v + sum b_i Q_i)
 //   coef[2m+2] = (1 / nu, 0), coef[2m+3] = -d / nu
-__device__ __noinline__ void dcgs_coefficients(GmresState &st, const DcgsState &ds, int s, int m, int j,
-                                  double rtol, double inner_rtol)
+// on one system's arrays (global or shared memory): raw = its unrotated
+// Hessenberg columns, sum = its reduction results, Hj1 = its column j - 1 of
+// H, hs = scratch of j + 1 entries.  Returns 1 when the system stops
+// (converged, or no new direction), with *est set when j > 0.
+__device__ int dcgs_coefficients_p(double2 *raw, const double2 *sum, double2 *Hj1, double2 *cs,
+                                   double2 *sn, double2 *g, double2 gsave, double2 *cf, double2 *hs,
+                                   int m, int j, double bnorm, double beta0, double rtol,
+                                   double inner_rtol, double *est)
 {
-    const double2 *sum = ds.dsum + (size_t)s * 2 * (m + 1);
     const double2 *sv = sum;               // s_i = q_i^H v, i < j;  sum[j] = ||v||^2
     const double2 *tv = sum + (j + 1);     // t_i = q_i^H w, i < j;  tv[j] = v^H w
-    double2 *raw = ds.Hraw + (size_t)s * (m + 1) * m;
-    double2 *cf = ds.coef + (size_t)s * ds.cstride;
     double ss = 0.0;
     for (int i = 0; i < j; ++i) ss += cabs2(sv[i]);
     const double nu2 = sum[j].x - ss;
     const double nu = sqrt(fmax(nu2, 0.0));
     if (j == 0) {
         // v = q_0 up to rounding; g[0] = beta follows q_0 = v / nu
-        double2 *g = st.g + (size_t)s * (m + 1);
         g[0] = cscale(g[0], nu);
     } else {
         double2 *col = raw + (size_t)(j - 1) * (m + 1);
         for (int i = 0; i < j; ++i) col[i] = cadd(col[i], sv[i]);
         col[j] = make_double2(nu, 0.0);
-        const double est = dcgs_rotate_column(st, ds, s, m, j - 1);
-        st.est[s] = est;
-        if (dcgs_stop(st, s, est, rtol, inner_rtol)) {
-            st.active[s] = 0;              // q_0 .. q_{j-1} are final; kcyc = j
-            return;
-        }
+        *est = dcgs_rotate_column_p(col, Hj1, cs, sn, g, gsave, j - 1);
+        if (!isfinite(*est) || *est <= fmax(rtol * bnorm, inner_rtol * beta0))
+            return 1;                      // q_0 .. q_{j-1} are final; kcyc = j
     }
-    if (!(nu > 1e-300) || !isfinite(nu)) {
-        st.active[s] = 0;
-        return;
-    }
+    if (!(nu > 1e-300) || !isfinite(nu)) return 1;
     const double inu = 1.0 / nu;
     // Hs = Hbar[:j+1, :j] s (column k has entries 0..k+1)
-    double2 hs[kMaxRestart + 1];
     for (int i = 0; i <= j; ++i) hs[i] = make_double2(0.0, 0.0);
     for (int k = 0; k < j; ++k) {
-        const double2 *col = raw + (size_t)k * (m + 1);
-        for (int i = 0; i <= k + 1; ++i) hs[i] = cadd(hs[i], cmul(col[i], sv[k]));
+        const double2 *colk = raw + (size_t)k * (m + 1);
+        for (int i = 0; i <= k + 1; ++i) hs[i] = cadd(hs[i], cmul(colk[i], sv[k]));
     }
     double2 sht = make_double2(0.0, 0.0);   // s^H t
     for (int i = 0; i < j; ++i) sht = cadd(sht, cmul(cconj(sv[i]), tv[i]));
@@ -1789,6 +1790,94 @@ __device__ __noinline__ void dcgs_coefficients(GmresState &st, const DcgsState &
     }
     cf[2 * m + 2] = make_double2(inu, 0.0);
     cf[2 * m + 3] = make_double2(-dn.x, -dn.y);
+    return 0;
+}
+
+__device__ __noinline__ void dcgs_coefficients(GmresState &st, const DcgsState &ds, int s, int m, int j,
+                                               double rtol, double inner_rtol)
+{
+    double2 hs[kMaxRestart + 1];
+    double est = 0.0;
+    const size_t hb = (size_t)s * (m + 1) * m;
+    const int stop = dcgs_coefficients_p(
+        ds.Hraw + hb, ds.dsum + (size_t)s * 2 * (m + 1), st.H + hb + (size_t)(j > 0 ? j - 1 : 0) * (m + 1),
+        st.cs + (size_t)s * m, st.sn + (size_t)s * m, st.g + (size_t)s * (m + 1), ds.gsave[s],
+        ds.coef + (size_t)s * ds.cstride, hs, m, j, st.bnorm[s], st.beta0[s], rtol, inner_rtol, &est);
+    if (j > 0) st.est[s] = est;
+    if (stop) st.active[s] = 0;
+}
+
+// Double2 entries of the shared scratch dcgs_coefficients_block needs.
+__host__ __device__ constexpr int dcgs_block_scratch(int m)
+{
+    return (m + 1) * (m + 1) + 5 * (m + 1) + 4 * m + 4;
+}
+
+// dcgs_coefficients for the last block of a system: the whole block copies
+// the system's Hessenberg columns 0..j, reduction results, rotations and g
+// into shared memory (one round of parallel loads), thread 0 runs the
+// serial algebra there, and the block writes back what changed.  The
+// serial part then waits on shared memory instead of an L2 round trip per
+// element (the tail of the reduction kernel).  sc: dcgs_block_scratch(m)
+// entries of shared memory.
+__device__ void dcgs_coefficients_block(GmresState &st, const DcgsState &ds, int s, int m, int j,
+                                        double rtol, double inner_rtol, double2 *sc)
+{
+    const int M1 = m + 1, ncol = j + 1;
+    double2 *raw = sc;                           // [ncol][M1] unrotated columns 0..j
+    double2 *sum = raw + (size_t)ncol * M1;      // [2 M1]
+    double2 *cs = sum + 2 * M1;                  // [m]
+    double2 *sn = cs + m;                        // [m]
+    double2 *g = sn + m;                         // [M1]
+    double2 *Hj1 = g + M1;                       // [M1] column j - 1 of H
+    double2 *cf = Hj1 + M1;                      // [2 m + 4]
+    double2 *hs = cf + 2 * m + 4;                // [M1]
+    __shared__ int res;
+    const size_t hb = (size_t)s * M1 * m;
+    const int nt = blockDim.x;
+    for (int i = threadIdx.x; i < ncol * M1; i += nt) raw[i] = ds.Hraw[hb + i];
+    for (int i = threadIdx.x; i < 2 * M1; i += nt) sum[i] = ds.dsum[(size_t)s * 2 * M1 + i];
+    for (int i = threadIdx.x; i < m; i += nt) {
+        cs[i] = st.cs[(size_t)s * m + i];
+        sn[i] = st.sn[(size_t)s * m + i];
+    }
+    for (int i = threadIdx.x; i < M1; i += nt) g[i] = st.g[(size_t)s * M1 + i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double est = 0.0;
+        res = dcgs_coefficients_p(raw, sum, Hj1, cs, sn, g, ds.gsave[s], cf, hs, m, j, st.bnorm[s],
+                                  st.beta0[s], rtol, inner_rtol, &est);
+        if (j > 0) st.est[s] = est;
+        if (res) st.active[s] = 0;
+    }
+    __syncthreads();
+    if (j == 0) {
+        if (threadIdx.x == 0) st.g[(size_t)s * M1] = g[0];
+    } else {
+        // column j - 1: its final entries 0..j, its rotated form, rotation j - 1, g
+        for (int i = threadIdx.x; i <= j; i += nt) {
+            ds.Hraw[hb + (size_t)(j - 1) * M1 + i] = raw[(size_t)(j - 1) * M1 + i];
+            st.H[hb + (size_t)(j - 1) * M1 + i] = Hj1[i];
+        }
+        if (threadIdx.x == 0) {
+            st.cs[(size_t)s * m + j - 1] = cs[j - 1];
+            st.sn[(size_t)s * m + j - 1] = sn[j - 1];
+            st.g[(size_t)s * M1 + j - 1] = g[j - 1];
+            st.g[(size_t)s * M1 + j] = g[j];
+        }
+    }
+    if (res == 0) {
+        double2 *cfg = ds.coef + (size_t)s * ds.cstride;
+        for (int i = threadIdx.x; i <= j; i += nt) ds.Hraw[hb + (size_t)j * M1 + i] = raw[(size_t)j * M1 + i];
+        for (int i = threadIdx.x; i < j; i += nt) {
+            cfg[i] = cf[i];
+            cfg[j + 1 + i] = cf[j + 1 + i];
+        }
+        if (threadIdx.x == 0) {
+            cfg[2 * m + 2] = cf[2 * m + 2];
+            cfg[2 * m + 3] = cf[2 * m + 3];
+        }
+    }
 }
 
 template <typename R> struct DcgsUnroll { static constexpr int value = 8; };
@@ -1914,6 +2003,9 @@ constexpr int kBulkChunk = 4096;
 constexpr int kBulkStages = 3;
 
 __host__ __device__ constexpr size_t dcgs_bulk_smem() { return (size_t)kBulkStages * kBulkChunk * 8; }
+// the last block's scalar work reuses the ring as its scratch
+static_assert((size_t)dcgs_block_scratch(kMaxRestart) * sizeof(double2) <= dcgs_bulk_smem(),
+              "the DCGS2 scalar scratch must fit in the streaming ring");
 
 __global__ void __launch_bounds__(256, 2)
 k_dcgs_reduce_bulk(ArnoldiArgs a, const float2 *__restrict__ Q, int j, const float2 *__restrict__ W,
@@ -2037,7 +2129,7 @@ k_dcgs_reduce_bulk(ArnoldiArgs a, const float2 *__restrict__ Q, int j, const flo
         out[k] = acc;
     }
     if (last_block_reduce(a, s, 2 * nv, ds.dsum + (size_t)s * 2 * (m + 1))) {
-        if (threadIdx.x == 0) dcgs_coefficients(st, ds, s, m, j, rtol, inner_rtol);
+        dcgs_coefficients_block(st, ds, s, m, j, rtol, inner_rtol, reinterpret_cast<double2 *>(smem_raw));
     }
 }
 
@@ -2062,6 +2154,53 @@ __device__ __forceinline__ void dcgs_update_finish(GmresState &st, const DcgsSta
     if (st.iters[s] >= max_iter) stop = true;
     if (beta <= 1e-300) stop = true;
     if (stop) st.active[s] = 0;
+}
+
+// dcgs_update_finish for the last block of a system, with column j, the
+// rotations and g staged in shared memory by the whole block (sc: 3 (m + 1)
+// + 2 m entries); thread 0 runs the serial part there.
+__device__ void dcgs_update_finish_block(GmresState &st, const DcgsState &ds, int s, int m, int j,
+                                         double rtol, int max_iter, double inner_rtol, double2 *sc)
+{
+    const int M1 = m + 1;
+    double2 *rawj = sc;                          // [M1] unrotated column j
+    double2 *Hj = rawj + M1;                     // [M1] its rotated form
+    double2 *cs = Hj + M1;                       // [m]
+    double2 *sn = cs + m;                        // [m]
+    double2 *g = sn + m;                         // [M1]
+    const size_t hb = (size_t)s * M1 * m + (size_t)j * M1;
+    const int nt = blockDim.x;
+    for (int i = threadIdx.x; i <= j; i += nt) rawj[i] = ds.Hraw[hb + i];
+    for (int i = threadIdx.x; i < m; i += nt) {
+        cs[i] = st.cs[(size_t)s * m + i];
+        sn[i] = st.sn[(size_t)s * m + i];
+    }
+    for (int i = threadIdx.x; i < M1; i += nt) g[i] = st.g[(size_t)s * M1 + i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double vn2 = st.h2[(size_t)s * (m + 2)].x;
+        const double beta = sqrt(fmax(vn2, 0.0));
+        rawj[j + 1] = make_double2(beta, 0.0);
+        ds.Hraw[hb + j + 1] = rawj[j + 1];
+        const double2 gj = g[j];
+        ds.gsave[s] = gj;
+        const double est = dcgs_rotate_column_p(rawj, Hj, cs, sn, g, gj, j);
+        st.cs[(size_t)s * m + j] = cs[j];
+        st.sn[(size_t)s * m + j] = sn[j];
+        st.g[(size_t)s * M1 + j] = g[j];
+        st.g[(size_t)s * M1 + j + 1] = g[j + 1];
+        st.est[s] = est;
+        st.kcyc[s] = j + 1;
+        st.iters[s] += 1;
+        st.projv[s] += j + 1;
+        bool stop = dcgs_stop(st, s, est, rtol, inner_rtol) || !isfinite(beta);
+        if (j + 1 >= m) stop = true;
+        if (st.iters[s] >= max_iter) stop = true;
+        if (beta <= 1e-300) stop = true;
+        if (stop) st.active[s] = 0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= j + 1; i += nt) st.H[hb + i] = Hj[i];
 }
 
 // Update pass of step j over row chunks: slot j <- q_j, slot j + 1 <- v_{j+1}
@@ -2300,7 +2439,8 @@ k_dcgs_update_bulk(ArnoldiArgs a, float2 *__restrict__ Q, int j, const float2 *_
         a.partial[(size_t)blk * a.pstride] = make_double2(t, 0.0);
     }
     if (last_block_reduce(a, s, 1, st.h2 + (size_t)s * (m + 2))) {
-        if (threadIdx.x == 0) dcgs_update_finish(st, ds, s, m, j, rtol, max_iter, inner_rtol);
+        dcgs_update_finish_block(st, ds, s, m, j, rtol, max_iter, inner_rtol,
+                                 reinterpret_cast<double2 *>(smem_raw));
     }
 }
 
