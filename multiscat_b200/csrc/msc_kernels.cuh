@@ -1675,7 +1675,7 @@ k_arnoldi_p2(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int nvec,
 struct DcgsState {
     double2 *Hraw;    // [B][(m+1)*m]  unrotated Hessenberg (column j at j*(m+1))
     double2 *dsum;    // [B][2(m+1)]   per-system reduction results of the step
-    double2 *coef;    // [B][cstride]  update coefficients (see dcgs_coefficients)
+    double2 *coef;    // [B][cstride]  update coefficients (see dcgs_coefficients_p)
     double2 *gsave;   // [B]           g[j] before the provisional rotation j
     int cstride;      // 2 m + 4
 };
@@ -1793,27 +1793,13 @@ __device__ int dcgs_coefficients_p(double2 *raw, const double2 *sum, double2 *Hj
     return 0;
 }
 
-__device__ __noinline__ void dcgs_coefficients(GmresState &st, const DcgsState &ds, int s, int m, int j,
-                                               double rtol, double inner_rtol)
-{
-    double2 hs[kMaxRestart + 1];
-    double est = 0.0;
-    const size_t hb = (size_t)s * (m + 1) * m;
-    const int stop = dcgs_coefficients_p(
-        ds.Hraw + hb, ds.dsum + (size_t)s * 2 * (m + 1), st.H + hb + (size_t)(j > 0 ? j - 1 : 0) * (m + 1),
-        st.cs + (size_t)s * m, st.sn + (size_t)s * m, st.g + (size_t)s * (m + 1), ds.gsave[s],
-        ds.coef + (size_t)s * ds.cstride, hs, m, j, st.bnorm[s], st.beta0[s], rtol, inner_rtol, &est);
-    if (j > 0) st.est[s] = est;
-    if (stop) st.active[s] = 0;
-}
-
 // Double2 entries of the shared scratch dcgs_coefficients_block needs.
 __host__ __device__ constexpr int dcgs_block_scratch(int m)
 {
     return (m + 1) * (m + 1) + 5 * (m + 1) + 4 * m + 4;
 }
 
-// dcgs_coefficients for the last block of a system: the whole block copies
+// dcgs_coefficients_p for the last block of a system: the whole block copies
 // the system's Hessenberg columns 0..j, reduction results, rotations and g
 // into shared memory (one round of parallel loads), thread 0 runs the
 // serial algebra there, and the block writes back what changed.  The
@@ -1888,7 +1874,7 @@ template <> struct DcgsUnroll<double> { static constexpr int value = 4; };
 // streams q_0 .. q_{j-1} and v itself (the basis slots 0 .. j), two dots per
 // vector (q_i^H v, q_i^H w), reduced across the warp per vector and added in
 // a fixed order (deterministic).  The last block of a system reduces the
-// per-block partials and runs dcgs_coefficients.
+// per-block partials and runs dcgs_coefficients_block.
 // Precision: a lane's products and its partial sum of U terms are formed in
 // the vectors' own type (FP32 for the inner solve of the mixed form: FP64
 // products there made the FP64 pipe, not memory, the limit), the sums across
@@ -1980,7 +1966,8 @@ k_dcgs_reduce(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int j,
         out[i] = acc;
     }
     if (last_block_reduce(a, s, 2 * nv, ds.dsum + (size_t)s * 2 * (m + 1))) {
-        if (threadIdx.x == 0) dcgs_coefficients(st, ds, s, m, j, rtol, inner_rtol);
+        extern __shared__ __align__(16) unsigned char dcgs_scratch[];   // dcgs_block_scratch(m) entries
+        dcgs_coefficients_block(st, ds, s, m, j, rtol, inner_rtol, reinterpret_cast<double2 *>(dcgs_scratch));
     }
 }
 
@@ -2133,32 +2120,12 @@ k_dcgs_reduce_bulk(ArnoldiArgs a, const float2 *__restrict__ Q, int j, const flo
     }
 }
 
-// Per-system scalar work at the end of the update (one thread): the
-// provisional column j from ||v_{j+1}||, its rotation, the iteration count
-// and the stop rules.
-__device__ __forceinline__ void dcgs_update_finish(GmresState &st, const DcgsState &ds, int s, int m, int j,
-                                                double rtol, int max_iter, double inner_rtol)
-{
-    const double vn2 = st.h2[(size_t)s * (m + 2)].x;
-    const double beta = sqrt(fmax(vn2, 0.0));
-    double2 *col = ds.Hraw + (size_t)s * (m + 1) * m + (size_t)j * (m + 1);
-    col[j + 1] = make_double2(beta, 0.0);
-    ds.gsave[s] = st.g[(size_t)s * (m + 1) + j];
-    const double est = dcgs_rotate_column(st, ds, s, m, j);
-    st.est[s] = est;
-    st.kcyc[s] = j + 1;
-    st.iters[s] += 1;
-    st.projv[s] += j + 1;
-    bool stop = dcgs_stop(st, s, est, rtol, inner_rtol) || !isfinite(beta);
-    if (j + 1 >= m) stop = true;
-    if (st.iters[s] >= max_iter) stop = true;
-    if (beta <= 1e-300) stop = true;
-    if (stop) st.active[s] = 0;
-}
 
-// dcgs_update_finish for the last block of a system, with column j, the
-// rotations and g staged in shared memory by the whole block (sc: 3 (m + 1)
-// + 2 m entries); thread 0 runs the serial part there.
+// Per-system scalar work at the end of the update, for the last block of a
+// system: the provisional column j from ||v_{j+1}||, its rotation, the
+// iteration count and the stop rules.  Column j, the rotations and g are
+// staged in shared memory by the whole block (sc: 3 (m + 1) + 2 m entries);
+// thread 0 runs the serial part there.
 __device__ void dcgs_update_finish_block(GmresState &st, const DcgsState &ds, int s, int m, int j,
                                          double rtol, int max_iter, double inner_rtol, double2 *sc)
 {
@@ -2299,7 +2266,9 @@ k_dcgs_update(ArnoldiArgs a, typename CT<R>::t *__restrict__ Q, int j,
         a.partial[(size_t)blk * a.pstride] = make_double2(t, 0.0);
     }
     if (last_block_reduce(a, s, 1, st.h2 + (size_t)s * (m + 2))) {
-        if (threadIdx.x == 0) dcgs_update_finish(st, ds, s, m, j, rtol, max_iter, inner_rtol);
+        extern __shared__ __align__(16) unsigned char dcgs_scratch[];   // 3 (m + 1) + 2 m entries
+        dcgs_update_finish_block(st, ds, s, m, j, rtol, max_iter, inner_rtol,
+                                 reinterpret_cast<double2 *>(dcgs_scratch));
     }
 }
 

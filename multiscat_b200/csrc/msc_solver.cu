@@ -676,6 +676,10 @@ void launch_update(msc_plan *p, const int *gate, int nvec, const int *nvec_sys,
 
 int sys_blocks(int B) { return (B + 127) / 128; }
 
+// Shared scratch of the register-streamed DCGS2 passes' last-block work.
+size_t dcgs_scratch_bytes(int m) { return (size_t)msc::dcgs_block_scratch(m) * sizeof(double2); }
+size_t dcgs_update_scratch_bytes(int m) { return (size_t)(5 * m + 3) * sizeof(double2); }
+
 // Block layout of an Arnoldi kernel: large row chunks (P1) or row tiles
 // split into about 600 blocks in all (P2).
 msc::ArnoldiArgs arnoldi_args(msc_plan *p, const int *gate, bool chunks)
@@ -818,11 +822,11 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
                         a1, Q, j, W, p->state(), p->dstate(), p->m, p->desc.rtol, inner,
                         p->wait_error.p);
                 else
-                    msc::k_dcgs_reduce<R><<<nblk1, 256, 0, st>>>(a1, Q, j, W, p->state(),
+                    msc::k_dcgs_reduce<R><<<nblk1, 256, dcgs_scratch_bytes(p->m), st>>>(a1, Q, j, W, p->state(),
                                                                  p->dstate(), p->m, p->desc.rtol,
                                                                  inner);
             } else {
-                msc::k_dcgs_reduce<R><<<nblk1, 256, 0, st>>>(a1, Q, j, W, p->state(), p->dstate(),
+                msc::k_dcgs_reduce<R><<<nblk1, 256, dcgs_scratch_bytes(p->m), st>>>(a1, Q, j, W, p->state(), p->dstate(),
                                                              p->m, p->desc.rtol, inner);
             }
             if (tm) mark(p, 2, j, 1, st);
@@ -837,7 +841,7 @@ void record_iterations_t(msc_plan *p, C2<R> *Q, C2<R> *W, C2<R> *U, cudaStream_t
                 }
             }
             if (!updated)
-                msc::k_dcgs_update<R><<<nblk1, 256, 0, st>>>(a1, Q, j, W, p->state(), p->dstate(),
+                msc::k_dcgs_update<R><<<nblk1, 256, dcgs_update_scratch_bytes(p->m), st>>>(a1, Q, j, W, p->state(), p->dstate(),
                                                              p->m, p->desc.rtol,
                                                              p->desc.max_iterations, inner);
             if (tm) mark(p, 3, j, 1, st);
@@ -1735,6 +1739,12 @@ msc_status finalize(msc_plan *p)
         if (bulk_ok && rmode && std::strcmp(rmode, "reduce") == 0) p->bulk_arnoldi = 1;
         MSC_CUDA(p->wait_error.alloc(1));
         MSC_CUDA(cudaMemset(p->wait_error.p, 0, sizeof(int)));
+        // the register-streamed reduction's last block stages its scalar work
+        // in dynamic shared memory (up to the largest restart)
+        MSC_CUDA(cudaFuncSetAttribute(msc::k_dcgs_reduce<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)dcgs_scratch_bytes(msc::kMaxRestart)));
+        MSC_CUDA(cudaFuncSetAttribute(msc::k_dcgs_reduce<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)dcgs_scratch_bytes(msc::kMaxRestart)));
         if (p->bulk_arnoldi > 0)
             MSC_CUDA(cudaFuncSetAttribute(msc::k_dcgs_reduce_bulk,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
