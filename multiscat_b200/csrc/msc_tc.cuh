@@ -462,11 +462,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                 }
             }
             mma_commit(&bar_mma[g]);
-            // the next active tile (its search reads gate and row_sys from
-            // global memory) is found while the MMAs run; every thread of
-            // the group read next_s before the previous tile's last barrier
-            next_s[g] = find_active(tile + G * gridDim.x);
         }
+        // the next active tile (its search reads gate and row_sys from
+        // global memory) is found by warp 1 while the MMAs run (on the
+        // issuing thread it held up the wait that follows); every thread of
+        // the group read next_s before the previous tile's last barrier
+        if (gtid == 32) next_s[g] = find_active(tile + G * gridDim.x);
         mma_pending = true;
         if (mbar_wait(&bar_mma[g], mma_phase)) {
             mma_phase ^= 1u;

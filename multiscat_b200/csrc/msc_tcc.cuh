@@ -239,10 +239,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tcc(TcParams prm)
                 mma_bf16(d1, al, bh, idesc1, 1u);
             }
             mma_commit(&bar_mma);
-            // the next active tile is found while the MMAs run; every thread
-            // read next_s before the previous tile's last barrier
-            next_s = find_active(tile + gridDim.x);
         }
+        // the next active tile is found by warp 1 while the MMAs run; every
+        // thread read next_s before the previous tile's last barrier
+        if (tid == 32) next_s = find_active(tile + gridDim.x);
         mma_pending = true;
         if (mbar_wait(&bar_mma, mma_phase)) {
             mma_phase ^= 1u;
