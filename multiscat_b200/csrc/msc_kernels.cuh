@@ -181,9 +181,11 @@ k_block_inverse(Tiles tiles, const int *__restrict__ gate, int n, const R *__res
 // ---------------------------------------------------------------------------
 // Residual diagonal part (FP64):  out = b - D x  on every row of a tile.
 //   D x = T x + (Re V00 + pkd) x - c x(z_n) e_n ; b = b_spec e_n on the
-// specular row.  One FP64 GEMM with the symmetric T.
+// specular row.  One FP64 GEMM with the symmetric T.  One item per
+// (z, half of the tile's rows); the plan launches 2 n threads (rounded up to
+// a warp) when that is at most 512, so that a block takes one round.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(512)
 k_residual_diag(Tiles tiles, const int *__restrict__ gate, int n,
                 const double *__restrict__ Tm, const double *__restrict__ v00,
                 const double *__restrict__ row_pkd, const double2 *__restrict__ row_c,
@@ -1972,20 +1974,22 @@ k_dcgs_reduce(ArnoldiArgs a, const typename CT<R>::t *__restrict__ Q, int j,
 }
 
 // Reduction pass of step j with the basis streamed through shared memory
-// (FP32 Krylov vectors).  The block's chunk of each basis vector is one
-// contiguous range, so it arrives by a single cp.async.bulk into a ring of
-// kBulkStages stages, each completing on its own mbarrier: up to
-// kBulkStages vectors are in flight while one is reduced (the register form
-// above keeps one).  Two blocks per SM (3 stages of 32 KB each and 128
-// registers); one block with 6 stages was slower (239 against 186 us per
-// launch on the 512-beam cfg2 batch: 8 warps cannot keep up the FP32 work).  v and w stay in registers (thread t holds element
-// pairs t, t + 256, ...), and slot j (v itself) is reduced from them, so v
-// is read once.  Sums, their fixed order across warps and the last block's
-// work are those of k_dcgs_reduce.  Needs chunks of at most kBulkChunk
-// elements, an even count, starting on an even element (16-byte aligned
-// copies).  A wait that times out sets *err; the block then stops reducing,
-// waits (bounded) for its copies in flight and still takes part in the
-// per-system arrival count.
+// (FP32 Krylov vectors).  The block's chunk of each vector is one contiguous
+// range, so it arrives by a single cp.async.bulk into a ring of kBulkStages
+// stages, each completing on its own mbarrier: up to kBulkStages vectors are
+// in flight while one is reduced (the register form above keeps one).  The
+// stream is v, w, q_0 .. q_{j-1}: v and w land in registers (thread t holds
+// element pairs t, t + 256, ...), slot j (v itself) is reduced from them,
+// so v is read once and no thread waits on a global load.  Two blocks per
+// SM (3 stages of 32 KB each and 128 registers); one block with 6 stages was
+// slower (239 against 186 us per launch on the 512-beam cfg2 batch: 8 warps
+// cannot keep up the FP32 work).  Sums and their fixed order across warps
+// are those of k_dcgs_reduce; the last block of a system runs
+// dcgs_coefficients_block with the ring as its scratch.  Needs chunks of at
+// most kBulkChunk elements, an even count, starting on an even element
+// (16-byte aligned copies).  A wait that times out sets *err; the block then
+// stops reducing, waits (bounded) for its copies in flight and still takes
+// part in the per-system arrival count.
 constexpr int kBulkChunk = 4096;
 constexpr int kBulkStages = 3;
 
@@ -2274,10 +2278,11 @@ k_dcgs_update(ArnoldiArgs a, typename CT<R>::t *__restrict__ Q, int j,
 
 // Update pass of step j with the basis streamed through shared memory
 // (FP32 Krylov vectors; the chunks and stages of k_dcgs_reduce_bulk).
-// Thread t forms q_j and v_{j+1} of its element pairs t, t + 256, ... in
-// registers from v and w, then adds a_i q_i and b_i q_i as q_0 .. q_{j-1}
-// arrive; the arithmetic, ||v_{j+1}||^2 and the last block's work are those
-// of k_dcgs_update.  A wait that times out sets *err; the block then writes
+// The stream is v, w, q_0 .. q_{j-1}: thread t forms q_j and v_{j+1} of its
+// element pairs t, t + 256, ... in registers from v and w, then adds a_i q_i
+// and b_i q_i as the basis arrives; the arithmetic and ||v_{j+1}||^2 are
+// those of k_dcgs_update, the last block runs dcgs_update_finish_block with
+// the ring as its scratch.  A wait that times out sets *err; the block then writes
 // nothing, waits (bounded) for its copies in flight and still takes part
 // in the per-system arrival count.
 __global__ void __launch_bounds__(256, 2)

@@ -445,7 +445,8 @@ void launch_block_inverse(msc_plan *p, const int *gate, const double2 *x, double
 void launch_residual_diag(msc_plan *p, const int *gate, const double2 *x, double2 *out, int with_b,
                           cudaStream_t st)
 {
-    msc::k_residual_diag<<<p->ntiles, 256, smem_residual(p->n), st>>>(
+    const int nt = 2 * p->n <= 512 ? (2 * p->n + 31) / 32 * 32 : 256;
+    msc::k_residual_diag<<<p->ntiles, nt, smem_residual(p->n), st>>>(
         p->tiles(), gate, p->n, p->Tm.p, p->v00.p, p->row_pkd.p, p->row_c.p, p->row_rhs.p, x, out,
         with_b);
 }
