@@ -715,7 +715,9 @@ struct SepTaps {
 
 // (Staging the halo by one bulk copy per halo position instead, on an
 // mbarrier, measured the same: 283 against 280 us on the 512-beam batch.)
-template <int HY, int BX, int ZC, typename R>
+// HXT > 0 fixes the x reach at compile time (square windows: HXT = HY), so
+// the x pass over the 2 HX + 1 halo columns unrolls; 0 takes it from ct.hx.
+template <int HY, int BX, int ZC, typename R, int HXT = 0>
 __global__ void __launch_bounds__(BX * ZC, HY <= 4 ? 3 : 1)
 k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps sep,
                const typename CT<R>::t *__restrict__ src, const typename CT<R>::t *__restrict__ in0,
@@ -727,7 +729,7 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
     constexpr int WY = 2 * HY + 1;
     constexpr int NT = BX * ZC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int HX = ct.hx;
+    const int HX = HXT > 0 ? HXT : ct.hx;
     const int HXW = BX + 2 * HX;
     const int WX = 2 * HX + 1;
     C2 *halo = reinterpret_cast<C2 *>(smem_raw);                       // [HXW][HYW][ZC]
@@ -823,6 +825,7 @@ k_coupling_sep(CouplingTiles ct, const int *__restrict__ gate, int n, SepTaps se
         tr[i] = 0;
         ti[i] = 0;
     }
+#pragma unroll
     for (int sdx = -HX; sdx <= HX; ++sdx) {
         const C2 pv = pw[(sdx + HX) * ZC + zl];
         const C2 *colp = halo + (size_t)(tx - sdx + HX) * HYW * ZC + zl;

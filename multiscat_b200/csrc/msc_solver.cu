@@ -505,8 +505,12 @@ void launch_sep(msc_plan *p, const int *gate, const C2<R> *src, const C2<R> *in0
     const msc::SepTaps sep{base, base + np, base + np + nq};
     dim3 grid(p->nwork, (p->n + ZC - 1) / ZC);
     const size_t sm = sep_smem(p->halo_hx, HY, ZC, sizeof(C2<R>));
-    msc::k_coupling_sep<HY, kHaloBX, ZC, R><<<grid, kHaloBX * ZC, sm, st>>>(
-        ct, gate, p->n, sep, src, in0, sgn, out);
+    if (p->halo_hx == HY)       // square window: the x reach at compile time
+        msc::k_coupling_sep<HY, kHaloBX, ZC, R, HY><<<grid, kHaloBX * ZC, sm, st>>>(
+            ct, gate, p->n, sep, src, in0, sgn, out);
+    else
+        msc::k_coupling_sep<HY, kHaloBX, ZC, R><<<grid, kHaloBX * ZC, sm, st>>>(
+            ct, gate, p->n, sep, src, in0, sgn, out);
 }
 
 // The row-wise separable kernel: square windows (hx = hy), x reach as a
@@ -985,6 +989,12 @@ msc_status set_kernel_attributes(int n, int K)
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>(), R>,              \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
                                   (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>(), sizeof(C2<R>)), 232448))); \
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>(), R, HY>,          \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                  (int)std::min<size_t>(sep_smem(HY, HY, halo_zc<R>(), sizeof(C2<R>)), 232448))); \
+    MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>() / 2, R, HY>,      \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                  (int)std::min<size_t>(sep_smem(HY, HY, halo_zc<R>() / 2, sizeof(C2<R>)), 232448))); \
     MSC_CUDA(cudaFuncSetAttribute(msc::k_coupling_sep<HY, kHaloBX, halo_zc<R>() / 2, R>,          \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
                                   (int)std::min<size_t>(sep_smem(8, HY, halo_zc<R>() / 2, sizeof(C2<R>)), 232448)));
