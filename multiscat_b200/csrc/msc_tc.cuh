@@ -268,6 +268,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     constexpr int NCG = NW / 4;                           // column groups (warps per lane quarter)
     constexpr int CW = (N / NCG >= 16) ? N / NCG : 16;    // columns per warp
     const int c_begin = (wl >> 2) * CW;
+    constexpr bool kInvCache = CW == 16 * kLdChunks;      // one TMEM pass per M tile
+    float invc[2][kInvCache ? CW / 2 : 1];                // 1 / (pkd_j + lam_k) of epilogue 1a
     const bool epi = c_begin < N;                         // narrow tiles: surplus column groups sit out
     const int n = prm.n, kp = prm.kp, mt_count = prm.mt;
     const int kb = kp >> 3;                               // 8-blocks along z and k
@@ -483,11 +485,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         // GEMM 2 consumes; pkd + lam in FP64).  Each 16-column chunk is
         // reduced over the warp's 32 k-lanes by a reduce-scatter butterfly
         // (16 shuffles), then over lane quarters and M tiles in a fixed order.
-        for (int m = 0; m < mt_count && epi; ++m) {
+        // With one TMEM pass per M tile (CW = 32) the thread keeps its
+        // 1 / (pkd_j + lam_k) values for epilogue 1b.
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            if (m >= mt_count || !epi) break;
             const int k = m * 128 + lq * 32 + lane;
             const bool valid = k < n;
             const double lam_k = lam_s[k];
             const float en_k = en_s[k];
+#pragma unroll
             for (int cb = c_begin; cb < c_begin + CW; cb += 16 * kLdChunks) {
             const int nch = min(kLdChunks, (c_begin + CW - cb) >> 4);
             float vv[kLdChunks][16];
@@ -504,7 +511,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     // NaN, which a zero weight would not remove
                     const int j = (c0 + c) >> 1;
                     if (valid && j < nrow) {
-                        const float w = en_k * shifted_inverse(pkd_s[g][j], lam_k);
+                        const float iv = shifted_inverse(pkd_s[g][j], lam_k);
+                        if constexpr (kInvCache) invc[m][(16 * q + c) >> 1] = iv;
+                        const float w = en_k * iv;
                         v[c] *= w;
                         v[c + 1] *= w;
                     } else {
@@ -540,12 +549,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         // GEMM 2 in the MN-major layout: one thread holds one k and 16
         // consecutive columns, i.e. two 16-byte units per hi / lo part
         // (rows k >= kp are never read; k in [n, kp) are zero).
-        for (int m = 0; m < mt_count && epi; ++m) {
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            if (m >= mt_count || !epi) break;
             const int k = m * 128 + lq * 32 + lane;
             const bool valid = k < n;
             const bool stage = k < kp;
             const double lam_k = lam_s[k];
             const float en_k = en_s[k];
+#pragma unroll
             for (int cb = c_begin; cb < c_begin + CW; cb += 16 * kLdChunks) {
             const int nch = min(kLdChunks, (c_begin + CW - cb) >> 4);
             float vv[kLdChunks][16];
@@ -562,7 +574,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                     const int j = (c0 + c) >> 1;
                     float yr = 0.f, yi = 0.f;
                     if (valid && j < nrow) {
-                        const float inv = shifted_inverse(pkd_s[g][j], lam_k);
+                        float inv;
+                        if constexpr (kInvCache) inv = invc[m][(16 * q + c) >> 1];
+                        else inv = shifted_inverse(pkd_s[g][j], lam_k);
                         const float2 b = beta_s[g][j];
                         yr = (v[c] + b.x * en_k) * inv;
                         yi = (v[c + 1] + b.y * en_k) * inv;
