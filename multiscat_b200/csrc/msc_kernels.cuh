@@ -2598,6 +2598,20 @@ __global__ void k_row_tables(int nrows, int n, int ntaps, int nkx, int nky,
     }
 }
 
+// The Sherman-Morrison factor of each row, c / (1 - c f_n), for the tcgen05
+// block inverse (its per-channel complex division, formed once per plan and
+// operator instead of in every tile).
+__global__ void k_row_cfac(int nrows, const double2 *__restrict__ row_c,
+                           const double *__restrict__ fn, double2 *__restrict__ cf)
+{
+    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < nrows;
+         row += gridDim.x * blockDim.x) {
+        const double2 c = row_c[row];
+        const double f = fn[row];
+        cf[row] = cdiv(c, make_double2(1.0 - c.x * f, -c.y * f));
+    }
+}
+
 // dst = src (add = 0) or dst += src (add = 1) on the rows of the gated tiles.
 template <typename R>
 __global__ void __launch_bounds__(256)

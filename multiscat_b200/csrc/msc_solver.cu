@@ -163,6 +163,7 @@ struct msc_plan {
     // device data
     DevBuf<double> E, ET, Tm, lam, en, v00, row_pkd, row_fn;
     DevBuf<double2> Vt, row_c, row_b, row_rhs, sys_aspec;
+    DevBuf<double2> row_cf;        // c / (1 - c f_n) per row (tcgen05 block inverse)
     std::vector<double2> row_c_h, rhs_default_h;   // c per row; default right-hand side
     DevBuf<int> row_pos, pos_map;                  // [R] torus position; [B][nkx*nky] row or -1
     DevBuf<int> sys_row0;                          // [B + 1] first row of each system
@@ -254,6 +255,7 @@ struct msc_plan {
         if (stream) cudaStreamDestroy(stream);
         E.release(); ET.release(); Tm.release(); lam.release(); en.release(); v00.release();
         row_pkd.release(); row_fn.release(); Vt.release(); row_c.release(); row_b.release();
+        row_cf.release();
         row_rhs.release(); sys_aspec.release(); row_pos.release(); pos_map.release();
         sys_row0.release(); nbr.release(); tile_row0.release();
         tile_nrow.release(); tile_sys.release(); sys_tile0.release(); sys_spec_row.release();
@@ -382,8 +384,7 @@ void launch_block_inverse_tc(msc_plan *p, const int *gate, const float2 *x, floa
     prm.lam = p->lam.p;
     prm.en = p->en.p;
     prm.row_pkd = p->row_pkd.p;
-    prm.row_fn = p->row_fn.p;
-    prm.row_c = p->row_c.p;
+    prm.row_cf = p->row_cf.p;
     prm.row_sys = p->row_sys.p;
     prm.gate = gate;
     prm.x = x;
@@ -1623,6 +1624,10 @@ msc_status finalize(msc_plan *p)
         p->row_pkd.p, p->en.p, p->lam.p, p->row_fn.p, p->mixed ? p->row_fn32.p : nullptr,
         p->K > 0 ? p->nbr.p : nullptr);
     MSC_CUDA(cudaGetLastError());
+    MSC_CUDA(p->row_cf.alloc(p->R));
+    msc::k_row_cfac<<<std::min((p->R + 255) / 256, 4096), 256>>>(p->R, p->row_c.p, p->row_fn.p,
+                                                                 p->row_cf.p);
+    MSC_CUDA(cudaGetLastError());
     MSC_CUDA(cudaDeviceSynchronize());
     tm.mark("row tables (device)");
     {
@@ -2665,6 +2670,10 @@ msc_status msc_plan_set_adjoint(msc_plan *p, int32_t adjoint)
         for (double2 &c : rc) c = msc::cconj(c);
     if (p->K > 0) MSC_CUDA(refill(p->Vt, vt));
     MSC_CUDA(refill(p->row_c, rc));
+    msc::k_row_cfac<<<std::min((p->R + 255) / 256, 4096), 256>>>(p->R, p->row_c.p, p->row_fn.p,
+                                                                 p->row_cf.p);
+    MSC_CUDA(cudaGetLastError());
+    MSC_CUDA(cudaDeviceSynchronize());    // the factors are in place before the next solve
     p->adjoint = want;
     if (p->sep_ok) {
         msc_status sst = upload_separable(p);

@@ -220,8 +220,8 @@ struct TcParams {
     int tile_rows;     // channels per tile (N / 2)
     int ntiles;        // ceil(R / tile_rows)
     const __nv_bfloat16 *e_img;   // [2][kp/8][kp/8][8][8]  hi part then lo part
-    const double *lam, *en, *row_pkd, *row_fn;
-    const double2 *row_c;
+    const double *lam, *en, *row_pkd;
+    const double2 *row_cf;        // [R] c / (1 - c f_n) of each row (Sherman-Morrison factor)
     const int *row_sys;           // [R]
     const int *gate;              // [B] or null
     const float2 *x;
@@ -255,8 +255,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
     __shared__ float sm_part[G][4][2][N];     // Sherman-Morrison partial sums [group][lane quarter][M tile][col]
     __shared__ float2 beta_s[G][TR];
     __shared__ double pkd_s[G][TR];
-    __shared__ double2 rc_s[G][TR];            // the tile's boundary constants c_j and fn_j,
-    __shared__ double fn_s[G][TR];             // loaded with pkd while the tile is staged
+    __shared__ double2 cf_s[G][TR];            // the tile's c_j / (1 - c_j fn_j), loaded with pkd
     __shared__ double lam_s[256];             // eigenvalues of H0 (k < n <= 256), 0 past n
     __shared__ float en_s[256];               // last components E[n-1, k] (FP32), 0 past n
 
@@ -389,8 +388,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
         for (int j = gtid; j < TR; j += GT) {
             const bool in = j < nrow;
             pkd_s[g][j] = in ? prm.row_pkd[row0 + j] : 0.0;
-            rc_s[g][j] = in ? prm.row_c[row0 + j] : make_double2(0.0, 0.0);
-            fn_s[g][j] = in ? prm.row_fn[row0 + j] : 0.0;
+            cf_s[g][j] = in ? prm.row_cf[row0 + j] : make_double2(0.0, 0.0);
         }
 
         // ---- stage x as the B operand of GEMM 1 (K-major: rows = 2 TR re/im
@@ -537,9 +535,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tc(TcParams prm)
                         sr += sm_part[g][w][m][2 * j];
                         si += sm_part[g][w][m][2 * j + 1];
                     }
-                const double2 c = rc_s[g][j];
-                const double fn = fn_s[g][j];
-                b = cdiv(cmul(c, make_double2(sr, si)), make_double2(1.0 - c.x * fn, -c.y * fn));
+                b = cmul(cf_s[g][j], make_double2(sr, si));
             }
             beta_s[g][j] = make_float2((float)b.x, (float)b.y);
         }

@@ -53,8 +53,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tcc(TcParams prm)
     __shared__ double sm_part[4][ROWS];       // Sherman-Morrison partial sums [column group][row]
     __shared__ float2 beta_s[TR];
     __shared__ double pkd_s[TR];
-    __shared__ double2 rc_s[TR];
-    __shared__ double fn_s[TR];
+    __shared__ double2 cf_s[TR];              // c_j / (1 - c_j fn_j)
     __shared__ double lam_s[256];
     __shared__ float en_s[256];
     __shared__ int next_s;
@@ -171,8 +170,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tcc(TcParams prm)
         for (int j = tid; j < TR; j += kThreads) {
             const bool in = j < nrow;
             pkd_s[j] = in ? prm.row_pkd[row0 + j] : 0.0;
-            rc_s[j] = in ? prm.row_c[row0 + j] : make_double2(0.0, 0.0);
-            fn_s[j] = in ? prm.row_fn[row0 + j] : 0.0;
+            cf_s[j] = in ? prm.row_cf[row0 + j] : make_double2(0.0, 0.0);
         }
 
         // ---- stage x as the A operand of GEMM 1 (K-major: rows = 2 TR re/im, K = z)
@@ -285,9 +283,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_block_inverse_tcc(TcParams prm)
                     sr += sm_part[w][2 * j];
                     si += sm_part[w][2 * j + 1];
                 }
-                const double2 cj = rc_s[j];
-                const double fn = fn_s[j];
-                b = cdiv(cmul(cj, make_double2(sr, si)), make_double2(1.0 - cj.x * fn, -cj.y * fn));
+                b = cmul(cf_s[j], make_double2(sr, si));
             }
             beta_s[j] = make_float2((float)b.x, (float)b.y);
         }
